@@ -1,0 +1,178 @@
+"""Helpers that run and read the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  It runs either the reference build (_ref/disco_ref, compiled
+from the reference's own sources by oracle/Makefile) or the C restatement
+(_build/disco_port, compiled from oracle/port/), both with the same command
+line and the same dump formats (documented in ref_driver.c).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(HERE, "_ref", "disco_ref")
+PORT_BIN = os.path.join(HERE, "_build", "disco_port")
+PORT_LIB = os.path.join(HERE, "_build", "libdisco_port.so")
+REFSRC = "/root/reference/src"
+
+
+def build(ref: bool | None = None, port: bool = True) -> None:
+    """Compile the oracle.  The reference build needs the reference sources,
+    which exist only where they were mounted; the restatement builds anywhere."""
+    if ref is None:
+        ref = os.path.isdir(REFSRC)
+    targets = (["ref"] if ref else []) + (["port"] if port else [])
+    if targets:
+        subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+def have_port() -> bool:
+    return os.path.exists(PORT_BIN)
+
+
+@dataclass
+class State:
+    NR: int
+    NZ: int
+    NQ: int
+    N: int
+    t: float
+    dt: float
+    gm: np.ndarray          # [2, 6]: r phi M omega Mdot Macc
+    N_p: np.ndarray         # [NR] int32
+    r_faces: np.ndarray     # [NR+1]
+    prim: np.ndarray        # [N, NQ]
+    cons: np.ndarray        # [N, NQ]
+    tiph: np.ndarray        # [N]
+    dphi: np.ndarray        # [N]
+    ext: dict = field(default_factory=dict)
+
+    @property
+    def cell_off(self) -> np.ndarray:
+        return np.concatenate([[0], np.cumsum(self.N_p.astype(np.int64))])
+
+
+def read_state(path: str) -> State:
+    with open(path, "rb") as f:
+        buf = f.read()
+    assert buf[:8] == b"DSTATE1\0", path
+    o = 8
+    NR, NZ, NQ, N, ext = np.frombuffer(buf, np.int32, 5, o); o += 20
+    t, dt = np.frombuffer(buf, np.float64, 2, o); o += 16
+    gm = np.frombuffer(buf, np.float64, 12, o).reshape(2, 6).copy(); o += 96
+
+    def take(dtype, n):
+        nonlocal o
+        a = np.frombuffer(buf, dtype, n, o).copy()
+        o += a.nbytes
+        return a
+
+    N_p = take(np.int32, NR)
+    r_faces = take(np.float64, NR + 1)
+    prim = take(np.float64, N * NQ).reshape(N, NQ)
+    cons = take(np.float64, N * NQ).reshape(N, NQ)
+    tiph = take(np.float64, N)
+    dphi = take(np.float64, N)
+    st = State(int(NR), int(NZ), int(NQ), int(N), float(t), float(dt), gm, N_p, r_faces,
+               prim, cons, tiph, dphi)
+    if ext:
+        st.ext["grad"] = take(np.float64, N * NQ).reshape(N, NQ)
+        st.ext["gradp"] = take(np.float64, N * NQ).reshape(N, NQ)
+        st.ext["wiph"] = take(np.float64, N)
+        st.ext["RKcons"] = take(np.float64, N * NQ).reshape(N, NQ)
+        st.ext["RKtiph"] = take(np.float64, N)
+    return st
+
+
+def write_state(path: str, st: State) -> None:
+    """Write a state file in the driver's format (for --load)."""
+    with open(path, "wb") as f:
+        f.write(b"DSTATE1\0")
+        f.write(np.array([st.NR, st.NZ, st.NQ, st.N, 0], np.int32).tobytes())
+        f.write(np.array([st.t, st.dt], np.float64).tobytes())
+        f.write(np.asarray(st.gm, np.float64).reshape(12).tobytes())
+        f.write(np.asarray(st.N_p, np.int32).tobytes())
+        f.write(np.asarray(st.r_faces, np.float64).tobytes())
+        f.write(np.ascontiguousarray(st.prim, np.float64).tobytes())
+        f.write(np.ascontiguousarray(st.cons, np.float64).tobytes())
+        f.write(np.ascontiguousarray(st.tiph, np.float64).tobytes())
+        f.write(np.ascontiguousarray(st.dphi, np.float64).tobytes())
+
+
+@dataclass
+class Faces:
+    nri: np.ndarray
+    L: np.ndarray
+    R: np.ndarray
+    r: np.ndarray
+    dphi: np.ndarray
+    dA: np.ndarray
+    deltaL: np.ndarray
+    deltaR: np.ndarray
+    cm: np.ndarray
+
+
+def read_faces(path: str) -> Faces:
+    with open(path, "rb") as f:
+        buf = f.read()
+    assert buf[:8] == b"DFACES1\0", path
+    o = 8
+    NR, Nf = np.frombuffer(buf, np.int32, 2, o); o += 8
+    nri = np.frombuffer(buf, np.int32, NR, o).copy(); o += 4 * NR
+    L = np.frombuffer(buf, np.int32, Nf, o).copy(); o += 4 * Nf
+    R = np.frombuffer(buf, np.int32, Nf, o).copy(); o += 4 * Nf
+    arrs = []
+    for _ in range(6):
+        arrs.append(np.frombuffer(buf, np.float64, Nf, o).copy())
+        o += 8 * Nf
+    return Faces(nri, L, R, *arrs)
+
+
+def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = None,
+        faces: bool = False, dtlog: bool = False, workdir: str | None = None):
+    """Run `nsteps` RK2 steps; returns (final State, Faces|None, dt log array|None)."""
+    exe = REF_BIN if impl == "ref" else PORT_BIN
+    if not os.path.exists(exe):
+        raise FileNotFoundError(f"oracle binary missing: {exe} (run oracle.build())")
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        out = os.path.join(td, "out.bin")
+        cmd = [exe, "run", parfile, str(nsteps), out]
+        if load is not None:
+            lp = os.path.join(td, "in.bin")
+            write_state(lp, load)
+            cmd += ["--load", lp]
+        fp = os.path.join(td, "faces.bin")
+        if faces:
+            cmd += ["--faces", fp]
+        lg = os.path.join(td, "dt.log")
+        if dtlog:
+            cmd += ["--dtlog", lg]
+        subprocess.run(cmd, check=True, stderr=subprocess.PIPE)
+        st = read_state(out)
+        fc = read_faces(fp) if faces else None
+        log = np.loadtxt(lg, ndmin=2) if dtlog else None
+    return st, fc, log
+
+
+def stage(parfile: str, phase: int, *, impl: str = "ref", load: State | None = None) -> State:
+    """Run the prologue of one RK2 step and the first substep up to `phase`."""
+    exe = REF_BIN if impl == "ref" else PORT_BIN
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "out.bin")
+        cmd = [exe, "stage", parfile, str(phase), out]
+        if load is not None:
+            lp = os.path.join(td, "in.bin")
+            write_state(lp, load)
+            cmd += ["--load", lp]
+        subprocess.run(cmd, check=True, stderr=subprocess.PIPE)
+        return read_state(out)

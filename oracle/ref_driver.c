@@ -1,0 +1,312 @@
+/*
+ * Oracle driver: runs the reference's own hot path (compiled unmodified from
+ * its src/ tree, see oracle/Makefile) on a parfile and writes binary dumps.
+ * Test infrastructure only; it replaces src/main.c and is never linked into
+ * the product.
+ *
+ * Set-up follows src/main.c:56-123 (MPIsetup, Sim from the parfile, GravMass,
+ * cell_create with its srand(666) phi offsets, clean_pi, syncs, initial data,
+ * calc_cons) without IO or Diagnostics.  Then:
+ *
+ *   disco_ref run <par> <nsteps> <out.bin> [--load in.bin] [--faces f.bin]
+ *                 [--dtlog log.txt]
+ *       loops timestep_rk2 (src/TimeStep/timestep_algorithm.c:11-41) nsteps
+ *       times and dumps the final state.  --load replaces prim/tiph/dphi after
+ *       the initial data (then calc_cons); --faces dumps the r-face list
+ *       (face_create, src/Face/face_create_destroy.c:130-193) of the initial
+ *       state; --dtlog writes "t dt" per step.
+ *
+ *   disco_ref stage <par> <phase> <out.bin> [--load in.bin]
+ *       runs the prologue of timestep_rk2 and then the body of
+ *       timestep_substep (src/TimeStep/timestep_routines.c:16-113), calling
+ *       the same reference functions in the same order, and stops after
+ *       <phase> (0: faces+clean_pi+set_w+RK blend, 1: PLM, 2: phi fluxes,
+ *       3: r fluxes, 4: sources, 5: mesh motion+cons2prim, 6: BC+damping,
+ *       7: calc_cons), dumping the extended cell data.
+ *
+ * State file (little endian): "DSTATE1\0", int32 NR NZ NUM_Q Ncells ext,
+ * double t dt, double gm[2][6] (r phi M omega Mdot Macc), int32 N_p[NR],
+ * double r_faces[NR+1], double prim[Ncells][NUM_Q], cons[Ncells][NUM_Q],
+ * tiph[Ncells], dphi[Ncells]; if ext: grad, gradp ([Ncells][NUM_Q]),
+ * wiph[Ncells], RKcons[Ncells][NUM_Q], RKtiph[Ncells].
+ * Face file: "DFACES1\0", int32 NR Nf, int32 nri[NR], int32 L[Nf] R[Nf]
+ * (cell numbers in (k,i,j) order), double r dphi dA deltaL deltaR cm [Nf].
+ */
+#define CELL_PRIVATE_DEFS
+#define FACE_PRIVATE_DEFS
+#define TIMESTEP_PRIVATE_DEFS
+#define PLANET_PRIVATE_DEFS
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "Headers/Cell.h"
+#include "Headers/Face.h"
+#include "Headers/GravMass.h"
+#include "Headers/MPIsetup.h"
+#include "Headers/Riemann.h"
+#include "Headers/Sim.h"
+#include "Headers/TimeStep.h"
+#include "Headers/header.h"
+#include "ref_newic.h"
+
+int readvar(char *filename, char *varname, int vartype, void *ptr);
+
+static struct Cell *cell_base(struct Cell ***c) { return c[0][0]; }
+
+static int count_cells(struct Sim *s) {
+  int n = 0, i;
+  for (i = 0; i < sim_N(s, R_DIR); ++i) n += sim_N_p(s, i) * sim_N(s, Z_DIR);
+  return n;
+}
+
+static void wr(FILE *f, const void *p, size_t sz, size_t n) {
+  if (fwrite(p, sz, n, f) != n) {
+    fprintf(stderr, "write failed\n");
+    exit(2);
+  }
+}
+static void rd(FILE *f, void *p, size_t sz, size_t n) {
+  if (fread(p, sz, n, f) != n) {
+    fprintf(stderr, "read failed\n");
+    exit(2);
+  }
+}
+
+static void dump_state(const char *path, struct Sim *s, struct Cell ***cells, struct GravMass *gm,
+                       struct TimeStep *ts, int ext) {
+  FILE *f = fopen(path, "wb");
+  int NR = sim_N(s, R_DIR), NZ = sim_N(s, Z_DIR), NQ = sim_NUM_Q(s), N = count_cells(s);
+  int hdr[5];
+  double td[2];
+  double g[12];
+  int i, n, p;
+  struct Cell *c = cell_base(cells);
+  if (!f) {
+    fprintf(stderr, "cannot open %s\n", path);
+    exit(2);
+  }
+  wr(f, "DSTATE1", 1, 8);
+  hdr[0] = NR; hdr[1] = NZ; hdr[2] = NQ; hdr[3] = N; hdr[4] = ext;
+  wr(f, hdr, sizeof(int), 5);
+  td[0] = ts->t; td[1] = ts->dt;
+  wr(f, td, sizeof(double), 2);
+  for (p = 0; p < 2; ++p) {
+    g[6 * p + 0] = gm[p].r; g[6 * p + 1] = gm[p].phi; g[6 * p + 2] = gm[p].M;
+    g[6 * p + 3] = gm[p].omega; g[6 * p + 4] = gm[p].Mdot; g[6 * p + 5] = gm[p].Macc;
+  }
+  wr(f, g, sizeof(double), 12);
+  for (i = 0; i < NR; ++i) { int np = sim_N_p(s, i); wr(f, &np, sizeof(int), 1); }
+  for (i = -1; i < NR; ++i) { double rf = sim_FacePos(s, i, R_DIR); wr(f, &rf, sizeof(double), 1); }
+  for (n = 0; n < N; ++n) wr(f, c[n].prim, sizeof(double), NQ);
+  for (n = 0; n < N; ++n) wr(f, c[n].cons, sizeof(double), NQ);
+  for (n = 0; n < N; ++n) wr(f, &c[n].tiph, sizeof(double), 1);
+  for (n = 0; n < N; ++n) wr(f, &c[n].dphi, sizeof(double), 1);
+  if (ext) {
+    for (n = 0; n < N; ++n) wr(f, c[n].grad, sizeof(double), NQ);
+    for (n = 0; n < N; ++n) wr(f, c[n].gradp, sizeof(double), NQ);
+    for (n = 0; n < N; ++n) wr(f, &c[n].wiph, sizeof(double), 1);
+    for (n = 0; n < N; ++n) wr(f, c[n].RKcons, sizeof(double), NQ);
+    for (n = 0; n < N; ++n) wr(f, &c[n].RKtiph, sizeof(double), 1);
+  }
+  fclose(f);
+}
+
+static void load_state(const char *path, struct Sim *s, struct Cell ***cells) {
+  FILE *f = fopen(path, "rb");
+  int NR = sim_N(s, R_DIR), NQ = sim_NUM_Q(s), N = count_cells(s);
+  char magic[8];
+  int hdr[5], n;
+  double skip[14];
+  struct Cell *c = cell_base(cells);
+  double *buf;
+  if (!f) {
+    fprintf(stderr, "cannot open %s\n", path);
+    exit(2);
+  }
+  rd(f, magic, 1, 8);
+  rd(f, hdr, sizeof(int), 5);
+  if (memcmp(magic, "DSTATE1", 8) != 0 || hdr[0] != NR || hdr[2] != NQ || hdr[3] != N) {
+    fprintf(stderr, "state file %s does not match the parfile grid\n", path);
+    exit(2);
+  }
+  rd(f, skip, sizeof(double), 14);
+  buf = malloc(sizeof(double) * (size_t)(NR + 1) * 2 + sizeof(double) * (size_t)N * NQ);
+  rd(f, buf, sizeof(int), NR);
+  rd(f, buf, sizeof(double), NR + 1);
+  for (n = 0; n < N; ++n) rd(f, c[n].prim, sizeof(double), NQ);
+  rd(f, buf, sizeof(double), (size_t)N * NQ); /* cons: recomputed by calc_cons */
+  for (n = 0; n < N; ++n) rd(f, &c[n].tiph, sizeof(double), 1);
+  for (n = 0; n < N; ++n) rd(f, &c[n].dphi, sizeof(double), 1);
+  free(buf);
+  fclose(f);
+}
+
+static void dump_faces(const char *path, struct Sim *s, struct Cell ***cells, struct TimeStep *ts) {
+  struct Face *F = face_create(cells, s, ts, 0);
+  int NR = sim_N(s, R_DIR);
+  int Nf = ts->nri[NR - 1];
+  struct Cell *c0 = cell_base(cells);
+  FILE *f = fopen(path, "wb");
+  int n;
+  if (!f) {
+    fprintf(stderr, "cannot open %s\n", path);
+    exit(2);
+  }
+  wr(f, "DFACES1", 1, 8);
+  wr(f, &NR, sizeof(int), 1);
+  wr(f, &Nf, sizeof(int), 1);
+  wr(f, ts->nri, sizeof(int), NR);
+  for (n = 0; n < Nf; ++n) { int x = (int)(F[n].L - c0); wr(f, &x, sizeof(int), 1); }
+  for (n = 0; n < Nf; ++n) { int x = (int)(F[n].R - c0); wr(f, &x, sizeof(int), 1); }
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].r, sizeof(double), 1);
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].dphi, sizeof(double), 1);
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].dA, sizeof(double), 1);
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].deltaL, sizeof(double), 1);
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].deltaR, sizeof(double), 1);
+  for (n = 0; n < Nf; ++n) wr(f, &F[n].cm, sizeof(double), 1);
+  fclose(f);
+  face_destroy(F);
+}
+
+/* The body of timestep_substep (src/TimeStep/timestep_routines.c:16-113) as
+ * the same sequence of reference calls, stopping after phase `stop`. */
+static void substep_phases(struct TimeStep *ts, struct Cell ***cells, struct Sim *s,
+                           struct GravMass *gm, struct MPIsetup *mpi, double fac, int stop) {
+  double dt = fac * ts->dt;
+  struct Face *Fr = face_create(cells, s, ts, 0);
+  int i, j, k, n;
+  cell_clean_pi(cells, s);
+  gravMass_clean_pi(gm, s);
+  cell_clear_w(cells, s);
+  cell_set_w(cells, s);
+  cell_adjust_RK_cons(cells, s, ts->RK);
+  if (stop == 0) goto out;
+  cell_plm_p(cells, s);
+  cell_plm_rz(cells, s, Fr, ts, mpi, R_DIR);
+  if (stop == 1) goto out;
+  for (k = 0; k < sim_N(s, Z_DIR); ++k)
+    for (i = 0; i < sim_N(s, R_DIR); ++i)
+      for (j = 0; j < sim_N_p(s, i); ++j) {
+        struct Riemann *R = riemann_create(s);
+        riemann_setup_p(R, cells, s, i, j, k, PDIRECTION);
+        riemann_AddFlux(R, s, gm, dt);
+        riemann_destroy(R);
+      }
+  if (stop == 2) goto out;
+  for (n = 0; n < timestep_n(ts, sim_N(s, R_DIR) - 1, R_DIR); ++n) {
+    struct Riemann *R = riemann_create(s);
+    riemann_setup_rz(R, Fr, s, n, RDIRECTION);
+    riemann_AddFlux(R, s, gm, dt);
+    riemann_destroy(R);
+  }
+  if (stop == 3) goto out;
+  cell_add_src(cells, s, gm, dt);
+  if (sim_EXPLICIT_VISCOSITY(s) > 0.0) cell_add_visc_src(cells, s, gm, dt);
+  cell_add_split_fictitious(cells, s, gm, dt);
+  if (stop == 4) goto out;
+  cell_update_phi(cells, s, gm, ts->RK, dt);
+  cell_update_dphi(cells, s);
+  gravMass_update_RK(gm, s, ts->RK);
+  cell_calc_prim(cells, s);
+  if (stop == 5) goto out;
+  if (sim_BoundTypeR(s) == BOUND_OUTFLOW) {
+    cell_boundary_outflow_r(cells, Fr, s, mpi, ts);
+  } else if (sim_BoundTypeR(s) == BOUND_FIXED) {
+    cell_boundary_fixed_r(cells, s, gm, mpi, (*cell_single_init_ptr(s)));
+  }
+  if (sim_DAMP_TIME(s) > 0.0) cell_bc_damp(cells, s, gm, dt, (*cell_single_init_ptr(s)));
+  if (stop == 6) goto out;
+  cell_calc_cons(cells, s);
+out:
+  face_destroy(Fr);
+}
+
+int main(int argc, char **argv) {
+  const char *mode, *par, *out, *load = NULL, *faces = NULL, *dtlog = NULL;
+  int nsteps, a, step;
+  char parbuf[1024];
+  struct MPIsetup *mpi;
+  struct Sim *s;
+  struct GravMass *gm;
+  struct Cell ***cells;
+  struct TimeStep *ts;
+  FILE *flog = NULL;
+  if (argc < 5) {
+    fprintf(stderr, "usage: disco_ref run|stage <parfile> <nsteps|phase> <out.bin> [options]\n");
+    return 2;
+  }
+  mode = argv[1];
+  par = argv[2];
+  nsteps = atoi(argv[3]);
+  out = argv[4];
+  for (a = 5; a < argc; ++a) {
+    if (!strcmp(argv[a], "--load") && a + 1 < argc) load = argv[++a];
+    else if (!strcmp(argv[a], "--faces") && a + 1 < argc) faces = argv[++a];
+    else if (!strcmp(argv[a], "--dtlog") && a + 1 < argc) dtlog = argv[++a];
+    else {
+      fprintf(stderr, "unknown option %s\n", argv[a]);
+      return 2;
+    }
+  }
+  strncpy(parbuf, par, sizeof(parbuf) - 1);
+  parbuf[sizeof(parbuf) - 1] = 0;
+
+  /* the reference prints its per-step "t: dt:" line and read notices on stdout */
+  if (!freopen("/dev/null", "w", stdout)) return 2;
+
+  mpi = mpisetup_create(argc, argv);
+  mpisetup_setprocs(mpi, parbuf);
+  mpisetup_cart_create(mpi);
+  mpisetup_left_right(mpi);
+  s = sim_create(mpi);
+  if (sim_read_par_file(s, mpi, parbuf) != 0) {
+    fprintf(stderr, "parfile read failed: %s\n", par);
+    return 3;
+  }
+  readvar(parbuf, "IC_HoR", VAR_DOUB, &oracle_ic_hor);
+  readvar(parbuf, "IC_Noise", VAR_DOUB, &oracle_ic_noise);
+  readvar(parbuf, "IC_Seed", VAR_INT, &oracle_ic_seed);
+  sim_alloc_arr(s, mpi);
+  sim_set_rz(s, mpi);
+  sim_set_N_p(s);
+  sim_set_misc(s, mpi);
+  gm = gravMass_create(sim_NumGravMass(s));
+  cells = cell_create(s, mpi);
+  cell_clean_pi(cells, s);
+  cell_syncproc_r(cells, s, mpi);
+  cell_syncproc_z(cells, s, mpi);
+  ts = timestep_create(s);
+  ts->dt = 0.0;
+  (*gravMass_init_ptr(s))(gm, s);
+  (*cell_init_ptr(s))(cells, s, gm, mpi);
+  gravMass_clean_pi(gm, s);
+  if (load) load_state(load, s, cells);
+  cell_syncproc_r(cells, s, mpi);
+  cell_syncproc_z(cells, s, mpi);
+  cell_calc_cons(cells, s);
+
+  if (!strcmp(mode, "run")) {
+    if (faces) dump_faces(faces, s, cells, ts);
+    if (dtlog) flog = fopen(dtlog, "w");
+    for (step = 0; step < nsteps; ++step) {
+      timestep_rk2(ts, s, cells, gm, mpi);
+      if (flog) fprintf(flog, "%.17g %.17g\n", ts->t, ts->dt);
+    }
+    if (flog) fclose(flog);
+    dump_state(out, s, cells, gm, ts, 0);
+  } else if (!strcmp(mode, "stage")) {
+    /* prologue of timestep_rk2 (timestep_algorithm.c:13-24), then one substep */
+    cell_clear_w(cells, s);
+    cell_set_w(cells, s);
+    timestep_set_dt(ts, cells, s, gm);
+    cell_copy(cells, s);
+    gravMass_copy(gm, s);
+    timestep_set_RK(ts, 0.0);
+    substep_phases(ts, cells, s, gm, mpi, 1.0, nsteps);
+    dump_state(out, s, cells, gm, ts, 1);
+  } else {
+    fprintf(stderr, "unknown mode %s\n", mode);
+    return 2;
+  }
+  return 0;
+}
