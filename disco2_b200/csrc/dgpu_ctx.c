@@ -1,0 +1,735 @@
+/*
+ * Host orchestration of the B200 step (C99 over the CUDA runtime API).
+ *
+ * A context owns the device copy of one or more disks: the annulus-major
+ * structure-of-arrays state, the per-annulus tables, the r-face slabs and the
+ * per-disk GravMass/time state.  One RK2 step (timestep_rk2,
+ * src/TimeStep/timestep_algorithm.c:11-41) is eight kernel launches, captured
+ * once into a CUDA graph and replayed; no host synchronisation happens inside
+ * a step (dt, t and the GravMass orbit live on the device).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../include/disco_gpu.h"
+#include "dgpu_internal.h"
+#include "dgpu_sim.h"
+
+struct dgpu_ctx {
+  int device;
+  cudaStream_t stream;
+  int own_stream;
+  int n_inst;
+  struct dgpu_sim **sims;
+  DiskParams *h_par;
+  Annulus *h_ann;
+  int n_ann, n_cells, n_slots, n_runs, n_upd_blocks;
+  DevPtrs d;          /* device pointers */
+  DiskParams *d_par;
+  InstState *d_ist;
+  Annulus *d_ann;
+  int *d_cell_ann, *d_slot_ann;
+  double *d_stage;    /* AoS staging buffer: max cells of a disk x NQ */
+  double *d_torque;   /* partial sums + result */
+  cudaGraphExec_t graph;
+  int have_graph;
+  char err[512];
+};
+
+static __thread char g_err[512];
+
+static int fail(struct dgpu_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  char *dst = c ? c->err : g_err;
+  va_start(ap, fmt);
+  vsnprintf(dst, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(c, DGPU_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
+                  __FILE__, __LINE__);                                                    \
+  } while (0)
+#define CKK(call)                                                                         \
+  do {                                                                                    \
+    int e_ = (call);                                                                      \
+    if (e_ != 0)                                                                          \
+      return fail(c, DGPU_ERR_CUDA, "%s: %s (%s:%d)", #call,                              \
+                  cudaGetErrorString((cudaError_t)e_), __FILE__, __LINE__);               \
+  } while (0)
+
+/* ---------------- Sim ---------------- */
+
+int dgpu_sim_from_text(const char *text, dgpu_sim **out) {
+  struct dgpu_sim *s;
+  int rc;
+  if (!text || !out) return fail(NULL, DGPU_ERR_ARG, "null argument");
+  s = (struct dgpu_sim *)calloc(1, sizeof(*s));
+  if (!s) return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
+  rc = dsim_parse(text, s, g_err, sizeof(g_err));
+  if (rc == DGPU_OK) rc = dsim_build_grid(s, g_err, sizeof(g_err));
+  if (rc != DGPU_OK) {
+    dsim_free(s);
+    return rc;
+  }
+  *out = s;
+  return DGPU_OK;
+}
+
+int dgpu_sim_from_parfile(const char *path, dgpu_sim **out) {
+  FILE *f;
+  long n;
+  char *buf;
+  int rc;
+  if (!path) return fail(NULL, DGPU_ERR_ARG, "null path");
+  f = fopen(path, "rb");
+  if (!f) return fail(NULL, DGPU_ERR_PARFILE, "cannot open parfile %s", path);
+  fseek(f, 0, SEEK_END);
+  n = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  buf = (char *)malloc((size_t)n + 1);
+  if (!buf) {
+    fclose(f);
+    return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
+  }
+  if (fread(buf, 1, (size_t)n, f) != (size_t)n) {
+    fclose(f);
+    free(buf);
+    return fail(NULL, DGPU_ERR_PARFILE, "cannot read parfile %s", path);
+  }
+  fclose(f);
+  buf[n] = 0;
+  rc = dgpu_sim_from_text(buf, out);
+  free(buf);
+  return rc;
+}
+
+void dgpu_sim_destroy(dgpu_sim *sim) { dsim_free(sim); }
+int dgpu_sim_num_annuli(const dgpu_sim *sim) { return sim ? sim->NR : DGPU_ERR_ARG; }
+int dgpu_sim_num_cells(const dgpu_sim *sim) { return sim ? sim->Ncells : DGPU_ERR_ARG; }
+
+int dgpu_sim_grid(const dgpu_sim *sim, int *N_p, double *r_faces) {
+  if (!sim) return DGPU_ERR_ARG;
+  if (N_p) memcpy(N_p, sim->N_p, sizeof(int) * (size_t)sim->NR);
+  if (r_faces) memcpy(r_faces, sim->r_faces, sizeof(double) * (size_t)(sim->NR + 1));
+  return DGPU_OK;
+}
+
+int dgpu_sim_param(const dgpu_sim *sim, const char *key, double *value) {
+#define P_I(n, f) if (!strcmp(key, n)) { *value = (double)sim->f; return DGPU_OK; }
+#define P_D(n, f) if (!strcmp(key, n)) { *value = sim->f; return DGPU_OK; }
+  if (!sim || !key || !value) return DGPU_ERR_ARG;
+  P_I("Restart", Restart) P_I("InitialDataType", InitialDataType) P_I("GravMassType", GravMassType)
+  P_D("MassRatio", MassRatio) P_D("OrbShrinkTscale", OrbShrinkTscale) P_D("OrbShrinkT0", OrbShrinkT0)
+  P_I("BoundTypeR", BoundTypeR) P_I("BoundTypeZ", BoundTypeZ) P_I("NoInnerBC", NoInnerBC)
+  P_I("NumR", NumR) P_I("NumZ", NumZ) P_I("ng", ng) P_D("R_Min", R_Min) P_D("R_Max", R_Max)
+  P_D("Z_Min", Z_Min) P_D("Z_Max", Z_Max) P_I("NP_CONST", NP_CONST) P_I("NPCAP", NPCAP)
+  P_D("aspect", aspect) P_I("NUM_C", NUM_C) P_I("NUM_N", NUM_N) P_D("Time_Max", Time_Max)
+  P_I("w_numeric_type", w_numeric_type) P_I("RiemannSolver", RiemannSolver)
+  P_D("Adiabatic_Index", Adiabatic_Index) P_I("Cooling", Cooling)
+  P_D("Explicit_Viscosity", Explicit_Viscosity) P_I("ViscConst", ViscConst) P_D("PoRho_r1", PoRho_r1)
+  P_D("CFL", CFL) P_D("PLM", PLM) P_I("Grav_2D", Grav_2D) P_D("G_EPS", G_EPS)
+  P_I("RhoSinkOn", RhoSinkOn) P_I("PHI_ORDER", PHI_ORDER) P_D("Rho_Floor", Rho_Floor)
+  P_D("Cs_Floor", Cs_Floor) P_D("Cs_Cap", Cs_Cap) P_D("Vel_Cap", Vel_Cap) P_D("DAMP_TIME", DAMP_TIME)
+  P_D("RDAMP_INNER", RDAMP_INNER) P_D("RDAMP_OUTER", RDAMP_OUTER) P_D("RLogScale", RLogScale)
+  P_D("ZLogScale", ZLogScale) P_D("HiResSigma", HiResSigma) P_D("HiResR0a", HiResR0a)
+  P_D("HiResR0b", HiResR0b) P_D("HiResFac", HiResFac) P_I("w_analytic_type", w_analytic_type)
+  P_D("IC_HoR", IC_HoR) P_D("IC_Noise", IC_Noise) P_I("IC_Seed", IC_Seed)
+  P_I("NR", NR) P_I("Ncells", Ncells)
+#undef P_I
+#undef P_D
+  return DGPU_ERR_ARG;
+}
+
+int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double *dphi, double *gm) {
+  double *t = tiph, *d = dphi, g[12];
+  long idx = 0;
+  int i, j, rc;
+  if (!s) return fail(NULL, DGPU_ERR_ARG, "null sim");
+  if (!t) t = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
+  if (!d) d = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
+  if (!t || !d) {
+    if (t != tiph) free(t);
+    if (d != dphi) free(d);
+    return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
+  }
+  dsim_initial_tiph(s, t, d);
+  rc = DGPU_OK;
+  if (prim) {
+    for (i = 0; i < s->NR && rc == DGPU_OK; ++i)
+      for (j = 0; j < s->N_p[i]; ++j, ++idx)
+        if (dsim_grid_init(s, i, idx, prim + 5 * idx) != 0) {
+          rc = fail(NULL, DGPU_ERR_UNSUPPORTED, "InitialDataType %d has no whole-grid initialiser here", s->InitialDataType);
+          break;
+        }
+  }
+  if (rc == DGPU_OK) {
+    rc = dsim_initial_gravmass(s, g);
+    if (rc != DGPU_OK) rc = fail(NULL, rc, "bad GravMassType");
+    else if (gm) memcpy(gm, g, sizeof(g));
+  }
+  if (t != tiph) free(t);
+  if (d != dphi) free(d);
+  return rc;
+}
+
+/* ---------------- Context ---------------- */
+
+static int check_supported(const struct dgpu_sim *s, int k, char *err, int n) {
+  int i;
+  if (s->NumZ != 1) return snprintf(err, (size_t)n, "disk %d: NumZ > 1 (3-D z faces) is not implemented", k), DGPU_ERR_UNSUPPORTED;
+  if (s->NUM_C != 5 || s->NUM_N != 0) return snprintf(err, (size_t)n, "disk %d: only NUM_C = 5, NUM_N = 0 is implemented", k), DGPU_ERR_UNSUPPORTED;
+  if (s->NR < 3) return snprintf(err, (size_t)n, "disk %d: need at least 3 annuli", k), DGPU_ERR_UNSUPPORTED;
+  for (i = 0; i < s->NR; ++i)
+    if (s->N_p[i] < 2) return snprintf(err, (size_t)n, "disk %d: annulus %d has fewer than 2 cells", k, i), DGPU_ERR_UNSUPPORTED;
+  if (s->w_numeric_type == DC_WCELL || s->w_numeric_type < 0 || s->w_numeric_type > DC_POWERLAW)
+    return snprintf(err, (size_t)n, "disk %d: w_numeric_type %d is not usable (the reference exits on C_WCELL)", k, s->w_numeric_type), DGPU_ERR_UNSUPPORTED;
+  if (s->w_analytic_type < 0 || s->w_analytic_type > DA_POWERLAW)
+    return snprintf(err, (size_t)n, "disk %d: bad w_analytic_type", k), DGPU_ERR_PARFILE;
+  if (s->RiemannSolver != DR_HLLC && s->RiemannSolver != DR_HLL)
+    return snprintf(err, (size_t)n, "disk %d: bad RiemannSolver", k), DGPU_ERR_PARFILE;
+  if (s->BoundTypeR == DB_OUTFLOW)
+    return snprintf(err, (size_t)n, "disk %d: outflow radial boundaries are not implemented", k), DGPU_ERR_UNSUPPORTED;
+  if (s->GravMassType < 0 || s->GravMassType > 2)
+    return snprintf(err, (size_t)n, "disk %d: bad GravMassType", k), DGPU_ERR_PARFILE;
+  if (s->BoundTypeR == DB_FIXED || s->DAMP_TIME > 0.0) {
+    double prim[DGPU_NQ];
+    if (dsim_single_init(s, 0, prim) < 0)
+      return snprintf(err, (size_t)n, "disk %d: InitialDataType %d has no axisymmetric single-cell form for the fixed boundary/damping", k, s->InitialDataType), DGPU_ERR_UNSUPPORTED;
+  }
+  return DGPU_OK;
+}
+
+static void *dmalloc(size_t bytes, int *ok) {
+  void *p = NULL;
+  if (bytes == 0) bytes = 8;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    *ok = 0;
+    return NULL;
+  }
+  cudaMemset(p, 0, bytes);
+  return p;
+}
+
+void dgpu_destroy(dgpu_ctx *c) {
+  int k;
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->have_graph) cudaGraphExecDestroy(c->graph);
+  {
+    void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
+                  c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
+                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
+                  c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
+                  c->d.mdot_part, c->d.counters, c->d.err, c->d_stage, c->d_torque};
+    for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
+      if (ps[k]) cudaFree(ps[k]);
+  }
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->sims) {
+    for (k = 0; k < c->n_inst; ++k) dsim_free(c->sims[k]);
+    free(c->sims);
+  }
+  free(c->h_par);
+  free(c->h_ann);
+  free(c);
+}
+
+int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dgpu_ctx **out) {
+  struct dgpu_ctx *c;
+  int k, i, rc, ok = 1;
+  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0;
+  int *h_cell_ann, *h_slot_ann;
+  if (!sims || n < 1 || !out) return fail(NULL, DGPU_ERR_ARG, "bad arguments to dgpu_create");
+  for (k = 0; k < n; ++k) {
+    if (!sims[k]) return fail(NULL, DGPU_ERR_ARG, "sim %d is null", k);
+    rc = check_supported(sims[k], k, g_err, sizeof(g_err));
+    if (rc != DGPU_OK) return rc;
+  }
+  c = (struct dgpu_ctx *)calloc(1, sizeof(*c));
+  if (!c) return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
+  c->device = device;
+  c->n_inst = n;
+  c->sims = (struct dgpu_sim **)calloc((size_t)n, sizeof(*c->sims));
+  c->h_par = (DiskParams *)calloc((size_t)n, sizeof(DiskParams));
+  for (k = 0; k < n; ++k) {
+    c->sims[k] = dsim_clone(sims[k]);
+    if (!c->sims[k]) {
+      dgpu_destroy(c);
+      return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
+    }
+    ann += sims[k]->NR;
+    cells += sims[k]->Ncells;
+    if (sims[k]->Ncells > maxcells) maxcells = sims[k]->Ncells;
+  }
+  c->n_ann = ann;
+  c->n_cells = cells;
+  c->h_ann = (Annulus *)calloc((size_t)ann, sizeof(Annulus));
+  h_cell_ann = (int *)malloc(sizeof(int) * (size_t)cells);
+  /* tables */
+  ann = 0;
+  cells = 0;
+  for (k = 0; k < n; ++k) {
+    const struct dgpu_sim *s = c->sims[k];
+    DiskParams *p = &c->h_par[k];
+    dsim_fill_params(s, p);
+    p->ann_base = ann;
+    p->cell_base = cells;
+    for (i = 0; i < s->NR; ++i) {
+      Annulus *a = &c->h_ann[ann + i];
+      int j;
+      dsim_fill_annulus(s, i, a);
+      a->inst = k;
+      a->cell_off = cells;
+      for (j = 0; j < s->N_p[i]; ++j) h_cell_ann[cells + j] = ann + i;
+      cells += s->N_p[i];
+      if (i < s->NR - 1) {
+        a->face_base = slots;
+        a->face_cap = s->N_p[i] + s->N_p[i + 1] + DGPU_FACE_SLACK;
+        slots += a->face_cap;
+        a->run_base = runs;
+        a->run_cap = s->N_p[i + 1] + DGPU_RUN_SLACK;
+        runs += a->run_cap;
+      } else {
+        a->face_base = slots;
+        a->face_cap = 0;
+        a->run_base = runs;
+        a->run_cap = 0;
+      }
+    }
+    ann += s->NR;
+  }
+  c->n_slots = slots;
+  c->n_runs = runs;
+  h_slot_ann = (int *)malloc(sizeof(int) * (size_t)(slots > 0 ? slots : 1));
+  for (i = 0; i < c->n_ann; ++i) {
+    int f;
+    for (f = 0; f < c->h_ann[i].face_cap; ++f) h_slot_ann[c->h_ann[i].face_base + f] = i;
+  }
+  c->n_upd_blocks = dgk_update_blocks(c->n_cells);
+
+  if (cudaSetDevice(device) != cudaSuccess) {
+    free(h_cell_ann);
+    free(h_slot_ann);
+    dgpu_destroy(c);
+    return fail(NULL, DGPU_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  }
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      free(h_cell_ann);
+      free(h_slot_ann);
+      dgpu_destroy(c);
+      return fail(NULL, DGPU_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    c->own_stream = 1;
+  }
+  {
+    size_t N = (size_t)c->n_cells, S = (size_t)c->n_slots, A = (size_t)c->n_ann;
+    c->d_par = (DiskParams *)dmalloc(sizeof(DiskParams) * (size_t)n, &ok);
+    c->d_ist = (InstState *)dmalloc(sizeof(InstState) * (size_t)n, &ok);
+    c->d_ann = (Annulus *)dmalloc(sizeof(Annulus) * A, &ok);
+    c->d_cell_ann = (int *)dmalloc(sizeof(int) * N, &ok);
+    c->d_slot_ann = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
+    c->d.prim = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.cons = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.rkcons = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.grad = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.gradp = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.tiph0 = (double *)dmalloc(sizeof(double) * N, &ok);
+    c->d.tiph1 = (double *)dmalloc(sizeof(double) * N, &ok);
+    c->d.tiphw = (double *)dmalloc(sizeof(double) * N, &ok);
+    c->d.rktiph = (double *)dmalloc(sizeof(double) * N, &ok);
+    c->d.dphi = (double *)dmalloc(sizeof(double) * N, &ok);
+    c->d.w_ann = (double *)dmalloc(sizeof(double) * A, &ok);
+    c->d.fphi = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
+    c->d.frf = (double *)dmalloc(sizeof(double) * 8 * (S ? S : 1), &ok);
+    c->d.fstart = (int *)dmalloc(sizeof(int) * N, &ok);
+    c->d.fL = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
+    c->d.fR = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
+    c->d.fdphi = (double *)dmalloc(sizeof(double) * (S ? S : 1), &ok);
+    c->d.fcm = (double *)dmalloc(sizeof(double) * (S ? S : 1), &ok);
+    c->d.pair_nf = (int *)dmalloc(sizeof(int) * A, &ok);
+    c->d.pair_jpmin = (int *)dmalloc(sizeof(int) * A, &ok);
+    c->d.pair_T = (int *)dmalloc(sizeof(int) * A, &ok);
+    c->d.pair_seq = (int *)dmalloc(sizeof(int) * A, &ok);
+    c->d.runs = (int *)dmalloc(sizeof(int) * (size_t)(c->n_runs ? c->n_runs : 1), &ok);
+    c->d.mdot_part = (double *)dmalloc(sizeof(double) * 2 * (size_t)c->n_upd_blocks, &ok);
+    c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
+    c->d.err = (int *)dmalloc(sizeof(int), &ok);
+    c->d_stage = (double *)dmalloc(sizeof(double) * 5 * (size_t)maxcells, &ok);
+    c->d_torque = (double *)dmalloc(sizeof(double) * ((size_t)maxcells / 256 + 8), &ok);
+  }
+  if (!ok) {
+    free(h_cell_ann);
+    free(h_slot_ann);
+    dgpu_destroy(c);
+    return fail(NULL, DGPU_ERR_NOMEM, "device allocation failed");
+  }
+  c->d.n_inst = n;
+  c->d.n_ann = c->n_ann;
+  c->d.n_cells = c->n_cells;
+  c->d.n_slots = c->n_slots;
+  c->d.n_runs = c->n_runs;
+  c->d.par = c->d_par;
+  c->d.ist = c->d_ist;
+  c->d.ann = c->d_ann;
+  c->d.cell_ann = c->d_cell_ann;
+  c->d.slot_ann = c->d_slot_ann;
+  if (cudaMemcpy(c->d_par, c->h_par, sizeof(DiskParams) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_ann, c->h_ann, sizeof(Annulus) * (size_t)c->n_ann, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_cell_ann, h_cell_ann, sizeof(int) * (size_t)c->n_cells, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_slot_ann, h_slot_ann, sizeof(int) * (size_t)(c->n_slots ? c->n_slots : 1),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    free(h_cell_ann);
+    free(h_slot_ann);
+    dgpu_destroy(c);
+    return fail(NULL, DGPU_ERR_CUDA, "table upload failed");
+  }
+  free(h_cell_ann);
+  free(h_slot_ann);
+  *out = c;
+  return DGPU_OK;
+}
+
+const char *dgpu_last_error(const dgpu_ctx *c) { return c ? c->err : g_err; }
+int dgpu_num_instances(const dgpu_ctx *c) { return c ? c->n_inst : DGPU_ERR_ARG; }
+
+static int check_inst(struct dgpu_ctx *c, int inst) {
+  if (!c) return DGPU_ERR_ARG;
+  if (inst < 0 || inst >= c->n_inst) return fail(c, DGPU_ERR_ARG, "instance %d out of range", inst);
+  cudaSetDevice(c->device);
+  return DGPU_OK;
+}
+
+static int read_err(struct dgpu_ctx *c) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, c->d.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (e & (DGPU_EF_FACE_OVERFLOW | DGPU_EF_RUN_OVERFLOW))
+    return fail(c, DGPU_ERR_FACE_OVERFLOW, "face list overflowed its buffer (flags 0x%x)", e);
+  if (e & DGPU_EF_WRAP_LIMIT)
+    return fail(c, DGPU_ERR_NUMERIC, "a phi wrap loop did not terminate (non-finite phi edge; flags 0x%x)", e);
+  if (e & DGPU_EF_VISC_VZ)
+    return fail(c, DGPU_ERR_NUMERIC, "viscosity with nonzero v_z (the reference exits here, Riemann_routines.c:271-274)");
+  return DGPU_OK;
+}
+
+int dgpu_synchronize(dgpu_ctx *c) {
+  if (!c) return DGPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return read_err(c);
+}
+
+/* state upload of one disk: prim AoS [N][5], tiph, dphi (host) */
+static int upload_disk(struct dgpu_ctx *c, int inst, const double *prim, const double *tiph, const double *dphi) {
+  const DiskParams *p = &c->h_par[inst];
+  int n = p->n_cells, base = p->cell_base;
+  if (prim) {
+    CK(cudaMemcpyAsync(c->d_stage, prim, sizeof(double) * 5 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    CKK(dgk_aos_to_soa(c->d.prim, 5, c->n_cells, base, c->d_stage, n, c->stream));
+  }
+  if (tiph) CK(cudaMemcpyAsync(c->d.tiph0 + base, tiph, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  if (dphi) CK(cudaMemcpyAsync(c->d.dphi + base, dphi, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+  CKK(dgk_calc_cons(&c->d, c->stream));
+  return DGPU_OK;
+}
+
+int dgpu_set_state(dgpu_ctx *c, int inst, const double *prim, const double *tiph, const double *dphi) {
+  int rc = check_inst(c, inst);
+  if (rc) return rc;
+  rc = upload_disk(c, inst, prim, tiph, dphi);
+  if (rc) return rc;
+  return DGPU_OK;
+}
+
+int dgpu_get_state(dgpu_ctx *c, int inst, double *prim, double *cons, double *tiph, double *dphi) {
+  const DiskParams *p;
+  int n, base, rc = check_inst(c, inst);
+  if (rc) return rc;
+  p = &c->h_par[inst];
+  n = p->n_cells;
+  base = p->cell_base;
+  if (prim) {
+    CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, c->d.prim, n, c->stream));
+    CK(cudaMemcpyAsync(prim, c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    if (cons) CK(cudaStreamSynchronize(c->stream));
+  }
+  if (cons) {
+    CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, c->d.cons, n, c->stream));
+    CK(cudaMemcpyAsync(cons, c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  }
+  if (tiph) CK(cudaMemcpyAsync(tiph, c->d.tiph0 + base, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  if (dphi) CK(cudaMemcpyAsync(dphi, c->d.dphi + base, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  return dgpu_synchronize(c);
+}
+
+int dgpu_get_stage_data(dgpu_ctx *c, int inst, double *grad, double *gradp, double *wiph, double *rkcons,
+                        double *rktiph) {
+  const DiskParams *p;
+  int n, base, rc = check_inst(c, inst);
+  if (rc) return rc;
+  p = &c->h_par[inst];
+  n = p->n_cells;
+  base = p->cell_base;
+  {
+    double *srcs[3] = {c->d.grad, c->d.gradp, c->d.rkcons};
+    double *dsts[3] = {grad, gradp, rkcons};
+    int k;
+    for (k = 0; k < 3; ++k) {
+      if (!dsts[k]) continue;
+      CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, srcs[k], n, c->stream));
+      CK(cudaMemcpyAsync(dsts[k], c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+  }
+  if (rktiph) CK(cudaMemcpyAsync(rktiph, c->d.rktiph + base, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  if (wiph) {
+    /* wiph is one value per annulus */
+    const struct dgpu_sim *s = c->sims[inst];
+    double *w = (double *)malloc(sizeof(double) * (size_t)s->NR);
+    int i, j, m = 0;
+    if (!w) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+    if (cudaMemcpyAsync(w, c->d.w_ann + p->ann_base, sizeof(double) * (size_t)s->NR, cudaMemcpyDeviceToHost,
+                        c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      free(w);
+      return fail(c, DGPU_ERR_CUDA, "wiph download failed");
+    }
+    for (i = 0; i < s->NR; ++i)
+      for (j = 0; j < s->N_p[i]; ++j) wiph[m++] = w[i];
+    free(w);
+  }
+  return dgpu_synchronize(c);
+}
+
+static int get_ist(struct dgpu_ctx *c, int inst, InstState *st) {
+  CK(cudaMemcpyAsync(st, c->d_ist + inst, sizeof(InstState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DGPU_OK;
+}
+static int put_ist(struct dgpu_ctx *c, int inst, const InstState *st) {
+  CK(cudaMemcpyAsync(c->d_ist + inst, st, sizeof(InstState), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DGPU_OK;
+}
+
+int dgpu_set_gravmass(dgpu_ctx *c, int inst, const double *gm) {
+  InstState st;
+  int p, rc = check_inst(c, inst);
+  if (rc) return rc;
+  if (!gm) return fail(c, DGPU_ERR_ARG, "null gm");
+  if ((rc = get_ist(c, inst, &st))) return rc;
+  for (p = 0; p < 2; ++p) {
+    st.gr[p] = gm[6 * p + 0];
+    st.gphi[p] = gm[6 * p + 1];
+    st.gM[p] = gm[6 * p + 2];
+    st.gom[p] = gm[6 * p + 3];
+    st.mdot[p] = gm[6 * p + 4];
+    st.macc[p] = gm[6 * p + 5];
+  }
+  return put_ist(c, inst, &st);
+}
+
+int dgpu_get_gravmass(dgpu_ctx *c, int inst, double *gm) {
+  InstState st;
+  int p, rc = check_inst(c, inst);
+  if (rc) return rc;
+  if ((rc = get_ist(c, inst, &st))) return rc;
+  for (p = 0; p < 2; ++p) {
+    gm[6 * p + 0] = st.gr[p];
+    gm[6 * p + 1] = st.gphi[p];
+    gm[6 * p + 2] = st.gM[p];
+    gm[6 * p + 3] = st.gom[p];
+    gm[6 * p + 4] = st.mdot[p];
+    gm[6 * p + 5] = st.macc[p];
+  }
+  return DGPU_OK;
+}
+
+int dgpu_get_time(dgpu_ctx *c, int inst, double *t, double *dt) {
+  InstState st;
+  int rc = check_inst(c, inst);
+  if (rc) return rc;
+  if ((rc = get_ist(c, inst, &st))) return rc;
+  if (t) *t = st.t;
+  if (dt) *dt = st.dt;
+  return DGPU_OK;
+}
+
+int dgpu_set_time(dgpu_ctx *c, int inst, double t) {
+  InstState st;
+  int rc = check_inst(c, inst);
+  if (rc) return rc;
+  if ((rc = get_ist(c, inst, &st))) return rc;
+  st.t = t;
+  return put_ist(c, inst, &st);
+}
+
+int dgpu_init_state(dgpu_ctx *c, int inst) {
+  const struct dgpu_sim *s;
+  double *prim, *tiph, *dphi, gm[12];
+  int rc = check_inst(c, inst);
+  if (rc) return rc;
+  s = c->sims[inst];
+  prim = (double *)malloc(sizeof(double) * 5 * (size_t)s->Ncells);
+  tiph = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
+  dphi = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
+  if (!prim || !tiph || !dphi) {
+    free(prim); free(tiph); free(dphi);
+    return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+  }
+  rc = dgpu_sim_initial_state(s, prim, tiph, dphi, gm);
+  if (rc != DGPU_OK) {
+    free(prim); free(tiph); free(dphi);
+    return fail(c, rc, "%s", g_err);
+  }
+  rc = upload_disk(c, inst, prim, tiph, dphi);
+  if (rc == DGPU_OK) rc = dgpu_synchronize(c);
+  free(prim); free(tiph); free(dphi);
+  if (rc) return rc;
+  {
+    InstState st;
+    int p;
+    memset(&st, 0, sizeof(st));
+    for (p = 0; p < 2; ++p) {
+      st.gr[p] = gm[6 * p + 0];
+      st.gphi[p] = gm[6 * p + 1];
+      st.gM[p] = gm[6 * p + 2];
+      st.gom[p] = gm[6 * p + 3];
+    }
+    rc = put_ist(c, inst, &st);
+  }
+  return rc;
+}
+
+static int launch_step(struct dgpu_ctx *c) {
+  int sub;
+  for (sub = 1; sub <= 2; ++sub) {
+    CKK(dgk_face(&c->d, sub, 1, c->stream));
+    CKK(dgk_plm_r(&c->d, sub, c->stream));
+    CKK(dgk_flux(&c->d, sub, c->stream));
+    CKK(dgk_update(&c->d, sub, 7, c->stream));
+  }
+  return DGPU_OK;
+}
+
+int dgpu_step_rk2(dgpu_ctx *c, int nsteps) {
+  int k;
+  if (!c || nsteps < 0) return DGPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (!c->have_graph) {
+    cudaGraph_t g;
+    int rc;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = launch_step(c);
+    {
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(c, DGPU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    }
+    {
+      cudaError_t e = cudaGraphInstantiate(&c->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(c, DGPU_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    }
+    c->have_graph = 1;
+  }
+  for (k = 0; k < nsteps; ++k) CK(cudaGraphLaunch(c->graph, c->stream));
+  return DGPU_OK;
+}
+
+int dgpu_stage(dgpu_ctx *c, int phase) {
+  if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  CKK(dgk_face(&c->d, 1, 1, c->stream));
+  /* the CFL minimum (and dt) come from k_plm_r; PLM results are kept only from phase 1 on */
+  CKK(dgk_plm_r(&c->d, 1, c->stream));
+  if (phase >= 2) CKK(dgk_flux(&c->d, 1, c->stream));
+  CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
+  return dgpu_synchronize(c);
+}
+
+int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, double *r, double *dphi,
+                   double *dA, double *deltaL, double *deltaR, double *cm, int *nf_out) {
+  const struct dgpu_sim *s;
+  const DiskParams *p;
+  int i, total = 0, rc = check_inst(c, inst);
+  int *nf, *fL, *fR;
+  double *fd, *fc;
+  if (rc) return rc;
+  s = c->sims[inst];
+  p = &c->h_par[inst];
+  /* build the list of the current state: one k_face pass (substep-1 buffers) */
+  CKK(dgk_face(&c->d, 1, 0, c->stream));
+  if ((rc = dgpu_synchronize(c))) return rc;
+  nf = (int *)malloc(sizeof(int) * (size_t)s->NR);
+  fL = (int *)malloc(sizeof(int) * (size_t)c->n_slots);
+  fR = (int *)malloc(sizeof(int) * (size_t)c->n_slots);
+  fd = (double *)malloc(sizeof(double) * (size_t)c->n_slots);
+  fc = (double *)malloc(sizeof(double) * (size_t)c->n_slots);
+  if (!nf || !fL || !fR || !fd || !fc) {
+    free(nf); free(fL); free(fR); free(fd); free(fc);
+    return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+  }
+  if (cudaMemcpy(nf, c->d.pair_nf + p->ann_base, sizeof(int) * (size_t)s->NR, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fL, c->d.fL, sizeof(int) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fR, c->d.fR, sizeof(int) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fd, c->d.fdphi, sizeof(double) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fc, c->d.fcm, sizeof(double) * (size_t)c->n_slots, cudaMemcpyDeviceToHost)) {
+    free(nf); free(fL); free(fR); free(fd); free(fc);
+    return fail(c, DGPU_ERR_CUDA, "face download failed");
+  }
+  for (i = 0; i < s->NR - 1; ++i) total += nf[i];
+  if (nf_out) *nf_out = total;
+  if (total > cap) {
+    free(nf); free(fL); free(fR); free(fd); free(fc);
+    return fail(c, DGPU_ERR_ARG, "face list has %d faces, capacity %d", total, cap);
+  }
+  {
+    int n = 0;
+    for (i = 0; i < s->NR - 1; ++i) {
+      const Annulus *A = &c->h_ann[p->ann_base + i];
+      const Annulus *B = &c->h_ann[p->ann_base + i + 1];
+      int f;
+      if (nri) nri[i] = n;
+      for (f = 0; f < nf[i]; ++f, ++n) {
+        int slot = A->face_base + f;
+        if (L) L[n] = A->cell_off - p->cell_base + fL[slot];
+        if (R) R[n] = B->cell_off - p->cell_base + fR[slot];
+        if (r) r[n] = A->f_r;
+        if (dphi) dphi[n] = fd[slot];
+        if (dA) dA[n] = A->f_r * fd[slot] * A->f_dperp;
+        if (deltaL) deltaL[n] = A->f_dl;
+        if (deltaR) deltaR[n] = A->f_dr;
+        if (cm) cm[n] = fc[slot];
+      }
+    }
+    if (nri) nri[s->NR - 1] = n;
+  }
+  free(nf); free(fL); free(fR); free(fd); free(fc);
+  return DGPU_OK;
+}
+
+int dgpu_torque(dgpu_ctx *c, int inst, double *torque) {
+  const DiskParams *p;
+  int rc = check_inst(c, inst), nb;
+  if (rc) return rc;
+  if (!torque) return fail(c, DGPU_ERR_ARG, "null torque");
+  p = &c->h_par[inst];
+  nb = (p->n_cells + 255) / 256;
+  CKK(dgk_torque(&c->d, inst, c->d_torque, c->d_torque + nb, p->n_cells, c->stream));
+  CK(cudaMemcpyAsync(torque, c->d_torque + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return dgpu_synchronize(c);
+}

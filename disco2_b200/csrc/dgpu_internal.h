@@ -1,0 +1,148 @@
+/*
+ * Internal data layout shared by the C host layer and the CUDA kernels.
+ *
+ * Cells of every disk in a context are numbered globally, disk after disk,
+ * each disk in the reference's (k, i, j) order (annulus-major: annulus i holds
+ * N_p[i] consecutive cells).  Per-cell variables are structure-of-arrays:
+ * variable q of cell g lives at X[q * n_cells + g].  Annulus-level constants
+ * (radii, frame terms, boundary profile) live in an Annulus table; the r-faces
+ * of the annulus pair (i, i+1) of a disk live in a slab of capacity
+ * N_p[i] + N_p[i+1] + DGPU_FACE_SLACK starting at Annulus.face_base.
+ */
+#ifndef DGPU_INTERNAL_H
+#define DGPU_INTERNAL_H
+
+#include <stdint.h>
+
+#define DGPU_NQ 5
+#define DGPU_FACE_SLACK 8
+#define DGPU_RUN_SLACK 8
+#define DGPU_WRAP_LIMIT 64
+
+/* enums of src/Headers/header.h:1-13 */
+enum { D_RHO, D_PPP, D_URR, D_UPP, D_UZZ };
+enum { D_DDD, D_TAU, D_SRR, D_LLL, D_SZZ };
+enum { DC_FIXED, DC_WCELL, DC_RIGID, DC_KEPLER, DC_OMEGA20, DC_MILOS, DC_POWERLAW };
+enum { DA_FIXED, DA_KEPLER, DA_OMEGA20, DA_MILOS, DA_POWERLAW };
+enum { DS_LEFT, DS_LEFTSTAR, DS_RIGHTSTAR, DS_RIGHT };
+enum { DB_FIXED, DB_OUTFLOW, DB_PERIODIC };
+enum { DI_SHEAR, DI_VORTEX, DI_SSTEST, DI_TORUS, DI_MILOS_MACFADYEN, DI_RAD_DOM, DI_MIDDLE,
+       DI_GRESHO, DI_KEPLER_RING, DI_CIRCUMBINARY };
+enum { DR_HLLC, DR_HLL };
+
+/* device error flags (bitwise) */
+#define DGPU_EF_FACE_OVERFLOW 1
+#define DGPU_EF_WRAP_LIMIT 2
+#define DGPU_EF_VISC_VZ 4
+#define DGPU_EF_RUN_OVERFLOW 8
+
+/* annulus kind bits */
+#define DGPU_AK_CFL 1        /* non-ghost: enters the CFL minimum (cell_mindt.c:38-42) */
+#define DGPU_AK_BC_FIXED 2   /* ghost annulus reset by the fixed radial boundary */
+#define DGPU_AK_DAMP 4       /* inside a damping zone (cell_misc.c:98-132) */
+#define DGPU_AK_SINK_SUM 8   /* counted in the Mdot sum (cell_source.c:80-88,181) */
+#define DGPU_AK_IC 16        /* boundary profile ic[] is defined for this annulus */
+
+/* Per-disk parameters (constant during a run). */
+typedef struct {
+  int NR;           /* annuli incl. ghosts, sim_N(R_DIR) */
+  int ann_base;     /* global index of annulus 0 */
+  int cell_base;    /* global index of cell 0 */
+  int n_cells;
+  int riemann;      /* DR_HLLC / DR_HLL */
+  int visc_const;
+  int has_visc;     /* EXPLICIT_VISCOSITY > 0 */
+  int w_numeric;
+  int w_analytic;
+  int grav2d;
+  int phi_order;
+  int rho_sink_on;
+  int cooling;
+  int init_type;
+  int has_damp;     /* DAMP_TIME > 0 */
+  int num_sinks;    /* GravMassType (cell_source.c:177) */
+  double gamma, plm, cfl, visc, g_eps;
+  double rho_floor, cs_floor, cs_cap, vel_cap;
+  double t_max, poro_r1, orb_tscale, orb_t0;
+  double dz, z;     /* z-extent and centre of the single z layer */
+} DiskParams;
+
+/* Per-annulus constants (host-computed with the host libm, like the reference). */
+typedef struct {
+  int inst;         /* owning disk */
+  int i;            /* annulus index within the disk */
+  int np;           /* N_p */
+  int cell_off;     /* global cell index of j = 0 */
+  int kind;         /* DGPU_AK_* bits */
+  int face_base;    /* r-faces of pair (i, i+1): slab start, capacity */
+  int face_cap;
+  int run_base;     /* run starts of pair (i, i+1): slab start, capacity */
+  int run_cap;
+  int pad;
+  double rm, rp, r; /* FacePos(i-1), FacePos(i), 0.5*(rp+rm) */
+  double dr;        /* rp - rm */
+  double dv_half;   /* .5*(rp*rp-rm*rm)   (cell_calc_cons dV factor) */
+  double dv_diff;   /* rp*rp-rm*rm          (cell_add_src dV factor)  */
+  double rom, rdrom, dtom; /* sim_rOm_a, sim_rdrOm_a, sim_dtOm_a at r (a = 1 tables; MILOS: device) */
+  double wnum;      /* wiph for the non-rigid w_numeric_type choices (cell_set_w.c:158-201) */
+  double ic[DGPU_NQ];/* single-cell initial data (boundary + damping target) */
+  double damp_rate; /* rate of cell_bc_damp (0 outside the zones) */
+  /* pair (i, i+1) constants (build_jloop, face_create_destroy.c:27-35) */
+  double f_r, f_dl, f_dr, f_dperp;
+  double f_rdrom;   /* sim_rdrOm_a at the face radius (riemann_visc_flux) */
+} Annulus;
+
+/* Per-disk dynamic state (device-resident, updated by the kernels). */
+typedef struct {
+  double t, dt;     /* time, dt of the current step */
+  double gr[2], gphi[2], gM[2], gom[2];         /* GravMass r, phi, M, omega */
+  double grk_r[2], grk_phi[2], grk_M[2], grk_om[2]; /* GravMass RK copies */
+  double mdot[2], macc[2];
+  unsigned long long dtkey;                      /* CFL minimum (bit pattern of a positive double) */
+  int pad[2];
+} InstState;
+
+/* Device pointers and sizes handed to every kernel. */
+typedef struct {
+  int n_inst, n_ann, n_cells, n_slots, n_runs;
+  const DiskParams *par;
+  InstState *ist;
+  const Annulus *ann;
+  const int *cell_ann;    /* cell -> global annulus */
+  const int *slot_ann;    /* face slot -> global annulus of its pair (or -1) */
+  double *prim, *cons, *rkcons, *grad, *gradp;
+  double *tiph0, *tiph1;  /* ping-pong raw phi edges */
+  double *tiphw;          /* phi edges wrapped into [0, 2pi] (cell_clean_pi) */
+  double *rktiph, *dphi;
+  double *w_ann;          /* wiph per annulus */
+  double *fphi;           /* [8][n_cells] phi-face increments, face (j, j+1) at cell j */
+  double *frf;            /* [8][n_slots] r-face increments */
+  int *fstart;            /* first r-face (within the pair slab) of each inner cell */
+  int *fL, *fR;           /* r-face cells (local j of inner / outer annulus) */
+  double *fdphi, *fcm;    /* r-face dphi and cm */
+  int *pair_nf, *pair_jpmin, *pair_T, *pair_seq; /* per annulus (pair i, i+1) */
+  int *runs;              /* run starts */
+  double *mdot_part;      /* [n_blocks_update][2] per-block sink sums */
+  unsigned int *counters; /* last-block counters */
+  int *err;               /* error flags */
+} DevPtrs;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* kernel launchers (dgpu_kernels.cu); return cudaError_t as int */
+int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream);
+int dgk_plm_r(const DevPtrs *d, int substep, void *stream);
+int dgk_flux(const DevPtrs *d, int substep, void *stream);
+int dgk_update(const DevPtrs *d, int substep, int stop, void *stream);
+int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
+int dgk_calc_cons(const DevPtrs *d, void *stream);
+int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
+int dgk_update_blocks(int n_cells);
+int dgk_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n, void *stream);
+int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa, int n, void *stream);
+#ifdef __cplusplus
+}
+#endif
+
+#endif

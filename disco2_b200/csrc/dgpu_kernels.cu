@@ -1,0 +1,1479 @@
+// sm_100a kernels of the moving-mesh finite-volume step.
+//
+// One RK substep is four launches:
+//   k_face    per annulus : cell_clean_pi, cell_plm_p, cell_set_w, GravMass
+//                           copy/clean_pi, and the r-face list of the annulus
+//                           pair (i, i+1) (build_jloop) as a checked parallel
+//                           merge of the two sorted phi-edge lists
+//   k_plm_r   per cell    : cell_plm_rz (face-weighted slope + limiter) and,
+//                           in substep 1, the CFL minimum (cell_mindt)
+//   k_flux    per face    : riemann_setup_p/_rz + riemann_AddFlux (HLL/HLLC in
+//                           the moving frame + viscous flux), stored as the
+//                           per-face increment dt*dA*F
+//   k_update  per cell    : gathers the face increments in the reference's
+//                           accumulation order, then cell_add_src,
+//                           cell_add_visc_src, cell_add_split_fictitious,
+//                           cell_update_phi/_dphi, cell_calc_prim, the fixed
+//                           radial boundary, cell_bc_damp and cell_calc_cons;
+//                           its last block advances the GravMass state.
+//
+// Built with -fmad=false: every expression keeps the reference's operation
+// order and rounding (double '/' and sqrt are IEEE-rounded on the GPU), so
+// paths without transcendentals reproduce the reference bit for bit.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "dgpu_internal.h"
+
+#define PHIMAX (2.0 * M_PI)
+#define BLK 256
+
+namespace {
+
+__device__ __forceinline__ void set_err(int *err, int flag) { atomicOr(err, flag); }
+
+// while(dp > PHIMAX) dp -= PHIMAX; while(dp < 0.0) dp += PHIMAX;  (bounded)
+__device__ __forceinline__ double wrap_pos(double dp, int *err) {
+  int it = 0;
+  while (dp > PHIMAX) {
+    dp -= PHIMAX;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
+  }
+  while (dp < 0.0) {
+    dp += PHIMAX;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
+  }
+  return dp;
+}
+// while(dp > PHIMAX/2.) dp -= PHIMAX; while(dp < -PHIMAX/2.) dp += PHIMAX;  (bounded)
+__device__ __forceinline__ double wrap_pm(double dp, int *err) {
+  int it = 0;
+  while (dp > PHIMAX / 2.) {
+    dp -= PHIMAX;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
+  }
+  while (dp < -PHIMAX / 2.) {
+    dp += PHIMAX;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
+  }
+  return dp;
+}
+
+// pow with the two exponents the reference's point-mass force uses exactly
+// (PHI_ORDER = 2: r^1 and r^2), whose correctly rounded values are x and x*x.
+__device__ __forceinline__ double dpow(double x, double y) {
+  if (y == 1.0) return x;
+  if (y == 2.0) return x * x;
+  return pow(x, y);
+}
+
+// sim_rOm_a / sim_rdrOm_a / sim_dtOm_a for A_MILOS (src/Sim/sim_w_a.c:8-72);
+// other frame types use the host-computed annulus tables.
+__device__ double milos_rom(double r, double a) {
+  const int n = 8;
+  return r * (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
+}
+__device__ double milos_rdrom(double r, double a) {
+  const int n = 8;
+  double Omega_a = (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
+  double arn = pow(a / r, n);
+  return ((-1.5 + n * arn / (1. + arn)) * Omega_a +
+          (1.5 - n) * pow(a / r, n - 1.5) / (1. + arn) * pow(r, -1.5));
+}
+__device__ double milos_dtom(double r, double a, double tau) {
+  const int n = 8;
+  double a0 = 1.0;
+  double dta_o_a = -.25 * pow(a / a0, -4) / tau;
+  double Omega_a = (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
+  double arn = pow(a / r, n);
+  if (a > 0.0) return (dta_o_a * (Omega_a * (-1.5 + n / (1. + arn)) + (1.5 - n) * pow(r, -1.5) / (1. + arn)));
+  return 0.0;
+}
+__device__ __forceinline__ double frame_rom(const DiskParams &P, double tab, double r, double a) {
+  return P.w_analytic == DA_MILOS ? milos_rom(r, a) : tab;
+}
+__device__ __forceinline__ double frame_rdrom(const DiskParams &P, double tab, double r, double a) {
+  return P.w_analytic == DA_MILOS ? milos_rdrom(r, a) : tab;
+}
+__device__ __forceinline__ double frame_dtom(const DiskParams &P, double tab, double r, double a) {
+  return P.w_analytic == DA_MILOS ? milos_dtom(r, a, P.orb_tscale) : tab;
+}
+
+// gravMass_dist (src/GravMass/GravMass_access.c:25-31) with (xbh, ybh) given.
+__device__ __forceinline__ double gm_dist(double xbh, double ybh, double r, double phi) {
+  double x = r * cos(phi);
+  double y = r * sin(phi);
+  double z = 0.;
+  return sqrt((x - xbh) * (x - xbh) + (y - ybh) * (y - ybh) + z * z);
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solver: riemann_set_vel / _set_state / _set_flux / _set_star_hll /
+// _set_star_hllc and the flux choice of riemann_AddFlux
+// (src/Riemann/Riemann_routines.c:14-191,314-371).  dir 0 = r face, 1 = phi.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void phys_flux(const double *p, double r, double n0, double n1, double n2,
+                                          double gam, double *F) {
+  double rho = p[D_RHO];
+  double Pp = p[D_PPP];
+  double vr = p[D_URR];
+  double vp = p[D_UPP] * r;
+  double vz = p[D_UZZ];
+  double vn = vr * n0 + vp * n1 + vz * n2;
+  double rhoe = Pp / (gam - 1.);
+  double v2 = vr * vr + vp * vp + vz * vz;
+  F[D_DDD] = rho * vn;
+  F[D_SRR] = rho * vr * vn + Pp * n0;
+  F[D_LLL] = r * (rho * vp * vn + Pp * n1);
+  F[D_SZZ] = rho * vz * vn + Pp * n2;
+  F[D_TAU] = (.5 * rho * v2 + rhoe + Pp) * vn;
+}
+// cell_prim2cons with dV = 1 (src/Cell/cell_conversion.c:11-33)
+__device__ __forceinline__ void prim2cons(const double *p, double *U, double r, double dV, double gam) {
+  double rho = p[D_RHO];
+  double Pp = p[D_PPP];
+  double vr = p[D_URR];
+  double vp = p[D_UPP] * r;
+  double vz = p[D_UZZ];
+  double v2 = vr * vr + vp * vp + vz * vz;
+  double rhoe = Pp / (gam - 1.);
+  U[D_DDD] = rho * dV;
+  U[D_SRR] = rho * vr * dV;
+  U[D_LLL] = r * rho * vp * dV;
+  U[D_SZZ] = rho * vz * dV;
+  U[D_TAU] = (.5 * rho * v2 + rhoe) * dV;
+}
+
+__device__ void riemann_flux(const double *pL, const double *pR, double r, int dir, double w, double gam,
+                             int solver, double *F) {
+  const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = 0.0;
+  double vnL, cf2L, vnR, cf2R;
+  {
+    double P = pL[D_PPP], rho = pL[D_RHO], vr = pL[D_URR], vp = r * pL[D_UPP], vz = pL[D_UZZ];
+    vnL = vr * n0 + vp * n1 + vz * n2;
+    cf2L = gam * (P / rho);
+  }
+  {
+    double P = pR[D_PPP], rho = pR[D_RHO], vr = pR[D_URR], vp = r * pR[D_UPP], vz = pR[D_UZZ];
+    vnR = vr * n0 + vp * n1 + vz * n2;
+    cf2R = gam * (P / rho);
+  }
+  double Sl = vnL - sqrt(cf2L);
+  double Sr = vnL + sqrt(cf2L);
+  if (Sl > vnR - sqrt(cf2R)) Sl = vnR - sqrt(cf2R);
+  if (Sr < vnR + sqrt(cf2R)) Sr = vnR + sqrt(cf2R);
+  double Ss = (pR[D_RHO] * vnR * (Sr - vnR) - pL[D_RHO] * vnL * (Sl - vnL) + pL[D_PPP] - pR[D_PPP]) /
+              (pR[D_RHO] * (Sr - vnR) - pL[D_RHO] * (Sl - vnL));
+  int state;
+  if (w < Sl) state = DS_LEFT;
+  else if (w > Sr) state = DS_RIGHT;
+  else if (w < Ss) state = DS_LEFTSTAR;
+  else state = DS_RIGHTSTAR;
+
+  double Fk[5], Uk[5];
+  if (state == DS_LEFT || state == DS_RIGHT) {
+    const double *p = state == DS_LEFT ? pL : pR;
+    phys_flux(p, r, n0, n1, n2, gam, Fk);
+    prim2cons(p, Uk, r, 1.0, gam);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) F[q] = Fk[q] - w * Uk[q];
+    return;
+  }
+  double Ustar[5], Fstar[5];
+  if (solver == DR_HLL) {
+    double FL[5], FR[5], UL[5], UR[5];
+    phys_flux(pL, r, n0, n1, n2, gam, FL);
+    phys_flux(pR, r, n0, n1, n2, gam, FR);
+    prim2cons(pL, UL, r, 1.0, gam);
+    prim2cons(pR, UR, r, 1.0, gam);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      Ustar[q] = (Sr * UR[q] - Sl * UL[q] + FL[q] - FR[q]) / (Sr - Sl);
+      Fstar[q] = (Sr * FL[q] - Sl * FR[q] - Sr * Sl * (UL[q] - UR[q])) / (Sr - Sl);
+    }
+  } else {
+    const double *prim = state == DS_LEFTSTAR ? pL : pR;
+    double Sk = state == DS_LEFTSTAR ? Sl : Sr;
+    phys_flux(prim, r, n0, n1, n2, gam, Fk);
+    prim2cons(prim, Uk, r, 1.0, gam);
+    double rho = prim[D_RHO];
+    double vr = prim[D_URR];
+    double vp = prim[D_UPP] * r;
+    double vz = prim[D_UZZ];
+    double Pp = prim[D_PPP];
+    double v2 = vr * vr + vp * vp + vz * vz;
+    double vn = vr * n0 + vp * n1 + vz * n2;
+    double rhoe = Pp / (gam - 1.);
+    double D = rho;
+    double mr = rho * vr;
+    double mp = rho * vp;
+    double mz = rho * vz;
+    double E_hydro = .5 * rho * v2 + rhoe;
+    double Ps = rho * (Sk - vn) * (Ss - vn) + Pp;
+    double Dstar = (Sk - vn) * D / (Sk - Ss);
+    double Msn = Dstar * Ss;
+    double Msr = (Sk - vn) * mr / (Sk - Ss);
+    double Msp = (Sk - vn) * mp / (Sk - Ss);
+    double Msz = (Sk - vn) * mz / (Sk - Ss);
+    double Estar = ((Sk - vn) * E_hydro + Ps * Ss - Pp * vn) / (Sk - Ss);
+    double mn = Msr * n0 + Msp * n1 + Msz * n2;
+    Msr += n0 * (Msn - mn);
+    Msp += n1 * (Msn - mn);
+    Msz += n2 * (Msn - mn);
+    Ustar[D_DDD] = Dstar;
+    Ustar[D_SRR] = Msr;
+    Ustar[D_LLL] = r * Msp;
+    Ustar[D_SZZ] = Msz;
+    Ustar[D_TAU] = Estar;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Fstar[q] = Fk[q] + Sk * (Ustar[q] - Uk[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) F[q] = Fstar[q] - w * Ustar[q];
+}
+
+// Inputs of riemann_visc_flux (src/Riemann/Riemann_routines.c:193-311).
+struct ViscIn {
+  const double *pL, *pR;        // reconstructed face states (primL, primR)
+  double cL[5], cR[5];          // cell prims
+  double gpL[5], gpR[5];        // cell gradp
+  double grL[5], grR[5];        // cell grad
+  double tL, tR, dL, dR;        // cell tiph (wrapped) and dphi
+  double r, cm, r_cell_L, r_cell_R;
+  double rdr_om;                // sim_rdrOm_a at r
+};
+
+__device__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const InstState &S,
+                          const double *gx, const double *gy, double *Fv, int *err) {
+  const double r = v.r;
+  double Avg[5], Gr[5], Gp[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    Avg[q] = .5 * (v.pL[q] + v.pR[q]);
+    Gp[q] = .5 * (v.gpL[q] + v.gpR[q]) / r;
+    Gr[q] = .5 * (v.grL[q] + v.grR[q]);
+  }
+  if (dir == 0) {
+    double pLc = v.tL - .5 * v.dL;
+    double pRc = v.tR - .5 * v.dR;
+    double dpL = v.cm - pLc;
+    double dpR = -v.cm + pRc;
+    dpL = wrap_pm(dpL, err);
+    dpR = wrap_pm(dpR, err);
+    double deltaL = v.r - v.r_cell_L;
+    double deltaR = v.r_cell_R - v.r;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double WL = v.cL[q] + dpL * v.gpL[q];
+      double WR = v.cR[q] - dpR * v.gpR[q];
+      Avg[q] = 0.5 * (WL + WR);
+      Gr[q] = (WR - WL) / (deltaR + deltaL);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      Avg[q] = 0.5 * (v.cR[q] + v.cL[q]);
+      Gp[q] = (v.cR[q] - v.cL[q]) / (v.tR - v.tL) / r;
+    }
+  }
+  double nu;
+  double alpha = P.visc;
+  if (P.visc_const == 1) {
+    nu = alpha;
+  } else if (P.init_type == DI_SHEAR) {
+    nu = alpha * P.gamma * Avg[D_PPP] / Avg[D_RHO] * dpow(fabs(r * cos(v.cm)), 2.0);
+    if (r * cos(v.cm) > 20.) nu = 0.0;
+  } else {
+    double d0 = gm_dist(gx[0], gy[0], r, v.cm);
+    double d1 = gm_dist(gx[1], gy[1], r, v.cm);
+    double eps = P.g_eps;
+    nu = alpha * Avg[D_PPP] / Avg[D_RHO] /
+         sqrt(pow(d0 * d0 + eps * eps, -1.5) * S.gM[0] + pow(d1 * d1 + eps * eps, -1.5) * S.gM[1]);
+  }
+  double rho = Avg[D_RHO];
+  double vr = Avg[D_URR];
+  double om = Avg[D_UPP];
+  double vz = Avg[D_UZZ];
+  if (fabs(vz) > 1.e-12) set_err(err, DGPU_EF_VISC_VZ);
+  double Gr_vr = Gr[D_URR], Gr_om = Gr[D_UPP];
+  double Gp_vr = Gp[D_URR], Gp_om = Gp[D_UPP];
+  double rdr = v.rdr_om;
+  if (dir == 0) {
+    Fv[0] = -nu * rho * (r * Gr_vr - vr - r * r * Gp_om);
+    Fv[1] = -nu * rho * (r * (r * Gr_om + rdr) + r * Gp_vr);
+    Fv[2] = -nu * rho * (vr * (Gr_vr - vr / r - r * Gp_om) + r * om * (Gp_vr + (rdr + r * Gr_om)));
+  } else {
+    Fv[0] = -nu * rho * (r * (r * Gr_om + rdr) + r * Gp_vr);
+    Fv[1] = -nu * rho * (-r * Gr_vr + vr + r * r * Gp_om);
+    Fv[2] = -nu * rho * (-r * om * (Gr_vr - vr / r - r * Gp_om) + vr * (Gp_vr + (rdr + r * Gr_om)));
+  }
+}
+
+__device__ __forceinline__ double ld(const double *p, int q, int n, int g) { return p[(size_t)q * n + g]; }
+
+// ---------------------------------------------------------------------------
+// r-face list of one annulus pair (build_jloop, face_create_destroy.c:22-128)
+// ---------------------------------------------------------------------------
+struct FaceCtx {
+  const double *tin, *din, *tout, *dout;
+  int Nin, Nout;
+  int *fL, *fR;
+  double *fdphi, *fcm;
+  int *runs;
+  int *fstart;  // fstart of the inner annulus cells (indexed by j)
+  int cap, rcap;
+  int *err;
+};
+
+// The body of the reference's j loop for inner cell j starting at outer cell
+// jp: emits its faces and advances jp.  n = running face number, s = running
+// count of jp advances (the run index of the next face).  FILL writes.
+template <bool FILL>
+__device__ void face_cell(const FaceCtx &c, int j, int &jp, int &n, int &s) {
+  int jm = j - 1;
+  if (jm < 0) jm = c.Nin - 1;
+  bool mark = false;
+  auto emit = [&](double dphi, double tp) {
+    if (FILL) {
+      if (n < c.cap) {
+        c.fL[n] = j;
+        c.fR[n] = jp;
+        c.fdphi[n] = dphi;
+        c.fcm[n] = tp - .5 * dphi;
+      }
+      if (mark && s < c.rcap) c.runs[s] = n;
+    }
+    mark = false;
+    ++n;
+  };
+  auto advance = [&]() {
+    ++jp;
+    if (jp == c.Nout) jp = 0;
+    ++s;
+    mark = true;
+  };
+  if (FILL) c.fstart[j] = n;
+  double dp = c.tout[jp] - c.tin[jm];
+  dp = wrap_pos(dp, c.err);
+  if (c.din[j] < dp) {
+    emit(c.din[j], c.tin[j]);
+    return;
+  }
+  emit(dp, c.tout[jp]);
+  advance();
+  dp = c.tin[j] - c.tout[jp];
+  dp = wrap_pm(dp, c.err);
+  int guard = 0;
+  while (dp > 0.0) {
+    emit(c.dout[jp], c.tout[jp]);
+    advance();
+    dp = c.tin[j] - c.tout[jp];
+    dp = wrap_pm(dp, c.err);
+    if (++guard > c.Nout + 2) {
+      set_err(c.err, DGPU_EF_FACE_OVERFLOW);
+      break;
+    }
+  }
+  dp = c.dout[jp] + dp;
+  emit(dp, c.tin[j]);
+}
+
+template <typename T>
+__device__ T block_excl_scan(T v, T *sh, T &total) {
+  // Hillis-Steele over one value per thread (blockDim.x <= 1024)
+  int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int o = 1; o < blockDim.x; o <<= 1) {
+    T x = t >= o ? sh[t - o] : T(0);
+    __syncthreads();
+    sh[t] += x;
+    __syncthreads();
+  }
+  T incl = sh[t];
+  total = sh[blockDim.x - 1];
+  __syncthreads();
+  return incl - v;
+}
+
+__global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops) {
+  __shared__ int sh_i[BLK];
+  __shared__ int sh_j[BLK];
+  __shared__ double sh_v[BLK];
+  __shared__ int sh_flag;
+  const int a = blockIdx.x;
+  const Annulus A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int np = A.np, off = A.cell_off;
+  const int N = d.n_cells;
+
+  // cell_clean_pi (src/Cell/cell_misc.c:12-26)
+  for (int j = tid; j < np; j += nt) d.tiphw[off + j] = wrap_pos(traw[off + j], d.err);
+
+  // cell_plm_p (src/Cell/cell_plm.c:116-161)
+  for (int j = tid; j < np; j += nt) {
+    int g = off + j;
+    int gl = j == 0 ? off + np - 1 : g - 1;
+    int gr = j == np - 1 ? off : g + 1;
+    double dpL = .5 * (d.dphi[g] + d.dphi[gl]);
+    double dpR = .5 * (d.dphi[g] + d.dphi[gr]);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double pc = ld(d.prim, q, N, g), pl = ld(d.prim, q, N, gl), pr = ld(d.prim, q, N, gr);
+      double sL = (pc - pl) / dpL;
+      double sR = (pr - pc) / dpR;
+      double sM = (pr - pl) / (dpL + dpR);
+      double s = P.plm * sL;
+      if (fabs(s) > P.plm * fabs(sR)) s = P.plm * sR;
+      if (fabs(s) > fabs(sM)) s = sM;
+      if (sL * sR < 0.0) s = 0.0;
+      d.gradp[(size_t)q * N + g] = s;
+    }
+  }
+
+  // cell_clear_w + cell_set_w (src/Cell/cell_set_w.c:12-102): one value per annulus
+  if (tid == 0) {
+    if (P.w_numeric == DC_RIGID) {
+      double w = 0.0, Mring = 0.0;
+      for (int j = 0; j < np; ++j) {
+        double vp = A.r * ld(d.prim, D_UPP, N, off + j);
+        double m = ld(d.cons, D_DDD, N, off + j);
+        Mring += m;
+        w += vp * m;
+      }
+      d.w_ann[a] = w / Mring;
+    } else {
+      d.w_ann[a] = A.wnum;
+    }
+  }
+
+  // GravMass: gravMass_copy at the start of a step, then gravMass_clean_pi
+  if (gm_ops && A.i == 0 && tid == 0) {
+    InstState &S = d.ist[A.inst];
+    if (substep == 1) {
+      for (int p = 0; p < 2; ++p) {
+        S.grk_r[p] = S.gr[p];
+        S.grk_phi[p] = S.gphi[p];
+        S.grk_M[p] = S.gM[p];
+        S.grk_om[p] = S.gom[p];
+      }
+      S.dtkey = (unsigned long long)__double_as_longlong(1.e100);
+    }
+    for (int p = 0; p < 2; ++p) {
+      double phi = S.gphi[p];
+      while (phi > 2. * M_PI) phi -= 2. * M_PI;
+      while (phi < 0.0) phi += 2. * M_PI;
+      S.gphi[p] = phi;
+    }
+  }
+
+  if (A.i >= P.NR - 1) return;
+
+  // ---- r faces of the pair (a, a+1) ----
+  const Annulus B = d.ann[a + 1];
+  FaceCtx c;
+  c.tin = traw + off;
+  c.din = d.dphi + off;
+  c.tout = traw + B.cell_off;
+  c.dout = d.dphi + B.cell_off;
+  c.Nin = np;
+  c.Nout = B.np;
+  c.fL = d.fL + A.face_base;
+  c.fR = d.fR + A.face_base;
+  c.fdphi = d.fdphi + A.face_base;
+  c.fcm = d.fcm + A.face_base;
+  c.runs = d.runs + A.run_base;
+  c.fstart = d.fstart + off;
+  c.cap = A.face_cap;
+  c.rcap = A.run_cap;
+  c.err = d.err;
+  const double p0 = c.tin[np - 1];
+
+  // jpmin: first outer cell with the smallest wrap(tiph - p0), start (PHIMAX, 0)
+  {
+    double bv = PHIMAX;
+    int bi = 0;
+    for (int jp = tid; jp < c.Nout; jp += nt) {
+      double dp = wrap_pos(c.tout[jp] - p0, d.err);
+      if (dp < bv || (dp == bv && jp < bi)) {
+        bv = dp;
+        bi = jp;
+      }
+    }
+    sh_v[tid] = bv;
+    sh_i[tid] = bi;
+    __syncthreads();
+    for (int o = nt / 2; o > 0; o >>= 1) {
+      if (tid < o) {
+        double v2 = sh_v[tid + o];
+        int i2 = sh_i[tid + o];
+        if (v2 < sh_v[tid] || (v2 == sh_v[tid] && i2 < sh_i[tid])) {
+          sh_v[tid] = v2;
+          sh_i[tid] = i2;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const int jpmin = sh_i[0];
+  __syncthreads();
+
+  // contiguous chunk of inner cells per thread; speculative start outer cell
+  const int chunk = (np + nt - 1) / nt;
+  const int j0 = min(np, tid * chunk), j1 = min(np, j0 + chunk);
+  int jp_start = jpmin;
+  if (j0 > 0 && j0 < np) {
+    // lower bound of the left edge of inner cell j0 among the outer edges,
+    // both measured as wrap(edge - p0); verified below
+    double L = wrap_pos(c.tin[j0 - 1] - p0, d.err);
+    int lo = 0, hi = c.Nout;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      int k = jpmin + mid;
+      if (k >= c.Nout) k -= c.Nout;
+      double e = wrap_pos(c.tout[k] - p0, d.err);
+      if (e < L) lo = mid + 1;
+      else hi = mid;
+    }
+    jp_start = jpmin + lo;
+    if (jp_start >= c.Nout) jp_start -= c.Nout;
+  }
+  int cnt = 0, steps = 0, jp = jp_start;
+  {
+    int n = 0, s = 0;
+    for (int j = j0; j < j1; ++j) face_cell<false>(c, j, jp, n, s);
+    cnt = n;
+    steps = s;
+  }
+  if (tid == 0) sh_flag = 0;
+  sh_j[tid] = (j0 < j1) ? jp_start : -1;
+  __syncthreads();
+  if (j0 < j1 && tid + 1 < nt && sh_j[tid + 1] >= 0 && sh_j[tid + 1] != jp) sh_flag = 1;
+  __syncthreads();
+  const bool sequential = sh_flag != 0;
+
+  if (!sequential) {
+    int ntot, stot;
+    int fo = block_excl_scan<int>(cnt, sh_i, ntot);
+    int so = block_excl_scan<int>(steps, sh_j, stot);
+    if (ntot > c.cap || stot + 2 > c.rcap) {
+      if (tid == 0) {
+        set_err(d.err, DGPU_EF_FACE_OVERFLOW);
+        d.pair_nf[a] = 0;
+        d.pair_T[a] = 0;
+      }
+      return;
+    }
+    int n = fo, s = so;
+    jp = jp_start;
+    for (int j = j0; j < j1; ++j) face_cell<true>(c, j, jp, n, s);
+    if (tid == 0) {
+      c.runs[0] = 0;
+      c.runs[stot + 1] = ntot;
+      d.pair_nf[a] = ntot;
+      d.pair_jpmin[a] = jpmin;
+      d.pair_T[a] = stot;
+      d.pair_seq[a] = 0;
+    }
+  } else if (tid == 0) {
+    // exact sequential replay of build_jloop from jpmin
+    int n = 0, s = 0;
+    jp = jpmin;
+    for (int j = 0; j < np; ++j) face_cell<true>(c, j, jp, n, s);
+    if (n > c.cap || s + 2 > c.rcap) {
+      set_err(d.err, DGPU_EF_FACE_OVERFLOW);
+      d.pair_nf[a] = 0;
+      d.pair_T[a] = 0;
+      return;
+    }
+    c.runs[0] = 0;
+    c.runs[s + 1] = n;
+    d.pair_nf[a] = n;
+    d.pair_jpmin[a] = jpmin;
+    d.pair_T[a] = s;
+    d.pair_seq[a] = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cell_plm_rz (src/Cell/cell_plm.c:13-114) per cell + CFL (cell_mindt.c:32-100)
+// ---------------------------------------------------------------------------
+struct RFace {
+  int cL, cR;
+  double dphi, cm;
+  double r, dl, dr, dperp;
+};
+
+// Calls f(face) for every r face of cell g in the reference's face order:
+// first the faces of pair (i-1, i) where g is the outer cell, then the faces
+// of pair (i, i+1) where g is the inner cell.
+template <typename Fn>
+__device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus &A, int a, int g, int NR,
+                                                Fn f) {
+  const int j = g - A.cell_off;
+  if (A.i > 0) {
+    const Annulus &Q = d.ann[a - 1];
+    const int nf = d.pair_nf[a - 1];
+    const int T = d.pair_T[a - 1];
+    const int jpmin = d.pair_jpmin[a - 1];
+    if (nf > 0) {
+      int dd = j - jpmin;
+      if (dd < 0) dd += A.np;
+      const int *runs = d.runs + Q.run_base;
+      for (int s = dd; s <= T; s += A.np) {
+        int n0 = runs[s], n1 = runs[s + 1];
+        for (int n = n0; n < n1; ++n) {
+          RFace F;
+          F.cL = Q.cell_off + d.fL[Q.face_base + n];
+          F.cR = g;
+          F.dphi = d.fdphi[Q.face_base + n];
+          F.cm = d.fcm[Q.face_base + n];
+          F.r = Q.f_r;
+          F.dl = Q.f_dl;
+          F.dr = Q.f_dr;
+          F.dperp = Q.f_dperp;
+          f(F, Q.face_base + n, 1);
+        }
+      }
+    }
+  }
+  if (A.i < NR - 1) {
+    const int nf = d.pair_nf[a];
+    const Annulus &B = d.ann[a + 1];
+    int n0 = d.fstart[g];
+    int n1 = (j + 1 < A.np) ? d.fstart[g + 1] : nf;
+    if (nf <= 0) n1 = n0;
+    for (int n = n0; n < n1; ++n) {
+      RFace F;
+      F.cL = g;
+      F.cR = B.cell_off + d.fR[A.face_base + n];
+      F.dphi = d.fdphi[A.face_base + n];
+      F.cm = d.fcm[A.face_base + n];
+      F.r = A.f_r;
+      F.dl = A.f_dl;
+      F.dr = A.f_dr;
+      F.dperp = A.f_dperp;
+      f(F, A.face_base + n, 0);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  unsigned long long key = ~0ull;
+  int inst = -1;
+  if (g < N) {
+    const int a = d.cell_ann[g];
+    const Annulus A = d.ann[a];
+    const DiskParams &P = d.par[A.inst];
+    inst = A.inst;
+    double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    auto slopes = [&](const RFace &F, double *S) {
+      double pL = d.tiphw[F.cL] - .5 * d.dphi[F.cL];
+      double pR = d.tiphw[F.cR] - .5 * d.dphi[F.cR];
+      double dpL = F.cm - pL;
+      dpL = wrap_pm(dpL, d.err);
+      double dpR = pR - F.cm;
+      dpR = wrap_pm(dpR, d.err);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        double WL = ld(d.prim, q, N, F.cL) + dpL * ld(d.gradp, q, N, F.cL);
+        double WR = ld(d.prim, q, N, F.cR) - dpR * ld(d.gradp, q, N, F.cR);
+        S[q] = (WR - WL) / (F.dr + F.dl);
+      }
+    };
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int) {
+      double S[5];
+      slopes(F, S);
+      double dA = F.r * F.dphi * F.dperp;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) gq[q] += S[q] * dA;
+    });
+    {
+      double dz = P.dz, dp = d.dphi[g], dAtot;
+      if (A.i == 0) dAtot = dz * A.rp * dp;
+      else if (A.i == P.NR - 1) dAtot = dz * A.rm * dp;
+      else dAtot = dz * (A.rp + A.rm) * dp;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) gq[q] /= dAtot;
+    }
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int) {
+      double S[5];
+      slopes(F, S);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        if (S[q] * gq[q] < 0.0) gq[q] = 0.0;
+        else if (fabs(P.plm * S[q]) < fabs(gq[q])) gq[q] = P.plm * S[q];
+      }
+    });
+#pragma unroll
+    for (int q = 0; q < 5; ++q) d.grad[(size_t)q * N + g] = gq[q];
+
+    // CFL candidate (cell_mindt), substep 1 only, non-ghost annuli
+    if (substep == 1 && (A.kind & DGPU_AK_CFL)) {
+      const InstState &S = d.ist[A.inst];
+      const double *traw = d.tiph0;
+      double w = .5 * (d.w_ann[a] + d.w_ann[a]);
+      double dr = A.rp - A.rm;
+      double r = .5 * (A.rp + A.rm);
+      double dx = dr;
+      double rdphi = .5 * (A.rp + A.rm) * d.dphi[g];
+      if (rdphi < dr) dx = rdphi;
+      if (dx > P.dz) dx = P.dz;
+      double Pp = ld(d.prim, D_PPP, N, g), rho = ld(d.prim, D_RHO, N, g);
+      double vp = ld(d.prim, D_UPP, N, g) * r - w;
+      double vr = ld(d.prim, D_URR, N, g), vz = ld(d.prim, D_UZZ, N, g);
+      double cs = sqrt(P.gamma * Pp / rho);
+      double cf2 = cs * cs;
+      double maxv = sqrt(cf2) + sqrt(vr * vr + vp * vp + vz * vz);
+      double dt = P.cfl * dx / maxv;
+      if (P.has_visc) {
+        double nu;
+        if (P.visc_const == 1) {
+          nu = P.visc;
+        } else {
+          double tc = traw[g] - 0.5 * d.dphi[g];
+          if (P.init_type == DI_SHEAR) {
+            nu = P.visc * P.gamma * Pp / rho * dpow(fabs(r * cos(tc)), 2.0);
+            if (r * cos(tc) > 20.) nu = 0.000000001;
+          } else {
+            double xb0 = S.grk_r[0] * cos(S.grk_phi[0]), yb0 = S.grk_r[0] * sin(S.grk_phi[0]);
+            double xb1 = S.grk_r[1] * cos(S.grk_phi[1]), yb1 = S.grk_r[1] * sin(S.grk_phi[1]);
+            double d0 = gm_dist(xb0, yb0, r, tc);
+            double d1 = gm_dist(xb1, yb1, r, tc);
+            double eps = P.g_eps;
+            nu = P.visc * Pp / rho /
+                 sqrt(pow(d0 * d0 + eps * eps, -1.5) * S.grk_M[0] + pow(d1 * d1 + eps * eps, -1.5) * S.grk_M[1]);
+          }
+        }
+        double dt_visc = .25 * dx * dx / nu;
+        dt = dt / (1. + dt / dt_visc);
+      }
+      key = (unsigned long long)__double_as_longlong(dt);
+      if (__longlong_as_double((long long)key) < 0.0 || dt != dt) key = ~0ull;
+    }
+  }
+  if (substep != 1) return;
+
+  // minimum per disk: warp reduction when the warp holds one disk
+  const unsigned full = 0xffffffffu;
+  int inst0 = __shfl_sync(full, inst, 0);
+  bool uniform = __all_sync(full, inst == inst0);
+  if (uniform) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long k2 = __shfl_down_sync(full, key, o);
+      key = k2 < key ? k2 : key;
+    }
+    if ((threadIdx.x & 31) == 0 && inst0 >= 0 && key != ~0ull) atomicMin(&d.ist[inst0].dtkey, key);
+  } else if (inst >= 0 && key != ~0ull) {
+    atomicMin(&d.ist[inst].dtkey, key);
+  }
+
+  // last block: dt = min, clipped to Time_Max (timestep_set_dt, timestep_set.c:16-21)
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&d.counters[0], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
+    InstState &S = d.ist[k];
+    unsigned long long kk = atomicOr(&S.dtkey, 0ull);
+    double dt = __longlong_as_double((long long)kk);
+    if (S.t + dt > d.par[k].t_max) dt = d.par[k].t_max - S.t;
+    S.dt = dt;
+  }
+  if (threadIdx.x == 0) d.counters[0] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Face increments: one thread per phi face (at its left cell) and per r-face slot
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  if (t < N) {
+    // phi face (j, j+1): riemann_setup_p (Riemann_setup.c:46-80)
+    const int g = t;
+    const int a = d.cell_ann[g];
+    const Annulus A = d.ann[a];
+    const DiskParams &P = d.par[A.inst];
+    const InstState &S = d.ist[A.inst];
+    const int j = g - A.cell_off;
+    const int cL = g, cR = (j == A.np - 1) ? A.cell_off : g + 1;
+    const double dpL = d.dphi[cL], dpR = d.dphi[cR];
+    const double dz = P.dz;
+    const double dr = A.rp - A.rm;
+    const double r = .5 * (A.rp + A.rm);
+    const double dA = dr * dz;
+    double pL[5], pR[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      pL[q] = ld(d.prim, q, N, cL) + 0.5 * ld(d.gradp, q, N, cL) * dpL;
+      pR[q] = ld(d.prim, q, N, cR) - 0.5 * ld(d.gradp, q, N, cR) * dpR;
+    }
+    const double w = d.w_ann[a];
+    double F[5];
+    riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F);
+    const double dt = fac * S.dt;
+    const double k = dt * dA;
+    double *out = d.fphi;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) out[(size_t)q * N + g] = k * F[q];
+    if (P.has_visc) {
+      ViscIn v;
+      v.pL = pL;
+      v.pR = pR;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        v.cL[q] = ld(d.prim, q, N, cL);
+        v.cR[q] = ld(d.prim, q, N, cR);
+        v.gpL[q] = ld(d.gradp, q, N, cL);
+        v.gpR[q] = ld(d.gradp, q, N, cR);
+        v.grL[q] = ld(d.grad, q, N, cL);
+        v.grR[q] = ld(d.grad, q, N, cR);
+      }
+      v.tL = d.tiphw[cL];
+      v.tR = d.tiphw[cR];
+      v.dL = dpL;
+      v.dR = dpR;
+      v.r = r;
+      v.cm = d.tiphw[cL];
+      v.r_cell_L = r;
+      v.r_cell_R = r;
+      double a_sep = S.gr[0] + S.gr[1];
+      v.rdr_om = frame_rdrom(P, A.rdrom, r, a_sep);
+      double gx[2], gy[2];
+      for (int p = 0; p < 2; ++p) {
+        gx[p] = S.gr[p] * cos(S.gphi[p]);
+        gy[p] = S.gr[p] * sin(S.gphi[p]);
+      }
+      double Fv[3];
+      visc_flux(v, 1, P, S, gx, gy, Fv, d.err);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * N + g] = k * Fv[q];
+    }
+    return;
+  }
+  const int slot = t - N;
+  if (slot >= d.n_slots) return;
+  const int a = d.slot_ann[slot];
+  if (a < 0) return;
+  const Annulus A = d.ann[a];
+  const int n = slot - A.face_base;
+  if (n >= d.pair_nf[a]) return;
+  // r face: riemann_setup_rz (Riemann_setup.c:11-44)
+  const DiskParams &P = d.par[A.inst];
+  const InstState &S = d.ist[A.inst];
+  const Annulus &B = d.ann[a + 1];
+  const int cL = A.cell_off + d.fL[slot];
+  const int cR = B.cell_off + d.fR[slot];
+  const double fdphi = d.fdphi[slot], cm = d.fcm[slot];
+  const double deltaL = A.f_dl, deltaR = A.f_dr;
+  double pLc = d.tiphw[cL] - .5 * d.dphi[cL];
+  double pRc = d.tiphw[cR] - .5 * d.dphi[cR];
+  double dpL = cm - pLc;
+  double dpR = -cm + pRc;
+  dpL = wrap_pm(dpL, d.err);
+  dpR = wrap_pm(dpR, d.err);
+  const double r = A.f_r;
+  const double dA = r * fdphi * A.f_dperp;
+  const double r_cell_L = r - deltaL;
+  const double r_cell_R = r + deltaR;
+  double pL[5], pR[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    pL[q] = ld(d.prim, q, N, cL) + ld(d.grad, q, N, cL) * deltaL + ld(d.gradp, q, N, cL) * dpL;
+    pR[q] = ld(d.prim, q, N, cR) - ld(d.grad, q, N, cR) * deltaR - ld(d.gradp, q, N, cR) * dpR;
+  }
+  double F[5];
+  riemann_flux(pL, pR, r, 0, 0.0, P.gamma, P.riemann, F);
+  const double dt = fac * S.dt;
+  const double k = dt * dA;
+  const int NS = d.n_slots;
+  double *out = d.frf;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) out[(size_t)q * NS + slot] = k * F[q];
+  if (P.has_visc) {
+    ViscIn v;
+    v.pL = pL;
+    v.pR = pR;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      v.cL[q] = ld(d.prim, q, N, cL);
+      v.cR[q] = ld(d.prim, q, N, cR);
+      v.gpL[q] = ld(d.gradp, q, N, cL);
+      v.gpR[q] = ld(d.gradp, q, N, cR);
+      v.grL[q] = ld(d.grad, q, N, cL);
+      v.grR[q] = ld(d.grad, q, N, cR);
+    }
+    v.tL = d.tiphw[cL];
+    v.tR = d.tiphw[cR];
+    v.dL = d.dphi[cL];
+    v.dR = d.dphi[cR];
+    v.r = r;
+    v.cm = cm;
+    v.r_cell_L = r_cell_L;
+    v.r_cell_R = r_cell_R;
+    double a_sep = S.gr[0] + S.gr[1];
+    v.rdr_om = frame_rdrom(P, A.f_rdrom, r, a_sep);
+    double gx[2], gy[2];
+    for (int p = 0; p < 2; ++p) {
+      gx[p] = S.gr[p] * cos(S.gphi[p]);
+      gy[p] = S.gr[p] * sin(S.gphi[p]);
+    }
+    double Fv[3];
+    visc_flux(v, 0, P, S, gx, gy, Fv, d.err);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * NS + slot] = k * Fv[q];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-cell update: flux gather + sources + mesh motion + prim/cons + BC + damping
+// ---------------------------------------------------------------------------
+// fgrav (src/Cell/cell_source.c:11-13)
+__device__ __forceinline__ double fgrav(double M, double r, double eps, int n) {
+  return (M * dpow(r, n - 1.) / pow(dpow(r, n) + dpow(eps, n), 1. + 1. / n));
+}
+
+// Advanced phi edge of a cell (cell_update_phi, src/Cell/cell_misc.c:59-79).
+__device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, double w_total, double dt, double r) {
+  while (tw - rk > PHIMAX / 2.) rk += PHIMAX;
+  while (tw - rk < -PHIMAX / 2.) rk -= PHIMAX;
+  double t = (1.0 - RK) * tw + RK * rk;
+  t += w_total * dt / r;
+  return t;
+}
+
+__global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop, int tail) {
+  __shared__ double sh_md[2][BLK / 32];
+  __shared__ bool last;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double RK = substep == 1 ? 0.0 : 0.5;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  double md0 = 0.0, md1 = 0.0;
+  if (g < N) {
+    const int a = d.cell_ann[g];
+    const Annulus A = d.ann[a];
+    const DiskParams &P = d.par[A.inst];
+    const InstState &S = d.ist[A.inst];
+    const int j = g - A.cell_off;
+    const int np = A.np;
+    const double dt = fac * S.dt;
+    double c[5];
+    // cell_copy (substep 1) + cell_adjust_RK_cons (cell_misc.c:28-57)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      double cq = ld(d.cons, q, N, g);
+      double rk;
+      if (substep == 1) {
+        rk = cq;
+        d.rkcons[(size_t)q * N + g] = cq;
+      } else {
+        rk = ld(d.rkcons, q, N, g);
+      }
+      c[q] = (1.0 - RK) * cq + RK * rk;
+    }
+    bool done = stop <= 1;
+    // phi faces: for j = 0 the face (0,1) comes before (N-1,0)
+    if (!done) {
+      const int gl = j == 0 ? A.cell_off + np - 1 : g - 1;
+      const double r = .5 * (A.rp + A.rm);
+      auto addL = [&](int f) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) c[q] -= ld(d.fphi, q, N, f);
+        if (P.has_visc) {
+          c[D_SRR] -= ld(d.fphi, 5, N, f) / r;
+          c[D_LLL] -= ld(d.fphi, 6, N, f);
+          c[D_TAU] -= ld(d.fphi, 7, N, f);
+        }
+      };
+      auto addR = [&](int f) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) c[q] += ld(d.fphi, q, N, f);
+        if (P.has_visc) {
+          c[D_SRR] += ld(d.fphi, 5, N, f) / r;
+          c[D_LLL] += ld(d.fphi, 6, N, f);
+          c[D_TAU] += ld(d.fphi, 7, N, f);
+        }
+      };
+      if (j == 0) {
+        addL(g);
+        addR(gl);
+      } else {
+        addR(gl);
+        addL(g);
+      }
+      done = stop == 2;
+    }
+    // r faces in face-list order
+    if (!done) {
+      const int NS = d.n_slots;
+      for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int asR) {
+        if (asR) {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) c[q] += ld(d.frf, q, NS, slot);
+          if (P.has_visc) {
+            double rR = F.r + F.dr;
+            c[D_SRR] += ld(d.frf, 5, NS, slot) / rR;
+            c[D_LLL] += ld(d.frf, 6, NS, slot);
+            c[D_TAU] += ld(d.frf, 7, NS, slot);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) c[q] -= ld(d.frf, q, NS, slot);
+          if (P.has_visc) {
+            double rL = F.r - F.dl;
+            c[D_SRR] -= ld(d.frf, 5, NS, slot) / rL;
+            c[D_LLL] -= ld(d.frf, 6, NS, slot);
+            c[D_TAU] -= ld(d.frf, 7, NS, slot);
+          }
+        }
+      });
+      done = stop == 3;
+    }
+    const double tw = d.tiphw[g];
+    const double dphi = d.dphi[g];
+    const double rm = A.rm, rp = A.rp;
+    const double a_sep = S.gr[0] + S.gr[1];
+    if (!done) {
+      // cell_add_src (src/Cell/cell_source.c:73-214)
+      double phi = tw - .5 * dphi;
+      double rho = ld(d.prim, D_RHO, N, g);
+      double Pp = ld(d.prim, D_PPP, N, g);
+      double r = .5 * (rp + rm);
+      double vr = ld(d.prim, D_URR, N, g);
+      double vz = ld(d.prim, D_UZZ, N, g);
+      double vp = ld(d.prim, D_UPP, N, g) * r;
+      double dz = P.dz;
+      double dV = dphi * .5 * A.dv_diff * dz;
+      double cosp = cos(phi), sinp = sin(phi);
+      double xpos = r * cosp;
+      double ypos = r * sinp;
+      double z = P.z;
+      double R = sqrt(r * r + z * z);
+      double sint, cost, gravdist;
+      if (P.grav2d == 1) {
+        sint = 1.0;
+        cost = 0.0;
+        gravdist = r;
+      } else {
+        sint = r / R;
+        cost = z / R;
+        gravdist = R;
+      }
+      double Fr = 0.0, Fp = 0.0;
+      double xb[2], yb[2];
+      for (int p = 0; p < 2; ++p) {
+        double cpp = cos(S.gphi[p]), spp = sin(S.gphi[p]);
+        xb[p] = S.gr[p] * cpp;
+        yb[p] = S.gr[p] * spp;
+        // gravMassForce (src/Cell/cell_source.c:49-71)
+        double dx = gravdist * cosp - S.gr[p] * cpp;
+        double dy = gravdist * sinp - S.gr[p] * spp;
+        double script_r = sqrt(dx * dx + dy * dy);
+        double cosa = dx / script_r;
+        double sina = dy / script_r;
+        double cosap = cosa * cosp + sina * sinp;
+        double sinap = sina * cosp - cosa * sinp;
+        double f1 = -fgrav(S.gM[p], script_r, P.g_eps, P.phi_order);
+        Fr += cosap * f1;
+        Fp += sinap * f1;
+      }
+      double w_a = frame_rom(P, A.rom, r, a_sep);
+      double rdrOm_a = frame_rdrom(P, A.rdrom, r, a_sep);
+      double F_centrifugal_r = w_a * w_a / r;
+      double dtOm_a = frame_dtom(P, A.dtom, r, a_sep);
+      double F_euler_phi = -(r * dtOm_a + vr * rdrOm_a);
+      c[D_SRR] += dt * dV * (rho * vp * vp + Pp) / r;
+      c[D_SRR] += dt * dV * rho * (Fr * sint + F_centrifugal_r);
+      c[D_LLL] += dt * dV * rho * (Fp - r * dtOm_a) * r;
+      c[D_SZZ] += dt * dV * rho * Fr * cost;
+      c[D_TAU] += dt * dV * rho * ((Fr * sint + F_centrifugal_r) * vr + Fr * vz * cost + (Fp + F_euler_phi) * vp);
+      if (P.rho_sink_on == 1) {
+        // get_rho_sink (src/Cell/cell_source.c:15-47)
+        double r0 = sqrt((xpos - xb[0]) * (xpos - xb[0]) + (ypos - yb[0]) * (ypos - yb[0]));
+        double r1 = sqrt((xpos - xb[1]) * (xpos - xb[1]) + (ypos - yb[1]) * (ypos - yb[1]));
+        double M0 = S.gM[0], M1 = S.gM[1];
+        double Mtotal = M0 + M1;
+        double alpha = P.visc;
+        double one_o_nu = 1.0 / (alpha * Pp / rho) * sqrt(pow(r0, -3) * M0 / Mtotal + pow(r1, -3) * M1 / Mtotal);
+        double t_visc0 = 1.0 * 2. / 3. * r0 * r0 * one_o_nu;
+        double t_visc1 = 1.0 * 2. / 3. * r1 * r1 * one_o_nu;
+        if (t_visc0 < 10. * dt) t_visc0 = 10. * dt;
+        if (t_visc1 < 10. * dt) t_visc1 = 10. * dt;
+        double sink_size = 0.5;
+        for (int p = 0; p < P.num_sinks && p < 2; ++p) {
+          double drho = 0.0;
+          if (p == 0) { if (r0 < sink_size) drho = rho / t_visc0; }
+          else { if (r1 < sink_size) drho = rho / t_visc1; }
+          c[D_DDD] -= drho * dt * dV;
+          if (A.kind & DGPU_AK_SINK_SUM) {
+            if (p == 0) md0 += drho * dV;
+            else md1 += drho * dV;
+          }
+        }
+      }
+      if (P.cooling == 1) {
+        if (P.init_type == DI_SHEAR) {
+          double cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
+          if (cooling_term < 0.0) cooling_term = 0.0;
+          c[D_TAU] -= cooling_term * dt;
+        } else {
+          double numfac = 1.0;
+          double alpha = P.visc;
+          double cooling_cap = c[D_TAU] * numfac;
+          double cooling_term = 9. / 4. * alpha * pow(P.poro_r1, -3) / rho * pow(Pp / rho, 4.) * dt * dV;
+          if (cooling_term > cooling_cap) cooling_term = cooling_cap;
+          c[D_TAU] -= cooling_term;
+        }
+      }
+      // cell_add_visc_src (src/Cell/cell_source.c:216-277)
+      if (P.has_visc) {
+        double dist_bh0 = sqrt((xpos - xb[0]) * (xpos - xb[0]) + (ypos - yb[0]) * (ypos - yb[0]));
+        double dist_bh1 = sqrt((xpos - xb[1]) * (xpos - xb[1]) + (ypos - yb[1]) * (ypos - yb[1]));
+        double alpha = P.visc;
+        double eps = P.g_eps;
+        double Sigma_nu;
+        if (P.visc_const == 1) {
+          Sigma_nu = rho * alpha;
+        } else {
+          Sigma_nu = alpha * Pp /
+                     sqrt(pow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
+                          pow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
+        }
+        c[D_TAU] += dt * dV * Sigma_nu * rdrOm_a * (rdrOm_a + r * ld(d.grad, D_UPP, N, g) + ld(d.gradp, D_URR, N, g));
+      }
+      // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
+      {
+        double rom = w_a;
+        double Omega = rom / r;
+        double dr_r2Om = 2. * rom + r * rdrOm_a;
+        double kappa2 = 2. * Omega / r * dr_r2Om;
+        if (kappa2 > 0.) {
+          double kappa = sqrt(kappa2);
+          double l0 = c[D_LLL];
+          double rhov0 = c[D_SRR];
+          double ck = cos(kappa * dt), sk = sin(kappa * dt);
+          double l = l0 * ck - c[D_SRR] * dr_r2Om / kappa * sk;
+          double rhov = rhov0 * ck + 2.0 * Omega * c[D_LLL] / r / kappa * sk;
+          c[D_LLL] = l;
+          c[D_SRR] = rhov;
+        }
+      }
+      done = stop == 4;
+    }
+    if (done) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+    } else {
+      // cell_update_phi + cell_update_dphi (src/Cell/cell_misc.c:59-96)
+      const double r = .5 * (rm + rp);
+      const double w_total = d.w_ann[a] + frame_rom(P, A.rom, r, a_sep);
+      const double *tin = substep == 1 ? d.tiph0 : d.tiph1;
+      double *tout = substep == 1 ? d.tiph1 : d.tiph0;
+      const int gm1 = j == 0 ? A.cell_off + np - 1 : g - 1;
+      double rk = substep == 1 ? tin[g] : d.rktiph[g];
+      double rkm = substep == 1 ? tin[gm1] : d.rktiph[gm1];
+      double tn = new_tiph(tw, rk, RK, w_total, dt, r);
+      double tnm = new_tiph(d.tiphw[gm1], rkm, RK, w_total, dt, r);
+      if (substep == 1) d.rktiph[g] = rk;
+      double dphi_n = tn - tnm;
+      dphi_n = wrap_pos(dphi_n, d.err);
+      tout[g] = tn;
+      d.dphi[g] = dphi_n;
+      // cell_calc_prim -> cell_cons2prim (src/Cell/cell_conversion.c:57-122)
+      const double dz = P.dz;
+      const double dV = A.dv_half * dphi_n * dz;
+      double pr[5];
+      {
+        double rho = c[D_DDD] / dV;
+        if (rho < P.rho_floor) rho = P.rho_floor;
+        double Sr = c[D_SRR] / dV;
+        double Sp = c[D_LLL] / dV / r;
+        double Sz = c[D_SZZ] / dV;
+        double E = c[D_TAU] / dV;
+        double vr = Sr / rho;
+        double vp = Sp / rho;
+        double vz = Sz / rho;
+        double KE = .5 * (Sr * vr + Sp * vp + Sz * vz);
+        double v_magnitude = sqrt(2. * KE / rho);
+        double rhoe = E - KE;
+        double Pp = (P.gamma - 1.) * rhoe;
+        if (Pp < P.cs_floor * P.cs_floor * rho / P.gamma) Pp = P.cs_floor * P.cs_floor * rho / P.gamma;
+        if (Pp > P.cs_cap * P.cs_cap * rho / P.gamma) Pp = P.cs_cap * P.cs_cap * rho / P.gamma;
+        if (v_magnitude > P.vel_cap) {
+          vr = vr * P.vel_cap / v_magnitude;
+          vp = vp * P.vel_cap / v_magnitude;
+          vz = vz * P.vel_cap / v_magnitude;
+        }
+        pr[D_RHO] = rho;
+        pr[D_PPP] = Pp;
+        pr[D_URR] = vr;
+        pr[D_UPP] = vp / r;
+        pr[D_UZZ] = vz;
+      }
+      if (stop >= 6) {
+        // cell_boundary_fixed_r (src/Cell/cell_boundary.c:208-231)
+        if ((A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC)) {
+#pragma unroll
+          for (int q = 0; q < 5; ++q) pr[q] = A.ic[q];
+        }
+        // cell_bc_damp (src/Cell/cell_misc.c:98-132)
+        if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
+          double f = (1. - exp(-A.damp_rate * dt));
+#pragma unroll
+          for (int q = 0; q < 5; ++q) {
+            double dprim = A.ic[q] - pr[q];
+            pr[q] += f * dprim;
+          }
+        }
+      }
+      if (stop >= 7) {
+        // cell_calc_cons (src/Cell/cell_conversion.c:35-55)
+        prim2cons(pr, c, r, dV, P.gamma);
+      }
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        d.prim[(size_t)q * N + g] = pr[q];
+        d.cons[(size_t)q * N + g] = c[q];
+      }
+    }
+  }
+  if (tail == 0) return;
+
+  // deterministic per-block Mdot partial sums
+  {
+    const unsigned full = 0xffffffffu;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      md0 += __shfl_down_sync(full, md0, o);
+      md1 += __shfl_down_sync(full, md1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      sh_md[0][threadIdx.x >> 5] = md0;
+      sh_md[1][threadIdx.x >> 5] = md1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s0 = 0.0, s1 = 0.0;
+      for (int w = 0; w < BLK / 32; ++w) {
+        s0 += sh_md[0][w];
+        s1 += sh_md[1][w];
+      }
+      d.mdot_part[2 * blockIdx.x] = s0;
+      d.mdot_part[2 * blockIdx.x + 1] = s1;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&d.counters[1], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // GravMass after the substep: gravMass_update_RK (GravMass_misc.c:66-77),
+  // then gravMass_move(t, fac*dt) (GravMass_misc.c:31-64); after substep 2
+  // also t += dt and Macc += Mdot*dt (timestep_algorithm.c:27-39).
+  for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
+    InstState &S = d.ist[k];
+    const DiskParams &P = d.par[k];
+    // Mdot of this disk: block partials in block order
+    {
+      int c0 = P.cell_base, c1 = P.cell_base + P.n_cells;
+      int b0 = c0 / BLK, b1 = (c1 + BLK - 1) / BLK;
+      double s0 = 0.0, s1 = 0.0;
+      if (P.rho_sink_on == 1) {
+        for (int b = b0; b < b1; ++b) {
+          s0 += d.mdot_part[2 * b];
+          s1 += d.mdot_part[2 * b + 1];
+        }
+      }
+      S.mdot[0] = s0;
+      S.mdot[1] = s1;
+    }
+    for (int p = 0; p < 2; ++p) {
+      while (S.gphi[p] - S.grk_phi[p] > M_PI) S.grk_phi[p] += 2. * M_PI;
+      while (S.gphi[p] - S.grk_phi[p] < -M_PI) S.grk_phi[p] -= 2. * M_PI;
+      S.gr[p] = (1.0 - RK) * S.gr[p] + RK * S.grk_r[p];
+      S.gphi[p] = (1.0 - RK) * S.gphi[p] + RK * S.grk_phi[p];
+      S.gM[p] = (1.0 - RK) * S.gM[p] + RK * S.grk_M[p];
+      S.gom[p] = (1.0 - RK) * S.gom[p] + RK * S.grk_om[p];
+    }
+    if (tail >= 2) {
+      double t = S.t, dtm = fac * S.dt;
+      double m0 = S.gM[0], m1 = S.gM[1];
+      double M = m0 + m1;
+      double a_0 = 1.0, tau_0 = P.orb_tscale, T0 = P.orb_t0;
+      double asep, omega;
+      if ((t - T0) / tau_0 < 1.) {
+        asep = a_0 * pow((1.0 - (t - T0) / tau_0), 0.25);
+        omega = pow(asep / M, -1.5);
+      } else {
+        asep = 0.0;
+        omega = 0.0;
+      }
+      double r0, r1;
+      if (M < 1.e-12) {
+        r0 = 0.0;
+        r1 = 0.0;
+      } else {
+        r0 = m1 / M * asep;
+        r1 = m0 / M * asep;
+      }
+      S.gphi[0] += omega * dtm;
+      S.gphi[1] += omega * dtm;
+      S.gr[0] = r0;
+      S.gr[1] = r1;
+      S.gom[0] = omega;
+      S.gom[1] = omega;
+      if (substep == 2) {
+        S.t += S.dt;
+        for (int p = 0; p < 2; ++p) S.macc[p] = S.macc[p] + S.mdot[p] * S.dt;
+      }
+    }
+  }
+  if (threadIdx.x == 0) d.counters[1] = 0;
+}
+
+// cell_calc_cons over all cells (set-up and state upload)
+__global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  if (g >= N) return;
+  const Annulus A = d.ann[d.cell_ann[g]];
+  const DiskParams &P = d.par[A.inst];
+  double r = .5 * (A.rp + A.rm);
+  double dV = A.dv_half * d.dphi[g] * P.dz;
+  double p[5], c[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) p[q] = ld(d.prim, q, N, g);
+  prim2cons(p, c, r, dV, P.gamma);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+}
+
+// Torque on the binary: -sum over non-ghost cells of r*rho*dV*F_phi, with the
+// gas state's cell-centre phi and F_phi from gravMassForce; per-block partial
+// sums, reduced in block order by the last block.
+__global__ void __launch_bounds__(BLK) k_torque(DevPtrs d, int inst, double *part, double *out) {
+  __shared__ double sh[BLK / 32];
+  __shared__ bool last;
+  const DiskParams &P = d.par[inst];
+  const InstState &S = d.ist[inst];
+  const int N = d.n_cells;
+  const int g = P.cell_base + blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (g < P.cell_base + P.n_cells) {
+    const Annulus A = d.ann[d.cell_ann[g]];
+    if (A.kind & DGPU_AK_CFL) {
+      double dphi = d.dphi[g];
+      double phi = d.tiph0[g] - .5 * dphi;
+      double r = .5 * (A.rp + A.rm);
+      double rho = ld(d.prim, D_RHO, N, g);
+      double dV = dphi * .5 * A.dv_diff * P.dz;
+      double cosp = cos(phi), sinp = sin(phi);
+      double Fp = 0.0;
+      for (int p = 0; p < 2; ++p) {
+        double dx = r * cosp - S.gr[p] * cos(S.gphi[p]);
+        double dy = r * sinp - S.gr[p] * sin(S.gphi[p]);
+        double script_r = sqrt(dx * dx + dy * dy);
+        double cosa = dx / script_r, sina = dy / script_r;
+        double sinap = sina * cosp - cosa * sinp;
+        Fp += sinap * -fgrav(S.gM[p], script_r, P.g_eps, P.phi_order);
+      }
+      v = -(r * rho * dV * Fp);
+    }
+  }
+  const unsigned full = 0xffffffffu;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < BLK / 32; ++w) s += sh[w];
+    part[blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&d.counters[2], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double s = 0.0;
+  for (int b = 0; b < (int)gridDim.x; ++b) s += ((volatile double *)part)[b];
+  *out = s;
+  d.counters[2] = 0;
+}
+
+// AoS rows [n][nq] (the boundary format) <-> SoA columns X[q*stride + base + c]
+__global__ void k_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int q = 0; q < nq; ++q) soa[(size_t)q * stride + base + c] = aos[(size_t)c * nq + q];
+}
+__global__ void k_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int q = 0; q < nq; ++q) aos[(size_t)c * nq + q] = soa[(size_t)q * stride + base + c];
+}
+
+}  // namespace
+
+extern "C" {
+
+int dgk_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n, void *stream) {
+  if (n <= 0) return 0;
+  k_aos_to_soa<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(soa, nq, stride, base, aos, n);
+  return (int)cudaGetLastError();
+}
+int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa, int n, void *stream) {
+  if (n <= 0) return 0;
+  k_soa_to_aos<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(aos, nq, stride, base, soa, n);
+  return (int)cudaGetLastError();
+}
+
+int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
+
+int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream) {
+  k_face<<<d->n_ann, BLK, 0, (cudaStream_t)stream>>>(*d, substep, gm_ops);
+  return (int)cudaGetLastError();
+}
+int dgk_plm_r(const DevPtrs *d, int substep, void *stream) {
+  k_plm_r<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_flux(const DevPtrs *d, int substep, void *stream) {
+  int n = d->n_cells + d->n_slots;
+  k_flux<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_update(const DevPtrs *d, int substep, int stop, void *stream) {
+  int tail = stop >= 7 ? 2 : (stop >= 5 ? 1 : 0);
+  k_update<<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, substep, stop, tail);
+  return (int)cudaGetLastError();
+}
+int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
+  int tail = stop >= 5 ? 1 : 0;
+  k_update<<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, substep, stop, tail);
+  return (int)cudaGetLastError();
+}
+int dgk_calc_cons(const DevPtrs *d, void *stream) {
+  k_calc_cons<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
+  return (int)cudaGetLastError();
+}
+int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream) {
+  int nb = (n_inst_cells + BLK - 1) / BLK;
+  k_torque<<<nb, BLK, 0, (cudaStream_t)stream>>>(*d, inst, part, out);
+  return (int)cudaGetLastError();
+}
+
+}  // extern "C"

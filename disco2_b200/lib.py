@@ -1,0 +1,241 @@
+"""ctypes binding of libdisco_gpu.so (the C ABI in include/disco_gpu.h).
+
+Python is a thin caller here: every numerical step runs in the library's CUDA
+kernels.  Loading fails loudly when the shared library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import configs
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libdisco_gpu.so")
+
+OK = 0
+ERR_NAMES = {-1: "ARG", -2: "PARFILE", -3: "UNSUPPORTED", -4: "CUDA", -5: "FACE_OVERFLOW",
+             -6: "NUMERIC", -7: "NOMEM"}
+
+# Every symbol the header declares, with its ctypes signature.
+_P, _I, _D = C.c_void_p, C.c_int, C.c_double
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+SIGNATURES = {
+    "dgpu_sim_from_parfile": (_I, [C.c_char_p, C.POINTER(_P)]),
+    "dgpu_sim_from_text": (_I, [C.c_char_p, C.POINTER(_P)]),
+    "dgpu_sim_destroy": (None, [_P]),
+    "dgpu_sim_num_annuli": (_I, [_P]),
+    "dgpu_sim_num_cells": (_I, [_P]),
+    "dgpu_sim_grid": (_I, [_P, _ip, _dp]),
+    "dgpu_sim_param": (_I, [_P, C.c_char_p, _dp]),
+    "dgpu_sim_initial_state": (_I, [_P, _dp, _dp, _dp, _dp]),
+    "dgpu_create": (_I, [C.POINTER(_P), _I, _I, _P, C.POINTER(_P)]),
+    "dgpu_destroy": (None, [_P]),
+    "dgpu_last_error": (C.c_char_p, [_P]),
+    "dgpu_num_instances": (_I, [_P]),
+    "dgpu_init_state": (_I, [_P, _I]),
+    "dgpu_set_state": (_I, [_P, _I, _dp, _dp, _dp]),
+    "dgpu_get_state": (_I, [_P, _I, _dp, _dp, _dp, _dp]),
+    "dgpu_set_gravmass": (_I, [_P, _I, _dp]),
+    "dgpu_get_gravmass": (_I, [_P, _I, _dp]),
+    "dgpu_get_time": (_I, [_P, _I, _dp, _dp]),
+    "dgpu_set_time": (_I, [_P, _I, _D]),
+    "dgpu_step_rk2": (_I, [_P, _I]),
+    "dgpu_synchronize": (_I, [_P]),
+    "dgpu_stage": (_I, [_P, _I]),
+    "dgpu_get_stage_data": (_I, [_P, _I, _dp, _dp, _dp, _dp, _dp]),
+    "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
+    "dgpu_torque": (_I, [_P, _I, _dp]),
+}
+
+_lib = None
+
+
+class DiscoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load the library (once).  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m disco2_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _iptr(a):
+    return None if a is None else a.ctypes.data_as(_ip)
+
+
+class Sim:
+    """Host-side Sim built from a parfile (text, path or parameter dict)."""
+
+    def __init__(self, par):
+        lib = load()
+        h = _P()
+        if isinstance(par, dict):
+            rc = lib.dgpu_sim_from_text(configs.parfile_text(par).encode(), C.byref(h))
+        elif isinstance(par, str) and "\n" in par:
+            rc = lib.dgpu_sim_from_text(par.encode(), C.byref(h))
+        else:
+            rc = lib.dgpu_sim_from_parfile(os.fsencode(par), C.byref(h))
+        if rc != OK:
+            raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+        self._h = h
+        self.num_annuli = lib.dgpu_sim_num_annuli(h)
+        self.num_cells = lib.dgpu_sim_num_cells(h)
+
+    def grid(self):
+        N_p = np.zeros(self.num_annuli, np.int32)
+        rf = np.zeros(self.num_annuli + 1, np.float64)
+        load().dgpu_sim_grid(self._h, _iptr(N_p), _dptr(rf))
+        return N_p, rf
+
+    def param(self, key: str) -> float:
+        v = C.c_double()
+        rc = load().dgpu_sim_param(self._h, key.encode(), C.byref(v))
+        if rc != OK:
+            raise KeyError(key)
+        return v.value
+
+    def initial_state(self) -> dict:
+        """Host-computed initial state (what Context.init_state uploads)."""
+        n = self.num_cells
+        out = {"prim": np.zeros((n, 5)), "tiph": np.zeros(n), "dphi": np.zeros(n),
+               "gm": np.zeros((2, 6))}
+        rc = load().dgpu_sim_initial_state(self._h, _dptr(out["prim"]), _dptr(out["tiph"]),
+                                          _dptr(out["dphi"]), _dptr(out["gm"]))
+        if rc != OK:
+            raise DiscoError(rc, load().dgpu_last_error(None).decode())
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.dgpu_sim_destroy(self._h)
+            self._h = None
+
+
+class Context:
+    """Device state of one or more independent disks."""
+
+    def __init__(self, sims, device: int = 0, stream: int | None = None):
+        lib = load()
+        if isinstance(sims, Sim):
+            sims = [sims]
+        self.sims = list(sims)
+        arr = (_P * len(self.sims))(*[s._h for s in self.sims])
+        h = _P()
+        rc = lib.dgpu_create(arr, len(self.sims), device, _P(stream) if stream else None, C.byref(h))
+        if rc != OK:
+            raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+        self._h = h
+
+    def _ck(self, rc):
+        if rc != OK:
+            raise DiscoError(rc, load().dgpu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().dgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+    def init_state(self, inst: int = 0):
+        self._ck(load().dgpu_init_state(self._h, inst))
+
+    def set_state(self, inst, prim, tiph, dphi):
+        prim = np.ascontiguousarray(prim, np.float64)
+        tiph = np.ascontiguousarray(tiph, np.float64)
+        dphi = np.ascontiguousarray(dphi, np.float64)
+        n = self.sims[inst].num_cells
+        assert prim.shape == (n, 5) and tiph.shape == (n,) and dphi.shape == (n,)
+        self._ck(load().dgpu_set_state(self._h, inst, _dptr(prim), _dptr(tiph), _dptr(dphi)))
+        self._ck(load().dgpu_synchronize(self._h))
+
+    def get_state(self, inst: int = 0) -> dict:
+        n = self.sims[inst].num_cells
+        prim = np.zeros((n, 5))
+        cons = np.zeros((n, 5))
+        tiph = np.zeros(n)
+        dphi = np.zeros(n)
+        self._ck(load().dgpu_get_state(self._h, inst, _dptr(prim), _dptr(cons), _dptr(tiph), _dptr(dphi)))
+        return {"prim": prim, "cons": cons, "tiph": tiph, "dphi": dphi}
+
+    def stage_data(self, inst: int = 0) -> dict:
+        n = self.sims[inst].num_cells
+        out = {"grad": np.zeros((n, 5)), "gradp": np.zeros((n, 5)), "wiph": np.zeros(n),
+               "RKcons": np.zeros((n, 5)), "RKtiph": np.zeros(n)}
+        self._ck(load().dgpu_get_stage_data(self._h, inst, _dptr(out["grad"]), _dptr(out["gradp"]),
+                                            _dptr(out["wiph"]), _dptr(out["RKcons"]),
+                                            _dptr(out["RKtiph"])))
+        return out
+
+    def set_gravmass(self, inst, gm):
+        gm = np.ascontiguousarray(gm, np.float64).reshape(12)
+        self._ck(load().dgpu_set_gravmass(self._h, inst, _dptr(gm)))
+
+    def gravmass(self, inst: int = 0) -> np.ndarray:
+        gm = np.zeros(12)
+        self._ck(load().dgpu_get_gravmass(self._h, inst, _dptr(gm)))
+        return gm.reshape(2, 6)
+
+    def time(self, inst: int = 0):
+        t, dt = C.c_double(), C.c_double()
+        self._ck(load().dgpu_get_time(self._h, inst, C.byref(t), C.byref(dt)))
+        return t.value, dt.value
+
+    def set_time(self, inst, t):
+        self._ck(load().dgpu_set_time(self._h, inst, float(t)))
+
+    def step(self, nsteps: int = 1, sync: bool = True):
+        self._ck(load().dgpu_step_rk2(self._h, nsteps))
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        self._ck(load().dgpu_synchronize(self._h))
+
+    def stage(self, phase: int):
+        self._ck(load().dgpu_stage(self._h, phase))
+
+    def face_list(self, inst: int = 0) -> dict:
+        lib = load()
+        s = self.sims[inst]
+        nf = C.c_int()
+        lib.dgpu_face_list(self._h, inst, 0, None, None, None, None, None, None, None, None, None,
+                           C.byref(nf))
+        n = nf.value
+        out = {"nri": np.zeros(s.num_annuli, np.int32), "L": np.zeros(n, np.int32),
+               "R": np.zeros(n, np.int32)}
+        for k in ("r", "dphi", "dA", "deltaL", "deltaR", "cm"):
+            out[k] = np.zeros(n)
+        self._ck(lib.dgpu_face_list(self._h, inst, n, _iptr(out["nri"]), _iptr(out["L"]),
+                                    _iptr(out["R"]), _dptr(out["r"]), _dptr(out["dphi"]),
+                                    _dptr(out["dA"]), _dptr(out["deltaL"]), _dptr(out["deltaR"]),
+                                    _dptr(out["cm"]), C.byref(nf)))
+        return out
+
+    def torque(self, inst: int = 0) -> float:
+        v = C.c_double()
+        self._ck(load().dgpu_torque(self._h, inst, C.byref(v)))
+        return v.value

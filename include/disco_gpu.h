@@ -1,0 +1,143 @@
+/*
+ * disco_gpu.h -- C ABI of the B200 moving-mesh finite-volume step.
+ *
+ * The library replaces the per-step hot path of Disco2: timestep_rk2 and
+ * everything below it (src/Headers/TimeStep.h:21-32, Face.h:22, Riemann.h:37-42,
+ * Cell.h:25-91, GravMass.h:24-46).  Host code is C; all per-cell and per-face
+ * work runs in hand-written sm_100a kernels on one GPU.  Plain C types only:
+ * pointers, sizes, doubles, ints.  No CUDA or torch types appear here; the
+ * optional stream is passed as `void *` (a cudaStream_t, or NULL for the
+ * library's own stream).
+ *
+ * Conventions
+ *   - Every function that can fail returns int: 0 (DGPU_OK) or a negative
+ *     DGPU_ERR_* code; dgpu_last_error() returns the message.  The reference
+ *     printf()s and exit()s instead (19 sites, e.g. Riemann_routines.c:168,
+ *     Riemann_routines.c:271-274, cell_set_w.c:15-16).
+ *   - Ownership: the caller owns every host buffer; a context owns all device
+ *     memory it allocates.  No global state except the last-error string.
+ *   - Cell order at the boundary is the reference's (k, i, j) order of the
+ *     contiguous cell array built by cell_create (src/Cell/cell_create_destroy.c:
+ *     37-48), ghost annuli included; per-cell variables are NUM_Q-wide rows,
+ *     prim = (rho, P, v_r, omega, v_z), cons = (D, tau, S_r, L, S_z) x dV
+ *     (src/Headers/header.h:1-2).
+ *   - Threading: one host thread per context at a time.
+ *   - A context holds one or more independent disks ("instances"); the plain
+ *     method is a context with one instance, the batched sweep one with many.
+ */
+#ifndef DISCO_GPU_H
+#define DISCO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGPU_OK 0
+#define DGPU_ERR_ARG (-1)          /* bad argument or index */
+#define DGPU_ERR_PARFILE (-2)      /* parfile missing, unreadable or missing a key */
+#define DGPU_ERR_UNSUPPORTED (-3)  /* option outside the implemented path (e.g. NumZ > 1) */
+#define DGPU_ERR_CUDA (-4)         /* a CUDA runtime call failed */
+#define DGPU_ERR_FACE_OVERFLOW (-5)/* face list exceeded its buffer (device flag) */
+#define DGPU_ERR_NUMERIC (-6)      /* device-detected condition the reference exit()s on */
+#define DGPU_ERR_NOMEM (-7)        /* host or device allocation failed */
+
+typedef struct dgpu_sim dgpu_sim; /* host-side Sim: parameters + grid */
+typedef struct dgpu_ctx dgpu_ctx; /* device context: state of one or more disks */
+
+/* ---- Sim (host) -------------------------------------------------------
+ * Replaces sim_create + sim_read_par_file + sim_alloc_arr + sim_set_rz +
+ * sim_set_N_p + sim_set_misc (src/Sim/sim_readpar.c:48-122,
+ * src/Sim/sim_alloc_arr.c:9-46, src/Sim/sim_set.c:10-177): same 52 keys, same
+ * key matching and value parsing, same grid and N_p rules.  Unlike the
+ * reference, a missing key is an error (the reference prints "cant find" and
+ * leaves the field uninitialised, src/Sim/sim_readpar.c:25-28). */
+int dgpu_sim_from_parfile(const char *path, dgpu_sim **out);
+int dgpu_sim_from_text(const char *text, dgpu_sim **out);
+void dgpu_sim_destroy(dgpu_sim *sim);
+/* Numbers of annuli (sim_N(R_DIR), ghosts included) and cells. */
+int dgpu_sim_num_annuli(const dgpu_sim *sim);
+int dgpu_sim_num_cells(const dgpu_sim *sim);
+/* N_p[NR] (sim_N_p) and r_faces[NR+1] (r_faces[i+1] = sim_FacePos(i, R_DIR)). */
+int dgpu_sim_grid(const dgpu_sim *sim, int *N_p, double *r_faces);
+/* Value of a parfile key as read (ints are returned as doubles). */
+int dgpu_sim_param(const dgpu_sim *sim, const char *key, double *value);
+/* Host-only: the initial state dgpu_init_state uploads -- prim[N][NUM_Q],
+ * tiph[N], dphi[N] and gm[2][6] -- computed on the CPU (any pointer may be
+ * NULL).  Same set-up sequence as src/main.c:74-117 (see dgpu_init_state). */
+int dgpu_sim_initial_state(const dgpu_sim *sim, double *prim, double *tiph, double *dphi, double *gm);
+
+/* ---- Context ---------------------------------------------------------- */
+/* Allocates device state for n disks on `device`; stream may be NULL.
+ * The sims are copied; the caller may destroy them afterwards. */
+int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dgpu_ctx **out);
+void dgpu_destroy(dgpu_ctx *ctx);
+/* Message of the last failure on this context (ctx may be NULL: last failure
+ * of a create call on this thread). */
+const char *dgpu_last_error(const dgpu_ctx *ctx);
+int dgpu_num_instances(const dgpu_ctx *ctx);
+
+/* ---- State --------------------------------------------------------------
+ * dgpu_init_state repeats the reference set-up of src/main.c:74-119 for one
+ * disk: cell_create's phi offsets (srand(666); tiph_0 = 2pi*rand()/RAND_MAX
+ * per annulus, src/Cell/cell_create_destroy.c:64-91), cell_clean_pi, the
+ * GravMass initialiser of GravMassType (src/GravMass/GravMass_init.c:9-84),
+ * the initial data of InitialDataType, gravMass_clean_pi and cell_calc_cons.
+ * t is set to 0. */
+int dgpu_init_state(dgpu_ctx *ctx, int inst);
+/* Replace prim[N][NUM_Q], tiph[N], dphi[N] of a disk (host buffers), then
+ * recompute cons as cell_calc_cons does (src/Cell/cell_conversion.c:35-55). */
+int dgpu_set_state(dgpu_ctx *ctx, int inst, const double *prim, const double *tiph,
+                   const double *dphi);
+/* Copy a disk's state to host buffers; any pointer may be NULL. */
+int dgpu_get_state(dgpu_ctx *ctx, int inst, double *prim, double *cons, double *tiph,
+                   double *dphi);
+/* GravMass state gm[2][6] = (r, phi, M, omega, Mdot, Macc) per mass
+ * (src/Headers/GravMass.h:7-20). */
+int dgpu_set_gravmass(dgpu_ctx *ctx, int inst, const double *gm);
+int dgpu_get_gravmass(dgpu_ctx *ctx, int inst, double *gm);
+/* Simulation time t and the dt of the last step (timestep_get_t, timestep_dt). */
+int dgpu_get_time(dgpu_ctx *ctx, int inst, double *t, double *dt);
+int dgpu_set_time(dgpu_ctx *ctx, int inst, double t);
+
+/* ---- Stepping --------------------------------------------------------------
+ * dgpu_step_rk2 advances every disk of the context by nsteps calls of
+ * timestep_rk2 (src/TimeStep/timestep_algorithm.c:11-41), each disk with its
+ * own CFL dt.  The first call captures one step into a CUDA graph; later calls
+ * replay it.  Asynchronous: returns once the work is queued; device errors
+ * surface at the next dgpu_synchronize (or any dgpu_get_*). */
+int dgpu_step_rk2(dgpu_ctx *ctx, int nsteps);
+int dgpu_synchronize(dgpu_ctx *ctx);
+/* Stage parity: the prologue of timestep_rk2 and the first substep
+ * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`
+ * (0 faces/clean_pi/set_w/RK blend, 1 PLM, 2 phi fluxes, 3 r fluxes,
+ * 4 sources, 5 mesh motion + cons2prim, 6 boundary + damping, 7 calc_cons).
+ * Leaves the context mid-step; reload the state before stepping again. */
+int dgpu_stage(dgpu_ctx *ctx, int phase);
+/* Per-cell intermediates after dgpu_stage: grad, gradp ([N][NUM_Q]), wiph[N],
+ * RKcons[N][NUM_Q], RKtiph[N]; any pointer may be NULL. */
+int dgpu_get_stage_data(dgpu_ctx *ctx, int inst, double *grad, double *gradp, double *wiph,
+                        double *rkcons, double *rktiph);
+
+/* ---- Face list ---------------------------------------------------------------
+ * The r-face list of the current state, as face_create(..., 0) builds it
+ * (src/Face/face_create_destroy.c:130-193) and in its order: nri[NR] offsets
+ * (timestep_n(..., R_DIR)), L/R cell numbers in (k, i, j) order, r, dphi,
+ * dA, deltaL, deltaR, cm (src/Headers/Face.h:9-18).  cap = capacity of the
+ * per-face arrays; *nf receives the face count (also when cap is too small,
+ * which returns DGPU_ERR_ARG). */
+int dgpu_face_list(dgpu_ctx *ctx, int inst, int cap, int *nri, int *L, int *R, double *r,
+                   double *dphi, double *dA, double *deltaL, double *deltaR, double *cm,
+                   int *nf);
+
+/* ---- Objective -----------------------------------------------------------------
+ * Gravitational torque on the binary from the gas, T = sum over non-ghost cells
+ * of r * rho * dV * F_phi(r, phi) with F_phi the azimuthal point-mass force of
+ * gravMassForce (src/Cell/cell_source.c:49-71), evaluated on the current
+ * state (it has no counterpart in the reference, which has no torque
+ * diagnostic). */
+int dgpu_torque(dgpu_ctx *ctx, int inst, double *torque);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
