@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""FP64 zone-updates/s of the moving-mesh RK2 step on B200.
+
+A step is one timestep_rk2 of a disk (two substeps: face list, PLM,
+HLL/HLLC + viscous fluxes, sources, mesh motion, boundaries).  A zone-update
+is one non-ghost cell advanced by one full step.  Default workload: the
+circumbinary disk (400 log annuli, r in [0.4, 20], 258,078 cells, equal-mass
+binary, alpha = 0.1 viscosity, HLLC, outer damping zone).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank advances its own replica of the disk (the
+single-disk step does not shard): per-GPU work is fixed, the
+reported value is the sum over ranks, timed as the maximum over ranks.
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "FP64 zone-updates/s"
+UNIT = "zone-updates/s"
+PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Compulsory DRAM bytes per unit for each kernel as designed (each array
+# element touched once): per cell and per r-face of one substep.
+KERNELS = ["face", "plm_r", "flux", "update"]
+ALG_BYTES = {
+    # name: (bytes per cell, bytes per r-face)
+    "face": (8 + 8 + 40 + 8 + 40 + 4 + 4, 24),
+    "plm_r": (40 + 40 + 8 + 8 + 4 + 40, 24),
+    "flux": (40 + 40 + 40 + 8 + 8 + 64, 24 + 64),
+    "update": (40 + 40 + 40 + 8 + 8 + 8 + 8 + 16 + 64 + 8 + 40 + 40 + 8 + 8 + 8, 64),
+}
+STEP_ALG_BYTES = 240  # per zone-update: 5 conserved + 1 phi edge, read/written across 2 stages
+
+
+def workload_params(name: str):
+    from disco2_b200 import configs
+    if name == "circumbinary":
+        return configs.circumbinary(), ("circumbinary disk: equal-mass binary, 400 log annuli "
+                                        "r in [0.4, 20], aspect 1, alpha=0.1, HLLC, PLM 1.5, "
+                                        "outer damping r>16")
+    if name == "kepler_ring":
+        return configs.kepler_ring(), ("viscous Keplerian ring: 256 log annuli r in [0.5, 4], "
+                                       "nu=1e-3, HLL")
+    if name == "gresho":
+        return configs.gresho(), ("Gresho vortex: 96 uniform annuli r in [0.1, 1], rigidly "
+                                  "rotating mesh, HLLC")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def load_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50"]
+            if gpu_id:
+                cmd += ["-i", gpu_id]
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 8:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    smax.append(float(parts[1]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def cpu_baseline_run(par_text: str, steps: int, warmup: int):
+    """Time the reference build (or the C restatement) on the host cores."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle  # noqa: E402  (CPU baseline leg only)
+    exe, kind = (oracle.REF_BIN, "reference") if oracle.have_ref() else (oracle.PORT_BIN, "port")
+    if not os.path.exists(exe):
+        try:
+            oracle.build(ref=False, port=True)
+        except Exception:
+            pass
+        exe, kind = oracle.PORT_BIN, "port"
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        par = os.path.join(td, "w.par")
+        with open(par, "w") as f:
+            f.write(par_text)
+        r = subprocess.run([exe, "run", par, str(steps), os.path.join(td, "o.bin"), "--warmup",
+                            str(warmup)], capture_output=True, text=True, check=True)
+    wall = None
+    for line in r.stderr.splitlines():
+        if line.startswith("steps_wall_s"):
+            wall = float(line.split()[1])
+    return wall, kind
+
+
+def interior_cells(sim) -> int:
+    N_p, _ = sim.grid()
+    ngmin = 1
+    ngmax = int(sim.param("ng"))
+    return int(N_p[ngmin:len(N_p) - ngmax].sum())
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from disco2_b200 import configs
+    p, desc = workload_params(args.workload)
+    from disco2_b200 import lib
+    sim = lib.Sim(p)
+    nin = interior_cells(sim)
+    # the reference needs ~2 s per step here: time a bounded sample of the K steps
+    steps = max(1, min(args.steps, args.ref_max_steps))
+    warm = max(0, min(args.warmup, 1))
+    res = cpu_baseline_run(configs.parfile_text(p), steps, warm)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no oracle binary could be built"}))
+        return
+    wall, kind = res
+    value = nin * steps / wall
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * wall / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": desc, "cells": sim.num_cells,
+                                        "interior_cells": nin, "annuli": sim.num_annuli},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+                         "sample": f"{steps} of the {args.steps} requested RK2 steps of the same "
+                                   f"disk on one host core (the reference is single-threaded "
+                                   f"without MPI), after {warm} warm-up step(s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="circumbinary")
+    ap.add_argument("--ref-max-steps", type=int, default=12)
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from disco2_b200 import configs, lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p, desc = workload_params(args.workload)
+    sim = lib.Sim(p)
+    nin = interior_cells(sim)
+    stream = torch.cuda.Stream()
+    ctx = lib.Context(sim, device=local, stream=stream.cuda_stream)
+    ctx.init_state(0)
+    L = lib.load()
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+
+    # warm-up (also captures the step graph)
+    with torch.cuda.stream(stream):
+        ctx.step(args.warmup, sync=False)
+    ctx.synchronize()
+    sampler = ClockSampler(uuid)
+    # keep the GPU busy ~0.3 s before timing so the clock samples see load
+    t_end = time.time() + 0.3
+    while time.time() < t_end:
+        ctx.step(20, sync=False)
+        ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            starts[k].record(stream)
+            L.dgpu_step_rk2(ctx.handle, 1)
+            ends[k].record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ms = max_over_ranks(ms)
+    value = nin * args.steps * world / (ms / 1e3)
+
+    # per-kernel device times (same steps launched kernel by kernel, L2 flushed between steps)
+    kern = [0.0] * 8
+    nprof = max(3, min(args.steps, 50))
+    for k in range(nprof):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        km = ctx.step_timed(1)
+        kern = [a + b for a, b in zip(kern, km)]
+    per_kernel = {}
+    for i, nm in enumerate(KERNELS):
+        per_kernel[nm] = (kern[i] + kern[4 + i]) / (2 * nprof)  # ms per launch
+    dom = max(per_kernel, key=per_kernel.get)
+    # units: cells and r-faces of one substep
+    fl = ctx.face_list(0)
+    nfaces = int(len(fl["L"]))
+    ncell = sim.num_cells
+    bpc, bpf = ALG_BYTES[dom]
+    alg_bytes = bpc * ncell + bpf * nfaces
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (per_kernel[dom] * 1e-3) / 1e9
+
+    # end to end through the C ABI: host (pinned) state in, one step, host state out
+    n = sim.num_cells
+    prim_h = torch.empty((n, 5), dtype=torch.float64, pin_memory=True)
+    tiph_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    dphi_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    dp = C.POINTER(C.c_double)
+    P_prim = C.cast(prim_h.data_ptr(), dp)
+    P_tiph = C.cast(tiph_h.data_ptr(), dp)
+    P_dphi = C.cast(dphi_h.data_ptr(), dp)
+    rc = L.dgpu_get_state(ctx.handle, 0, P_prim, None, P_tiph, P_dphi)
+    assert rc == 0, L.dgpu_last_error(ctx.handle)
+    h2d = (5 + 2) * 8 * n
+    d2h = (5 + 2) * 8 * n
+    ke = max(3, min(args.steps, 50))
+    for _ in range(2):  # warm
+        L.dgpu_set_state(ctx.handle, 0, P_prim, P_tiph, P_dphi)
+        L.dgpu_step_rk2(ctx.handle, 1)
+        L.dgpu_get_state(ctx.handle, 0, P_prim, None, P_tiph, P_dphi)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        rc = L.dgpu_set_state(ctx.handle, 0, P_prim, P_tiph, P_dphi)
+        rc |= L.dgpu_step_rk2(ctx.handle, 1)
+        rc |= L.dgpu_get_state(ctx.handle, 0, P_prim, None, P_tiph, P_dphi)
+        assert rc == 0, L.dgpu_last_error(ctx.handle)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = nin * ke * world / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res = cpu_baseline_run(configs.parfile_text(p), args.cpu_steps, 1)
+        if res is not None:
+            wall, kind = res
+            cpu = {"value": nin * args.cpu_steps / wall, "unit": UNIT, "cores": 1, "kind": kind,
+                   "sample": f"{args.cpu_steps} RK2 steps of the same disk on one host core, "
+                             f"after 1 warm-up step ({wall:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "cells": ncell, "interior_cells": nin,
+                       "annuli": sim.num_annuli, "r_faces": nfaces,
+                       "l2": "flushed between timed steps (256 MiB write outside the events)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single disk"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "alg_bytes_per_launch": alg_bytes,
+                         "ms_per_launch": per_kernel[dom]},
+            "step_roofline": {"alg_bytes_per_zone_update": STEP_ALG_BYTES,
+                              "achieved_gbs": value / world * STEP_ALG_BYTES / 1e9,
+                              "frac": value / world * STEP_ALG_BYTES / 1e9 / peak},
+            "kernel_ms": per_kernel,
+            "gpu_launches": 8 * args.steps,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": ke, "how": "dgpu_set_state from pinned host prim/tiph/dphi, "
+                                        "dgpu_step_rk2(1), dgpu_get_state to pinned host, per step"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

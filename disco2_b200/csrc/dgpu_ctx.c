@@ -415,6 +415,8 @@ static int read_err(struct dgpu_ctx *c) {
   int e = 0;
   CK(cudaMemcpyAsync(&e, c->d.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  /* a flag is reported once; the caller reloads a valid state to continue */
+  if (e) CK(cudaMemsetAsync(c->d.err, 0, sizeof(int), c->stream));
   if (e & (DGPU_EF_FACE_OVERFLOW | DGPU_EF_RUN_OVERFLOW))
     return fail(c, DGPU_ERR_FACE_OVERFLOW, "face list overflowed its buffer (flags 0x%x)", e);
   if (e & DGPU_EF_WRAP_LIMIT)
@@ -650,6 +652,36 @@ int dgpu_step_rk2(dgpu_ctx *c, int nsteps) {
   return DGPU_OK;
 }
 
+int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
+  cudaEvent_t ev[9];
+  int k, s, sub, rc = DGPU_OK;
+  if (!c || nsteps < 0 || !kernel_ms) return DGPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  for (k = 0; k < 9; ++k) CK(cudaEventCreate(&ev[k]));
+  for (s = 0; s < nsteps && rc == DGPU_OK; ++s) {
+    int e = 0;
+    CK(cudaEventRecord(ev[e++], c->stream));
+    for (sub = 1; sub <= 2; ++sub) {
+      CKK(dgk_face(&c->d, sub, 1, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_plm_r(&c->d, sub, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_flux(&c->d, sub, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_update(&c->d, sub, 7, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+    }
+    CK(cudaEventSynchronize(ev[8]));
+    for (k = 0; k < 8; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      kernel_ms[k] += (double)ms;
+    }
+  }
+  for (k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+  return read_err(c);
+}
+
 int dgpu_stage(dgpu_ctx *c, int phase) {
   if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
@@ -658,6 +690,10 @@ int dgpu_stage(dgpu_ctx *c, int phase) {
   CKK(dgk_plm_r(&c->d, 1, c->stream));
   if (phase >= 2) CKK(dgk_flux(&c->d, 1, c->stream));
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
+  /* from phase 5 on the advanced phi edges live in the substep's output buffer */
+  if (phase >= 5)
+    CK(cudaMemcpyAsync(c->d.tiph0, c->d.tiph1, sizeof(double) * (size_t)c->n_cells,
+                       cudaMemcpyDeviceToDevice, c->stream));
   return dgpu_synchronize(c);
 }
 

@@ -60,6 +60,21 @@ __device__ __forceinline__ double wrap_pm(double dp, int *err) {
   return dp;
 }
 
+// while (x - y > h) y += p; while (x - y < -h) y -= p;  (bounded: the RK phase
+// adjustments of cell_update_phi and gravMass_update_RK)
+__device__ __forceinline__ double adjust_toward(double x, double y, double h, double per, int *err) {
+  int it = 0;
+  while (x - y > h) {
+    y += per;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return y; }
+  }
+  while (x - y < -h) {
+    y -= per;
+    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return y; }
+  }
+  return y;
+}
+
 // pow with the two exponents the reference's point-mass force uses exactly
 // (PHI_ORDER = 2: r^1 and r^2), whose correctly rounded values are x and x*x.
 __device__ __forceinline__ double dpow(double x, double y) {
@@ -463,10 +478,8 @@ __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops
       S.dtkey = (unsigned long long)__double_as_longlong(1.e100);
     }
     for (int p = 0; p < 2; ++p) {
-      double phi = S.gphi[p];
-      while (phi > 2. * M_PI) phi -= 2. * M_PI;
-      while (phi < 0.0) phi += 2. * M_PI;
-      S.gphi[p] = phi;
+      // gravMass_clean_pi: same loops as cell_clean_pi with 2.*M_PI == PHIMAX
+      S.gphi[p] = wrap_pos(S.gphi[p], d.err);
     }
   }
 
@@ -945,9 +958,9 @@ __device__ __forceinline__ double fgrav(double M, double r, double eps, int n) {
 }
 
 // Advanced phi edge of a cell (cell_update_phi, src/Cell/cell_misc.c:59-79).
-__device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, double w_total, double dt, double r) {
-  while (tw - rk > PHIMAX / 2.) rk += PHIMAX;
-  while (tw - rk < -PHIMAX / 2.) rk -= PHIMAX;
+__device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, double w_total, double dt, double r,
+                                           int *err) {
+  rk = adjust_toward(tw, rk, PHIMAX / 2., PHIMAX, err);
   double t = (1.0 - RK) * tw + RK * rk;
   t += w_total * dt / r;
   return t;
@@ -1184,8 +1197,8 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
       const int gm1 = j == 0 ? A.cell_off + np - 1 : g - 1;
       double rk = substep == 1 ? tin[g] : d.rktiph[g];
       double rkm = substep == 1 ? tin[gm1] : d.rktiph[gm1];
-      double tn = new_tiph(tw, rk, RK, w_total, dt, r);
-      double tnm = new_tiph(d.tiphw[gm1], rkm, RK, w_total, dt, r);
+      double tn = new_tiph(tw, rk, RK, w_total, dt, r, d.err);
+      double tnm = new_tiph(d.tiphw[gm1], rkm, RK, w_total, dt, r, d.err);
       if (substep == 1) d.rktiph[g] = rk;
       double dphi_n = tn - tnm;
       dphi_n = wrap_pos(dphi_n, d.err);
@@ -1301,8 +1314,7 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
       S.mdot[1] = s1;
     }
     for (int p = 0; p < 2; ++p) {
-      while (S.gphi[p] - S.grk_phi[p] > M_PI) S.grk_phi[p] += 2. * M_PI;
-      while (S.gphi[p] - S.grk_phi[p] < -M_PI) S.grk_phi[p] -= 2. * M_PI;
+      S.grk_phi[p] = adjust_toward(S.gphi[p], S.grk_phi[p], M_PI, 2. * M_PI, d.err);
       S.gr[p] = (1.0 - RK) * S.gr[p] + RK * S.grk_r[p];
       S.gphi[p] = (1.0 - RK) * S.gphi[p] + RK * S.grk_phi[p];
       S.gM[p] = (1.0 - RK) * S.gM[p] + RK * S.grk_M[p];

@@ -45,6 +45,7 @@ SIGNATURES = {
     "dgpu_set_time": (_I, [_P, _I, _D]),
     "dgpu_step_rk2": (_I, [_P, _I]),
     "dgpu_synchronize": (_I, [_P]),
+    "dgpu_step_rk2_timed": (_I, [_P, _I, _dp]),
     "dgpu_stage": (_I, [_P, _I]),
     "dgpu_get_stage_data": (_I, [_P, _I, _dp, _dp, _dp, _dp, _dp]),
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
@@ -211,6 +212,16 @@ class Context:
         self._ck(load().dgpu_step_rk2(self._h, nsteps))
         if sync:
             self.synchronize()
+
+    def step_timed(self, nsteps: int = 1) -> np.ndarray:
+        """Per-kernel device milliseconds summed over nsteps (8 kernels per step)."""
+        ms = np.zeros(8)
+        self._ck(load().dgpu_step_rk2_timed(self._h, nsteps, _dptr(ms)))
+        return ms
+
+    @property
+    def handle(self):
+        return self._h
 
     def synchronize(self):
         self._ck(load().dgpu_synchronize(self._h))

@@ -107,6 +107,11 @@ int dgpu_set_time(dgpu_ctx *ctx, int inst, double t);
  * surface at the next dgpu_synchronize (or any dgpu_get_*). */
 int dgpu_step_rk2(dgpu_ctx *ctx, int nsteps);
 int dgpu_synchronize(dgpu_ctx *ctx);
+/* The same steps launched one kernel at a time with CUDA events between the
+ * kernels on the context's stream (no graph); adds each kernel's device time in
+ * milliseconds to kernel_ms[8] (face, plm_r, flux, update of substep 1, then
+ * of substep 2).  Synchronous.  For measurement only. */
+int dgpu_step_rk2_timed(dgpu_ctx *ctx, int nsteps, double *kernel_ms);
 /* Stage parity: the prologue of timestep_rk2 and the first substep
  * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`
  * (0 faces/clean_pi/set_w/RK blend, 1 PLM, 2 phi fluxes, 3 r fluxes,

@@ -27,6 +27,7 @@ def build(ref: bool | None = None, port: bool = True) -> None:
     which exist only where they were mounted; the restatement builds anywhere."""
     if ref is None:
         ref = os.path.isdir(REFSRC)
+    port = port and os.path.exists(os.path.join(HERE, "port", "disco_port.c"))
     targets = (["ref"] if ref else []) + (["port"] if port else [])
     if targets:
         subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)

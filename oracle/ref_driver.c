@@ -9,12 +9,14 @@
  * calc_cons) without IO or Diagnostics.  Then:
  *
  *   disco_ref run <par> <nsteps> <out.bin> [--load in.bin] [--faces f.bin]
- *                 [--dtlog log.txt]
+ *                 [--dtlog log.txt] [--warmup W]
  *       loops timestep_rk2 (src/TimeStep/timestep_algorithm.c:11-41) nsteps
  *       times and dumps the final state.  --load replaces prim/tiph/dphi after
  *       the initial data (then calc_cons); --faces dumps the r-face list
  *       (face_create, src/Face/face_create_destroy.c:130-193) of the initial
- *       state; --dtlog writes "t dt" per step.
+ *       state; --dtlog writes "t dt" per step.  The wall time of the step
+ *       loop alone goes to stderr as "steps_wall_s <seconds>"; --warmup runs W
+ *       untimed steps first (not dumped).
  *
  *   disco_ref stage <par> <phase> <out.bin> [--load in.bin]
  *       runs the prologue of timestep_rk2 and then the body of
@@ -39,6 +41,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include "Headers/Cell.h"
 #include "Headers/Face.h"
 #include "Headers/GravMass.h"
@@ -223,7 +226,7 @@ out:
 
 int main(int argc, char **argv) {
   const char *mode, *par, *out, *load = NULL, *faces = NULL, *dtlog = NULL;
-  int nsteps, a, step;
+  int nsteps, a, step, warmup = 0;
   char parbuf[1024];
   struct MPIsetup *mpi;
   struct Sim *s;
@@ -243,6 +246,7 @@ int main(int argc, char **argv) {
     if (!strcmp(argv[a], "--load") && a + 1 < argc) load = argv[++a];
     else if (!strcmp(argv[a], "--faces") && a + 1 < argc) faces = argv[++a];
     else if (!strcmp(argv[a], "--dtlog") && a + 1 < argc) dtlog = argv[++a];
+    else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = atoi(argv[++a]);
     else {
       fprintf(stderr, "unknown option %s\n", argv[a]);
       return 2;
@@ -287,11 +291,16 @@ int main(int argc, char **argv) {
 
   if (!strcmp(mode, "run")) {
     if (faces) dump_faces(faces, s, cells, ts);
+    struct timespec t0, t1;
     if (dtlog) flog = fopen(dtlog, "w");
+    for (step = 0; step < warmup; ++step) timestep_rk2(ts, s, cells, gm, mpi);
+    clock_gettime(CLOCK_MONOTONIC, &t0);
     for (step = 0; step < nsteps; ++step) {
       timestep_rk2(ts, s, cells, gm, mpi);
       if (flog) fprintf(flog, "%.17g %.17g\n", ts->t, ts->dt);
     }
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    fprintf(stderr, "steps_wall_s %.9f\n", (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec));
     if (flog) fclose(flog);
     dump_state(out, s, cells, gm, ts, 0);
   } else if (!strcmp(mode, "stage")) {

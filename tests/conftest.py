@@ -1,0 +1,45 @@
+"""Shared test set-up: the `gpu` marker, import paths and the golden fixtures.
+
+Tests marked gpu run the CUDA path on a B200 and compare it with the oracle's
+golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py from
+the reference build).  Everything else runs on CPU.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+CASES = ("gresho16", "kepler24", "cbd32")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
+
+
+def golden(name: str) -> dict:
+    with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(params=CASES)
+def case(request):
+    return request.param, golden(request.param)
+
+
+def l1_rel(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.abs(b).sum()
+    return float(np.abs(a - b).sum() / den) if den > 0 else float(np.abs(a - b).sum())
+
+
+def max_rel(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.maximum(np.abs(b), np.abs(b).max() * 1e-3 + 1e-300)
+    return float((np.abs(a - b) / scale).max()) if a.size else 0.0

@@ -1,0 +1,147 @@
+"""Generate the golden fixtures of tests/golden/ from the reference build.
+
+Run where the reference sources are mounted (oracle/_ref/disco_ref is built
+from them by oracle/Makefile):
+
+    python tests/golden/make_golden.py
+
+Every fixture is the reference's own output (timestep_rk2 / face_create /
+the substep phases of timestep_substep) on a small disk, stored as a
+compressed .npz.  The reference has no tests or golden data of its own, so
+these are the pins of the oracle and of the GPU path.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle  # noqa: E402
+from disco2_b200 import configs  # noqa: E402
+
+# name -> parameter dict of a small disk of each workload
+CASES = {
+    "gresho16": configs.gresho(num_r=16),
+    "kepler24": configs.kepler_ring(num_r=24),
+    "cbd32": configs.circumbinary(num_r=32),
+}
+STEPS = (1, 5, 100)
+PHASES = (0, 1, 2, 3, 4, 5, 6, 7)
+# per phase, the arrays that phase of timestep_substep changes
+PHASE_KEYS = {0: ("cons", "wiph", "RKcons"), 1: ("grad", "gradp"), 2: ("cons",), 3: ("cons",),
+              4: ("cons",), 5: ("prim", "tiph", "dphi", "RKtiph"), 6: ("prim",),
+              7: ("prim", "cons")}
+
+
+def _state_dict(st: oracle.State, prefix: str, ext: bool = False) -> dict:
+    d = {f"{prefix}prim": st.prim, f"{prefix}cons": st.cons, f"{prefix}tiph": st.tiph,
+         f"{prefix}dphi": st.dphi, f"{prefix}gm": st.gm, f"{prefix}t": np.float64(st.t),
+         f"{prefix}dt": np.float64(st.dt)}
+    if ext:
+        for k, v in st.ext.items():
+            d[f"{prefix}{k}"] = v
+    return d
+
+
+def _faces_dict(fc: oracle.Faces, prefix: str, full: bool = True) -> dict:
+    keys = ("nri", "L", "R", "r", "dphi", "dA", "deltaL", "deltaR", "cm") if full else \
+        ("nri", "L", "R", "dphi", "dA", "cm")
+    return {f"{prefix}{k}": getattr(fc, k) for k in keys}
+
+
+def face_cases(par: str, st0: oracle.State, rng: np.random.Generator) -> dict:
+    """Face lists of perturbed phi-edge layouts: random rotations, exactly aligned
+    edges, edges given far outside [0, 2pi] (the wrap loops), jittered cells."""
+    out = {}
+    off = st0.cell_off
+    layouts = {}
+    # 1. a random rotation per annulus
+    t = st0.tiph.copy()
+    d = st0.dphi.copy()
+    for i in range(st0.NR):
+        a, b = off[i], off[i + 1]
+        n = b - a
+        dp = 2 * np.pi / n
+        t[a:b] = rng.uniform(0, 2 * np.pi) + np.arange(n) * dp
+        d[a:b] = dp
+    layouts["rot"] = (t.copy(), d.copy())
+    # 2. all annuli start at phi = 0: inner and outer edges coincide exactly where
+    #    j/N_i == k/N_o
+    t2 = t.copy()
+    for i in range(st0.NR):
+        a, b = off[i], off[i + 1]
+        n = b - a
+        t2[a:b] = np.arange(1, n + 1) * (2 * np.pi / n)
+    layouts["aligned"] = (t2, d.copy())
+    # 3. the rotated layout shifted by whole turns (the reference wraps on the fly)
+    t3 = t + 2 * np.pi * rng.integers(-3, 4, size=t.size)
+    layouts["turns"] = (t3, d.copy())
+    # 4. jittered cell widths (sliding mesh after many steps): edges perturbed, dphi
+    #    recomputed as cell_update_dphi does
+    t4 = t.copy()
+    d4 = d.copy()
+    for i in range(st0.NR):
+        a, b = off[i], off[i + 1]
+        n = b - a
+        dp = 2 * np.pi / n
+        t4[a:b] += rng.uniform(-0.3, 0.3, size=n) * dp
+        for j in range(n):
+            jm = j - 1 if j > 0 else n - 1
+            x = t4[a + j] - t4[a + jm]
+            while x > 2 * np.pi:
+                x -= 2 * np.pi
+            while x < 0.0:
+                x += 2 * np.pi
+            d4[a + j] = x
+    layouts["jitter"] = (t4, d4)
+    for name, (tt, dd) in layouts.items():
+        st = oracle.State(st0.NR, st0.NZ, st0.NQ, st0.N, 0.0, 0.0, st0.gm, st0.N_p, st0.r_faces,
+                          st0.prim, st0.cons, tt, dd)
+        _, fc, _ = oracle.run(par, 0, load=st, faces=True)
+        out[f"layout_{name}_tiph"] = tt
+        out[f"layout_{name}_dphi"] = dd
+        out.update(_faces_dict(fc, f"layout_{name}_face_", full=False))
+    return out
+
+
+def main() -> None:
+    if not oracle.have_ref():
+        oracle.build(ref=True, port=False)
+    rng = np.random.default_rng(20251203)
+    with tempfile.TemporaryDirectory() as td:
+        for name, p in CASES.items():
+            par = configs.write_parfile(p, os.path.join(td, name + ".par"))
+            data = {"parfile": np.array(configs.parfile_text(p))}
+            st0, fc0, _ = oracle.run(par, 0, faces=True)
+            data.update(_state_dict(st0, "init_"))
+            data["N_p"] = st0.N_p
+            data["r_faces"] = st0.r_faces
+            data.update(_faces_dict(fc0, "init_face_"))
+            for n in STEPS:
+                st, _, log = oracle.run(par, n, dtlog=True)
+                data.update(_state_dict(st, f"step{n}_"))
+                data[f"step{n}_dtlog"] = log
+            # stage phases of one substep from the 5-step state (loaded: prim, tiph,
+            # dphi; t = 0 and the initial GravMass)
+            st5 = oracle.run(par, 5)[0]
+            for ph in PHASES:
+                st = oracle.stage(par, ph, load=st5)
+                full = _state_dict(st, "", ext=True)
+                for k in PHASE_KEYS[ph]:
+                    data[f"stage{ph}_{k}"] = full[k]
+                data[f"stage{ph}_dt"] = np.float64(st.dt)
+                data[f"stage{ph}_gm"] = st.gm
+            data.update(face_cases(par, st0, rng))
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+            print(name, st0.N, "cells", os.path.getsize(os.path.join(HERE, name + ".npz")), "bytes")
+
+
+if __name__ == "__main__":
+    main()
