@@ -1489,3 +1489,306 @@ int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Face list without allocation (dgpu_face_list_noalloc).
+//
+// For callers that cannot allocate device memory: the face list of one disk is
+// built from the caller's device arrays into the caller's device arrays, and
+// the only working memory is g_noalloc_scratch below, a fixed static array
+// that every GPU loading this library holds until the process exits.  Per
+// annulus pair it keeps only counts and offsets, so its size is set by the
+// number of annuli (DGPU_NOALLOC_MAX_ANNULI), not by the number of cells.
+// ---------------------------------------------------------------------------
+extern "C" {
+#include "dgpu_sim.h"
+}
+
+#define NOALLOC_MAXA DGPU_NOALLOC_MAX_ANNULI
+
+struct NoallocScratch {
+  int np[NOALLOC_MAXA];        // N_p per annulus
+  int off[NOALLOC_MAXA];       // first cell of each annulus
+  int cnt[NOALLOC_MAXA];       // faces per pair
+  int base[NOALLOC_MAXA + 1];  // first face of each pair; base[NR-1] = total
+  double rface[NOALLOC_MAXA + 1];
+  double dperp;
+  int err;                     // DGPU_EF_* flags of this call
+  int total;
+  int fill_ok;                 // written only by k_noalloc_offsets: 1 when total <= cap
+};
+static_assert(sizeof(NoallocScratch) <= DGPU_NOALLOC_SCRATCH_BYTES, "scratch too small");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DGPU_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+__global__ void k_noalloc_setup(NoallocScratch *S, int NR) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int o = 0;
+  for (int i = 0; i < NR; ++i) {
+    S->off[i] = o;
+    o += S->np[i];
+  }
+  S->err = 0;
+  S->total = 0;
+  S->fill_ok = 0;
+}
+
+// Chunk start, count and verification of one pair; the same decisions as k_face.
+struct PairPlan {
+  int jpmin, jp_start, j0, j1, cnt, sequential;
+};
+
+__device__ PairPlan noalloc_plan(const FaceCtx &c, int *sh_i, int *sh_j, double *sh_v, int *sh_flag) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int np = c.Nin;
+  const double p0 = c.tin[np - 1];
+  PairPlan pl;
+  double bv = PHIMAX;
+  int bi = 0;
+  for (int jp = tid; jp < c.Nout; jp += nt) {
+    double dp = wrap_pos(c.tout[jp] - p0, c.err);
+    if (dp < bv || (dp == bv && jp < bi)) {
+      bv = dp;
+      bi = jp;
+    }
+  }
+  sh_v[tid] = bv;
+  sh_i[tid] = bi;
+  __syncthreads();
+  for (int o = nt / 2; o > 0; o >>= 1) {
+    if (tid < o) {
+      double v2 = sh_v[tid + o];
+      int i2 = sh_i[tid + o];
+      if (v2 < sh_v[tid] || (v2 == sh_v[tid] && i2 < sh_i[tid])) {
+        sh_v[tid] = v2;
+        sh_i[tid] = i2;
+      }
+    }
+    __syncthreads();
+  }
+  pl.jpmin = sh_i[0];
+  __syncthreads();
+  const int chunk = (np + nt - 1) / nt;
+  pl.j0 = min(np, tid * chunk);
+  pl.j1 = min(np, pl.j0 + chunk);
+  pl.jp_start = pl.jpmin;
+  if (pl.j0 > 0 && pl.j0 < np) {
+    double L = wrap_pos(c.tin[pl.j0 - 1] - p0, c.err);
+    int lo = 0, hi = c.Nout;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      int k = pl.jpmin + mid;
+      if (k >= c.Nout) k -= c.Nout;
+      double e = wrap_pos(c.tout[k] - p0, c.err);
+      if (e < L) lo = mid + 1;
+      else hi = mid;
+    }
+    pl.jp_start = pl.jpmin + lo;
+    if (pl.jp_start >= c.Nout) pl.jp_start -= c.Nout;
+  }
+  int jp = pl.jp_start, n = 0, s = 0;
+  for (int j = pl.j0; j < pl.j1; ++j) face_cell<false>(c, j, jp, n, s);
+  pl.cnt = n;
+  if (tid == 0) *sh_flag = 0;
+  sh_j[tid] = (pl.j0 < pl.j1) ? pl.jp_start : -1;
+  __syncthreads();
+  if (pl.j0 < pl.j1 && tid + 1 < nt && sh_j[tid + 1] >= 0 && sh_j[tid + 1] != jp) *sh_flag = 1;
+  __syncthreads();
+  pl.sequential = *sh_flag;
+  __syncthreads();
+  return pl;
+}
+
+__device__ FaceCtx noalloc_ctx(const NoallocScratch *S, int i, const double *tiph, const double *dphi,
+                               int *err) {
+  FaceCtx c;
+  c.tin = tiph + S->off[i];
+  c.din = dphi + S->off[i];
+  c.tout = tiph + S->off[i + 1];
+  c.dout = dphi + S->off[i + 1];
+  c.Nin = S->np[i];
+  c.Nout = S->np[i + 1];
+  c.fL = c.fR = nullptr;
+  c.fdphi = c.fcm = nullptr;
+  c.runs = c.fstart = nullptr;
+  c.cap = c.rcap = 0;
+  c.err = err;
+  return c;
+}
+
+__global__ void __launch_bounds__(BLK) k_noalloc_count(NoallocScratch *S, const double *tiph,
+                                                       const double *dphi) {
+  __shared__ int sh_i[BLK];
+  __shared__ int sh_j[BLK];
+  __shared__ double sh_v[BLK];
+  __shared__ int sh_flag;
+  const int i = blockIdx.x;
+  FaceCtx c = noalloc_ctx(S, i, tiph, dphi, &S->err);
+  PairPlan pl = noalloc_plan(c, sh_i, sh_j, sh_v, &sh_flag);
+  if (!pl.sequential) {
+    int tot;
+    block_excl_scan<int>(pl.cnt, sh_i, tot);
+    if (threadIdx.x == 0) S->cnt[i] = tot;
+  } else if (threadIdx.x == 0) {
+    int jp = pl.jpmin, n = 0, s = 0;
+    for (int j = 0; j < c.Nin; ++j) face_cell<false>(c, j, jp, n, s);
+    S->cnt[i] = n;
+  }
+}
+
+__global__ void k_noalloc_offsets(NoallocScratch *S, int NR, int cap, int *nri) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int o = 0;
+  for (int i = 0; i < NR - 1; ++i) {
+    S->base[i] = o;
+    nri[i] = o;
+    o += S->cnt[i];
+  }
+  S->base[NR - 1] = o;
+  nri[NR - 1] = o;
+  S->total = o;
+  S->fill_ok = o <= cap ? 1 : 0;
+  if (o > cap) S->err |= DGPU_EF_FACE_OVERFLOW;
+}
+
+// One inner cell of build_jloop writing the reference's face records
+// (addFace, face_create_destroy.c:11-20) straight into the caller's arrays.
+struct NoallocOut {
+  int *L, *R;
+  double *dphi, *dA, *cm;
+  int offL, offR;
+  int limit;                   // faces this pair may write (its count)
+  double r, dperp;
+  int *err;
+};
+
+__device__ void noalloc_cell(const FaceCtx &c, const NoallocOut &o, int j, int &jp, int &n) {
+  int jm = j - 1;
+  if (jm < 0) jm = c.Nin - 1;
+  auto emit = [&](double dphi, double tp) {
+    if (n >= 0 && n < o.limit) {
+      o.L[n] = o.offL + j;
+      o.R[n] = o.offR + jp;
+      o.dphi[n] = dphi;
+      o.dA[n] = o.r * dphi * o.dperp;
+      o.cm[n] = tp - .5 * dphi;
+    } else {
+      set_err(o.err, DGPU_EF_FACE_OVERFLOW);
+    }
+    ++n;
+  };
+  double dp = c.tout[jp] - c.tin[jm];
+  dp = wrap_pos(dp, c.err);
+  if (c.din[j] < dp) {
+    emit(c.din[j], c.tin[j]);
+    return;
+  }
+  emit(dp, c.tout[jp]);
+  ++jp;
+  if (jp == c.Nout) jp = 0;
+  dp = c.tin[j] - c.tout[jp];
+  dp = wrap_pm(dp, c.err);
+  int guard = 0;
+  while (dp > 0.0) {
+    emit(c.dout[jp], c.tout[jp]);
+    ++jp;
+    if (jp == c.Nout) jp = 0;
+    dp = c.tin[j] - c.tout[jp];
+    dp = wrap_pm(dp, c.err);
+    if (++guard > c.Nout + 2) {
+      set_err(c.err, DGPU_EF_FACE_OVERFLOW);
+      break;
+    }
+  }
+  dp = c.dout[jp] + dp;
+  emit(dp, c.tin[j]);
+}
+
+__global__ void __launch_bounds__(BLK) k_noalloc_fill(NoallocScratch *S, const double *tiph, const double *dphi,
+                                                      int *L, int *R, double *fdphi, double *fdA,
+                                                      double *fcm) {
+  __shared__ int sh_i[BLK];
+  __shared__ int sh_j[BLK];
+  __shared__ double sh_v[BLK];
+  __shared__ int sh_flag;
+  // fill_ok, base, cnt and total were written by the earlier kernels and are
+  // only read here, so these early exits are uniform across the block
+  if (!S->fill_ok) return;
+  const int i = blockIdx.x;
+  const int b = S->base[i];
+  if (b < 0 || S->cnt[i] < 0 || b + S->cnt[i] > S->total) return;
+  FaceCtx c = noalloc_ctx(S, i, tiph, dphi, &S->err);
+  PairPlan pl = noalloc_plan(c, sh_i, sh_j, sh_v, &sh_flag);
+  NoallocOut o;
+  o.L = L + b;
+  o.R = R + b;
+  o.dphi = fdphi + b;
+  o.dA = fdA + b;
+  o.cm = fcm + b;
+  o.offL = S->off[i];
+  o.offR = S->off[i + 1];
+  o.limit = S->cnt[i];
+  o.r = S->rface[i + 1];
+  o.dperp = S->dperp;
+  o.err = &S->err;
+  if (!pl.sequential) {
+    int tot;
+    int fo = block_excl_scan<int>(pl.cnt, sh_i, tot);
+    if (tot != S->cnt[i]) {
+      if (threadIdx.x == 0) set_err(&S->err, DGPU_EF_FACE_OVERFLOW);
+      return;
+    }
+    int jp = pl.jp_start, n = fo;
+    for (int j = pl.j0; j < pl.j1; ++j) noalloc_cell(c, o, j, jp, n);
+  } else if (threadIdx.x == 0) {
+    int jp = pl.jpmin, n = 0;
+    for (int j = 0; j < c.Nin; ++j) noalloc_cell(c, o, j, jp, n);
+  }
+}
+
+}  // namespace
+
+// Device address of the scratch array, looked up once per device (on the first
+// call made with that device current).
+static void *g_noalloc_ptr[64];
+
+extern "C" __attribute__((visibility("default"))) int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double *dphi, int cap,
+                                      int *nri, int *L, int *R, double *fdphi, double *fdA, double *fcm,
+                                      int *nf, void *stream) {
+  int dev = -1;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!sim || !tiph || !dphi || !nri || !L || !R || !fdphi || !fdA || !fcm || !nf || cap < 0)
+    return DGPU_ERR_ARG;
+  const int NR = sim->NR;
+  if (NR > NOALLOC_MAXA || NR < 3) return DGPU_ERR_ARG;  // more annuli than the static scratch holds
+  if (sim->NumZ != 1) return DGPU_ERR_UNSUPPORTED;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DGPU_ERR_CUDA;
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DGPU_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  NoallocScratch *S = (NoallocScratch *)g_noalloc_ptr[dev];
+  const double dperp = dsim_zface(sim, 0) - dsim_zface(sim, -1);
+  if (cudaMemcpyAsync(S->np, sim->N_p, sizeof(int) * (size_t)NR, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(S->rface, sim->r_faces, sizeof(double) * (size_t)(NR + 1), cudaMemcpyHostToDevice, st) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(&S->dperp, &dperp, sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return DGPU_ERR_CUDA;
+  k_noalloc_setup<<<1, 1, 0, st>>>(S, NR);
+  k_noalloc_count<<<NR - 1, BLK, 0, st>>>(S, tiph, dphi);
+  k_noalloc_offsets<<<1, 1, 0, st>>>(S, NR, cap, nri);
+  k_noalloc_fill<<<NR - 1, BLK, 0, st>>>(S, tiph, dphi, L, R, fdphi, fdA, fcm);
+  if (cudaGetLastError() != cudaSuccess) return DGPU_ERR_CUDA;
+  int res[2] = {0, 0};
+  if (cudaMemcpyAsync(&res[0], &S->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(&res[1], &S->total, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return DGPU_ERR_CUDA;
+  *nf = res[1];
+  if (res[0] & DGPU_EF_FACE_OVERFLOW) return res[1] > cap ? DGPU_ERR_ARG : DGPU_ERR_FACE_OVERFLOW;
+  if (res[0]) return DGPU_ERR_NUMERIC;
+  return DGPU_OK;
+}

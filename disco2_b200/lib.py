@@ -50,6 +50,7 @@ SIGNATURES = {
     "dgpu_get_stage_data": (_I, [_P, _I, _dp, _dp, _dp, _dp, _dp]),
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
     "dgpu_torque": (_I, [_P, _I, _dp]),
+    "dgpu_face_list_noalloc": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _ip, _P]),
 }
 
 _lib = None

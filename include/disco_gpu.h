@@ -134,6 +134,30 @@ int dgpu_face_list(dgpu_ctx *ctx, int inst, int cap, int *nri, int *L, int *R, d
                    double *dphi, double *dA, double *deltaL, double *deltaR, double *cm,
                    int *nf);
 
+/* ---- Face list without allocation ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- code running inside another framework's memory pool or a
+ * pre-sized arena, or a service that must not grow its footprint after start-up
+ * -- this builds the same r-face list as dgpu_face_list for one disk, reading
+ * the phi edges tiph[N] and widths dphi[N] from the caller's device memory and
+ * writing nri[NR], L, R, dphi, dA, cm (cap entries each) to the caller's device
+ * memory.  Cell numbers are in the disk's (k, i, j) order.  It calls no
+ * cudaMalloc/cudaFree or other allocating routine: its working memory is one
+ * static device array of DGPU_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library keeps until the process exits, sized for at most
+ * DGPU_NOALLOC_MAX_ANNULI annuli (any number of cells); larger grids return
+ * DGPU_ERR_ARG, as does a face count above cap (*nf then holds the count).
+ * The first call on a device looks up that array's device address (with the
+ * caller's current device), so make the first call before any stream capture.
+ * Every call reuses the same array, so calls that overlap on the GPU (other
+ * streams or threads) race; serialise them.  Synchronous: returns after the
+ * list is complete. */
+#define DGPU_NOALLOC_MAX_ANNULI 4096
+#define DGPU_NOALLOC_SCRATCH_BYTES (128 * 1024)
+int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double *dphi, int cap,
+                           int *nri, int *L, int *R, double *dphi_out, double *dA, double *cm,
+                           int *nf, void *stream);
+
 /* ---- Objective -----------------------------------------------------------------
  * Gravitational torque on the binary from the gas, T = sum over non-ghost cells
  * of r * rho * dV * F_phi(r, phi) with F_phi the azimuthal point-mass force of
