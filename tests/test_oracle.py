@@ -1,0 +1,73 @@
+"""The oracle is pinned to the reference's own outputs (tests/golden).
+
+Both halves must reproduce the golden fixtures bit for bit on the host:
+  - the reference build (oracle/_ref, compiled from the unmodified reference
+    sources), where it exists -- a check that the fixtures are current;
+  - the C restatement (oracle/port), everywhere -- the portable oracle.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import CASES, golden
+import oracle
+
+IMPLS = ["port"] + (["ref"] if oracle.have_ref() else [])
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    if not oracle.have_port():
+        oracle.build(ref=False, port=True)
+    assert oracle.have_port()
+
+
+def _par(g, td):
+    path = os.path.join(td, "case.par")
+    with open(path, "w") as f:
+        f.write(str(g["parfile"]))
+    return path
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_steps_and_faces_match_reference(impl, name):
+    g = golden(name)
+    with tempfile.TemporaryDirectory() as td:
+        par = _par(g, td)
+        st0, fc, _ = oracle.run(par, 0, impl=impl, faces=True)
+        for k in ("prim", "cons", "tiph", "dphi"):
+            assert np.array_equal(getattr(st0, k), g["init_" + k]), k
+        for k in ("nri", "L", "R", "r", "dphi", "dA", "deltaL", "deltaR", "cm"):
+            assert np.array_equal(getattr(fc, k), g["init_face_" + k]), k
+        for n in (5, 100):
+            st, _, log = oracle.run(par, n, impl=impl, dtlog=True)
+            for k in ("prim", "cons", "tiph", "dphi"):
+                assert np.array_equal(getattr(st, k), g[f"step{n}_" + k]), (n, k)
+            assert np.array_equal(st.gm, g[f"step{n}_gm"])
+            assert np.array_equal(log, g[f"step{n}_dtlog"])
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_phases_and_layouts_match_reference(impl, name):
+    g = golden(name)
+    keys = {0: ("cons", "wiph", "RKcons"), 1: ("grad", "gradp"), 2: ("cons",), 3: ("cons",),
+            4: ("cons",), 5: ("prim", "tiph", "dphi", "RKtiph"), 6: ("prim",), 7: ("prim", "cons")}
+    with tempfile.TemporaryDirectory() as td:
+        par = _par(g, td)
+        st5 = oracle.run(par, 5, impl=impl)[0]
+        for ph, ks in keys.items():
+            st = oracle.stage(par, ph, impl=impl, load=st5)
+            full = {"prim": st.prim, "cons": st.cons, "tiph": st.tiph, "dphi": st.dphi, **st.ext}
+            for k in ks:
+                assert np.array_equal(full[k], g[f"stage{ph}_{k}"]), (ph, k)
+        st0 = oracle.run(par, 0, impl=impl)[0]
+        for lay in ("rot", "aligned", "turns", "jitter"):
+            st0.tiph = g[f"layout_{lay}_tiph"]
+            st0.dphi = g[f"layout_{lay}_dphi"]
+            _, fc, _ = oracle.run(par, 0, impl=impl, load=st0, faces=True)
+            for k in ("nri", "L", "R", "dphi", "dA", "cm"):
+                assert np.array_equal(getattr(fc, k), g[f"layout_{lay}_face_{k}"]), (lay, k)
