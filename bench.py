@@ -36,12 +36,13 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Compulsory DRAM bytes per unit for each kernel as designed (each array
 # element touched once): per cell and per r-face of one substep.
-KERNELS = ["face", "plm_r", "flux", "update"]
+KERNELS = ["face", "rslope", "plm_r", "flux", "update"]
 ALG_BYTES = {
     # name: (bytes per cell, bytes per r-face)
     "face": (8 + 8 + 40 + 8 + 40 + 4 + 4, 24),
-    "plm_r": (40 + 40 + 8 + 8 + 4 + 40, 24),
-    "flux": (40 + 40 + 40 + 8 + 8 + 64, 24 + 64),
+    "rslope": (40 + 40 + 8 + 8, 24 + 40 + 16),
+    "plm_r": (8 + 4 + 40, 24 + 40),
+    "flux": (40 + 40 + 40 + 8 + 8 + 64, 24 + 16 + 64),
     "update": (40 + 40 + 40 + 8 + 8 + 8 + 8 + 16 + 64 + 8 + 40 + 40 + 8 + 8 + 8, 64),
 }
 STEP_ALG_BYTES = 240  # per zone-update: 5 conserved + 1 phi edge, read/written across 2 stages
@@ -273,7 +274,7 @@ def main():
     value = nin * args.steps * world / (ms / 1e3)
 
     # per-kernel device times (same steps launched kernel by kernel, L2 flushed between steps)
-    kern = [0.0] * 8
+    kern = [0.0] * (2 * len(KERNELS))
     nprof = max(3, min(args.steps, 50))
     for k in range(nprof):
         with torch.cuda.stream(stream):
@@ -282,8 +283,9 @@ def main():
         km = ctx.step_timed(1)
         kern = [a + b for a, b in zip(kern, km)]
     per_kernel = {}
+    nk = len(KERNELS)
     for i, nm in enumerate(KERNELS):
-        per_kernel[nm] = (kern[i] + kern[4 + i]) / (2 * nprof)  # ms per launch
+        per_kernel[nm] = (kern[i] + kern[nk + i]) / (2 * nprof)  # ms per launch
     dom = max(per_kernel, key=per_kernel.get)
     # units: cells and r-faces of one substep
     fl = ctx.face_list(0)
@@ -348,7 +350,7 @@ def main():
                               "achieved_gbs": value / world * STEP_ALG_BYTES / 1e9,
                               "frac": value / world * STEP_ALG_BYTES / 1e9 / peak},
             "kernel_ms": per_kernel,
-            "gpu_launches": 8 * args.steps,
+            "gpu_launches": 2 * len(KERNELS) * args.steps,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": ke, "how": "dgpu_set_state from pinned host prim/tiph/dphi, "
                                         "dgpu_step_rk2(1), dgpu_get_state to pinned host, per step"},

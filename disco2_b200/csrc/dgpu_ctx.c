@@ -227,7 +227,7 @@ void dgpu_destroy(dgpu_ctx *c) {
   {
     void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
-                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
+                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
                   c->d.mdot_part, c->d.counters, c->d.err, c->d_stage, c->d_torque};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
@@ -353,6 +353,9 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.w_ann = (double *)dmalloc(sizeof(double) * A, &ok);
     c->d.fphi = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
     c->d.frf = (double *)dmalloc(sizeof(double) * 8 * (S ? S : 1), &ok);
+    c->d.fS = (double *)dmalloc(sizeof(double) * 5 * (S ? S : 1), &ok);
+    c->d.fdp = (double *)dmalloc(sizeof(double) * 2 * (S ? S : 1), &ok);
+    c->d.ann_c = (double *)dmalloc(sizeof(double) * 4 * A, &ok);
     c->d.fstart = (int *)dmalloc(sizeof(int) * N, &ok);
     c->d.fL = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
     c->d.fR = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
@@ -374,6 +377,16 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     free(h_slot_ann);
     dgpu_destroy(c);
     return fail(NULL, DGPU_ERR_NOMEM, "device allocation failed");
+  }
+  {
+    /* k_face stages the phi edges and widths of its annulus pair in shared memory */
+    int a, mx = 0;
+    for (a = 0; a < c->n_ann; ++a) {
+      const Annulus *A = &c->h_ann[a];
+      int m = A->np + (A->face_cap > 0 ? c->h_ann[a + 1].np : 0);
+      if (m > mx) mx = m;
+    }
+    c->d.smem_face = (int)(2 * sizeof(double) * (size_t)mx) <= 48 * 1024 ? (int)(2 * sizeof(double) * (size_t)mx) : 0;
   }
   c->d.n_inst = n;
   c->d.n_ann = c->n_ann;
@@ -620,6 +633,7 @@ static int launch_step(struct dgpu_ctx *c) {
   int sub;
   for (sub = 1; sub <= 2; ++sub) {
     CKK(dgk_face(&c->d, sub, 1, c->stream));
+    CKK(dgk_rslope(&c->d, c->stream));
     CKK(dgk_plm_r(&c->d, sub, c->stream));
     CKK(dgk_flux(&c->d, sub, c->stream));
     CKK(dgk_update(&c->d, sub, 7, c->stream));
@@ -653,16 +667,18 @@ int dgpu_step_rk2(dgpu_ctx *c, int nsteps) {
 }
 
 int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
-  cudaEvent_t ev[9];
+  cudaEvent_t ev[DGPU_STEP_KERNELS + 1];
   int k, s, sub, rc = DGPU_OK;
   if (!c || nsteps < 0 || !kernel_ms) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
-  for (k = 0; k < 9; ++k) CK(cudaEventCreate(&ev[k]));
+  for (k = 0; k <= DGPU_STEP_KERNELS; ++k) CK(cudaEventCreate(&ev[k]));
   for (s = 0; s < nsteps && rc == DGPU_OK; ++s) {
     int e = 0;
     CK(cudaEventRecord(ev[e++], c->stream));
     for (sub = 1; sub <= 2; ++sub) {
       CKK(dgk_face(&c->d, sub, 1, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_rslope(&c->d, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_plm_r(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
@@ -671,14 +687,14 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
       CKK(dgk_update(&c->d, sub, 7, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
     }
-    CK(cudaEventSynchronize(ev[8]));
-    for (k = 0; k < 8; ++k) {
+    CK(cudaEventSynchronize(ev[DGPU_STEP_KERNELS]));
+    for (k = 0; k < DGPU_STEP_KERNELS; ++k) {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
       kernel_ms[k] += (double)ms;
     }
   }
-  for (k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+  for (k = 0; k <= DGPU_STEP_KERNELS; ++k) cudaEventDestroy(ev[k]);
   return read_err(c);
 }
 
@@ -687,6 +703,7 @@ int dgpu_stage(dgpu_ctx *c, int phase) {
   cudaSetDevice(c->device);
   CKK(dgk_face(&c->d, 1, 1, c->stream));
   /* the CFL minimum (and dt) come from k_plm_r; PLM results are kept only from phase 1 on */
+  CKK(dgk_rslope(&c->d, c->stream));
   CKK(dgk_plm_r(&c->d, 1, c->stream));
   if (phase >= 2) CKK(dgk_flux(&c->d, 1, c->stream));
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));

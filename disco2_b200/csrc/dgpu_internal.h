@@ -18,6 +18,7 @@
 #define DGPU_FACE_SLACK 8
 #define DGPU_RUN_SLACK 8
 #define DGPU_WRAP_LIMIT 64
+#define DGPU_STEP_KERNELS 10 /* launches per RK2 step: 5 per substep */
 
 /* enums of src/Headers/header.h:1-13 */
 enum { D_RHO, D_PPP, D_URR, D_UPP, D_UZZ };
@@ -100,6 +101,10 @@ typedef struct {
   double mdot[2], macc[2];
   unsigned long long dtkey;                      /* CFL minimum (bit pattern of a positive double) */
   int pad[2];
+  /* per-substep GravMass trigonometry, computed once per disk:
+     gx = r cos(phi), gy = r sin(phi) of the current positions (after clean_pi),
+     rkx/rky the same for the step-start copies (the CFL reads those) */
+  double gx[2], gy[2], gc[2], gs[2], rkx[2], rky[2];
 } InstState;
 
 /* Device pointers and sizes handed to every kernel. */
@@ -117,6 +122,10 @@ typedef struct {
   double *w_ann;          /* wiph per annulus */
   double *fphi;           /* [8][n_cells] phi-face increments, face (j, j+1) at cell j */
   double *frf;            /* [8][n_slots] r-face increments */
+  double *fS;             /* [5][n_slots] r-face slopes (WR - WL)/(deltaR + deltaL) */
+  double *fdp;            /* [2][n_slots] r-face offsets dpL, dpR (wrapped to [-pi, pi]) */
+  double *ann_c;          /* [4][n_ann] per substep: kappa, cos(kappa dt), sin(kappa dt), 1-exp(-rate dt) */
+  int smem_face;          /* dynamic shared bytes of k_face (0: merge reads global memory) */
   int *fstart;            /* first r-face (within the pair slab) of each inner cell */
   int *fL, *fR;           /* r-face cells (local j of inner / outer annulus) */
   double *fdphi, *fcm;    /* r-face dphi and cm */
@@ -132,6 +141,7 @@ extern "C" {
 #endif
 /* kernel launchers (dgpu_kernels.cu); return cudaError_t as int */
 int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream);
+int dgk_rslope(const DevPtrs *d, void *stream);
 int dgk_plm_r(const DevPtrs *d, int substep, void *stream);
 int dgk_flux(const DevPtrs *d, int substep, void *stream);
 int dgk_update(const DevPtrs *d, int substep, int stop, void *stream);

@@ -75,11 +75,14 @@ __device__ __forceinline__ double adjust_toward(double x, double y, double h, do
   return y;
 }
 
-// pow with the two exponents the reference's point-mass force uses exactly
-// (PHI_ORDER = 2: r^1 and r^2), whose correctly rounded values are x and x*x.
+// pow for the exponents the step uses: x^1 = x and x^2 = x*x are the correctly
+// rounded values; x^1.5 = x*sqrt(x) and x^-1.5 = 1/(x*sqrt(x)) are within 2 ulp
+// (like CUDA's pow, which also differs from the host libm in the last ulp).
 __device__ __forceinline__ double dpow(double x, double y) {
   if (y == 1.0) return x;
   if (y == 2.0) return x * x;
+  if (y == 1.5) return x * sqrt(x);
+  if (y == -1.5) return 1.0 / (x * sqrt(x));
   return pow(x, y);
 }
 
@@ -254,7 +257,8 @@ struct ViscIn {
   double cL[5], cR[5];          // cell prims
   double gpL[5], gpR[5];        // cell gradp
   double grL[5], grR[5];        // cell grad
-  double tL, tR, dL, dR;        // cell tiph (wrapped) and dphi
+  double tL, tR;                // cell tiph (wrapped)
+  double dpL, dpR;              // r faces: wrapped offsets of the face centre (k_rslope)
   double r, cm, r_cell_L, r_cell_R;
   double rdr_om;                // sim_rdrOm_a at r
 };
@@ -270,12 +274,7 @@ __device__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const I
     Gr[q] = .5 * (v.grL[q] + v.grR[q]);
   }
   if (dir == 0) {
-    double pLc = v.tL - .5 * v.dL;
-    double pRc = v.tR - .5 * v.dR;
-    double dpL = v.cm - pLc;
-    double dpR = -v.cm + pRc;
-    dpL = wrap_pm(dpL, err);
-    dpR = wrap_pm(dpR, err);
+    const double dpL = v.dpL, dpR = v.dpR;
     double deltaL = v.r - v.r_cell_L;
     double deltaR = v.r_cell_R - v.r;
 #pragma unroll
@@ -304,7 +303,7 @@ __device__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const I
     double d1 = gm_dist(gx[1], gy[1], r, v.cm);
     double eps = P.g_eps;
     nu = alpha * Avg[D_PPP] / Avg[D_RHO] /
-         sqrt(pow(d0 * d0 + eps * eps, -1.5) * S.gM[0] + pow(d1 * d1 + eps * eps, -1.5) * S.gM[1]);
+         sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.gM[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.gM[1]);
   }
   double rho = Avg[D_RHO];
   double vr = Avg[D_URR];
@@ -394,22 +393,34 @@ __device__ void face_cell(const FaceCtx &c, int j, int &jp, int &n, int &s) {
   emit(dp, c.tin[j]);
 }
 
+// Exclusive scan of one value per thread over the block (blockDim.x a multiple
+// of 32, at most 1024); sh needs blockDim.x / 32 entries.
 template <typename T>
 __device__ T block_excl_scan(T v, T *sh, T &total) {
-  // Hillis-Steele over one value per thread (blockDim.x <= 1024)
-  int t = threadIdx.x;
-  sh[t] = v;
-  __syncthreads();
-  for (int o = 1; o < blockDim.x; o <<= 1) {
-    T x = t >= o ? sh[t - o] : T(0);
-    __syncthreads();
-    sh[t] += x;
-    __syncthreads();
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(full, x, o);
+    if (lane >= o) x += y;
   }
-  T incl = sh[t];
-  total = sh[blockDim.x - 1];
+  if (lane == 31) sh[w] = x;
   __syncthreads();
-  return incl - v;
+  if (w == 0) {
+    T t = lane < nw ? sh[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      T y = __shfl_up_sync(full, t, o);
+      if (lane >= o) t += y;
+    }
+    if (lane < nw) sh[lane] = t;
+  }
+  __syncthreads();
+  T pre = w > 0 ? sh[w - 1] : T(0);
+  total = sh[nw - 1];
+  __syncthreads();
+  return pre + x - v;
 }
 
 __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops) {
@@ -417,6 +428,7 @@ __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops
   __shared__ int sh_j[BLK];
   __shared__ double sh_v[BLK];
   __shared__ int sh_flag;
+  extern __shared__ double sm[];  // staged phi edges and widths of the pair
   const int a = blockIdx.x;
   const Annulus A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -424,17 +436,41 @@ __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops
   const int tid = threadIdx.x, nt = blockDim.x;
   const int np = A.np, off = A.cell_off;
   const int N = d.n_cells;
+  const bool pair = A.i < P.NR - 1;
+  const int npo = pair ? d.ann[a + 1].np : 0;
+  const int offo = pair ? d.ann[a + 1].cell_off : 0;
+  const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo);
+  const double *tin = traw + off, *din = d.dphi + off;
+  const double *tout = traw + offo, *dout = d.dphi + offo;
+  if (staged) {
+    double *s_tin = sm, *s_din = sm + np, *s_tout = sm + 2 * np, *s_dout = sm + 2 * np + npo;
+    for (int j = tid; j < np; j += nt) {
+      s_tin[j] = tin[j];
+      s_din[j] = din[j];
+    }
+    for (int j = tid; j < npo; j += nt) {
+      s_tout[j] = tout[j];
+      s_dout[j] = dout[j];
+    }
+    __syncthreads();
+    tin = s_tin;
+    din = s_din;
+    tout = s_tout;
+    dout = s_dout;
+  }
 
   // cell_clean_pi (src/Cell/cell_misc.c:12-26)
-  for (int j = tid; j < np; j += nt) d.tiphw[off + j] = wrap_pos(traw[off + j], d.err);
+  for (int j = tid; j < np; j += nt) d.tiphw[off + j] = wrap_pos(tin[j], d.err);
 
   // cell_plm_p (src/Cell/cell_plm.c:116-161)
   for (int j = tid; j < np; j += nt) {
     int g = off + j;
-    int gl = j == 0 ? off + np - 1 : g - 1;
-    int gr = j == np - 1 ? off : g + 1;
-    double dpL = .5 * (d.dphi[g] + d.dphi[gl]);
-    double dpR = .5 * (d.dphi[g] + d.dphi[gr]);
+    int jl = j == 0 ? np - 1 : j - 1;
+    int jr = j == np - 1 ? 0 : j + 1;
+    int gl = off + jl;
+    int gr = off + jr;
+    double dpL = .5 * (din[j] + din[jl]);
+    double dpR = .5 * (din[j] + din[jr]);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       double pc = ld(d.prim, q, N, g), pl = ld(d.prim, q, N, gl), pr = ld(d.prim, q, N, gr);
@@ -474,6 +510,9 @@ __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops
         S.grk_phi[p] = S.gphi[p];
         S.grk_M[p] = S.gM[p];
         S.grk_om[p] = S.gom[p];
+        // gravMass_dist of the step-start positions (the CFL's viscosity)
+        S.rkx[p] = S.gr[p] * cos(S.gphi[p]);
+        S.rky[p] = S.gr[p] * sin(S.gphi[p]);
       }
       S.dtkey = (unsigned long long)__double_as_longlong(1.e100);
     }
@@ -483,17 +522,16 @@ __global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops
     }
   }
 
-  if (A.i >= P.NR - 1) return;
+  if (!pair) return;
 
   // ---- r faces of the pair (a, a+1) ----
-  const Annulus B = d.ann[a + 1];
   FaceCtx c;
-  c.tin = traw + off;
-  c.din = d.dphi + off;
-  c.tout = traw + B.cell_off;
-  c.dout = d.dphi + B.cell_off;
+  c.tin = tin;
+  c.din = din;
+  c.tout = tout;
+  c.dout = dout;
   c.Nin = np;
-  c.Nout = B.np;
+  c.Nout = npo;
   c.fL = d.fL + A.face_base;
   c.fR = d.fR + A.face_base;
   c.fdphi = d.fdphi + A.face_base;
@@ -674,37 +712,63 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
   }
 }
 
+// r-face slope and reconstruction offsets, once per face: the S of
+// cell_plm_rz (src/Cell/cell_plm.c:31-53) and the wrapped dpL, dpR that
+// cell_plm_rz, riemann_setup_rz (Riemann_setup.c:18-25) and riemann_visc_flux
+// (Riemann_routines.c:220-228) all form the same way.
+__global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= d.n_slots) return;
+  const int a = d.slot_ann[slot];
+  if (a < 0) return;
+  const Annulus &A = d.ann[a];
+  if (slot - A.face_base >= d.pair_nf[a]) return;
+  const int N = d.n_cells, NS = d.n_slots;
+  const int cL = A.cell_off + d.fL[slot];
+  const int cR = d.ann[a + 1].cell_off + d.fR[slot];
+  const double cm = d.fcm[slot];
+  double pL = d.tiphw[cL] - .5 * d.dphi[cL];
+  double pR = d.tiphw[cR] - .5 * d.dphi[cR];
+  double dpL = cm - pL;
+  dpL = wrap_pm(dpL, d.err);
+  double dpR = pR - cm;
+  dpR = wrap_pm(dpR, d.err);
+  d.fdp[slot] = dpL;
+  d.fdp[(size_t)NS + slot] = dpR;
+  const double den = A.f_dr + A.f_dl;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double WL = ld(d.prim, q, N, cL) + dpL * ld(d.gradp, q, N, cL);
+    double WR = ld(d.prim, q, N, cR) - dpR * ld(d.gradp, q, N, cR);
+    d.fS[(size_t)q * NS + slot] = (WR - WL) / den;
+  }
+}
+
 __global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int N = d.n_cells;
+  const int N = d.n_cells, NS = d.n_slots;
   unsigned long long key = ~0ull;
   int inst = -1;
+  if (g < d.n_inst) {
+    // GravMass positions of this substep (gravMass_dist, cell_source.c:103-107)
+    InstState &S = d.ist[g];
+    for (int p = 0; p < 2; ++p) {
+      S.gc[p] = cos(S.gphi[p]);
+      S.gs[p] = sin(S.gphi[p]);
+      S.gx[p] = S.gr[p] * S.gc[p];
+      S.gy[p] = S.gr[p] * S.gs[p];
+    }
+  }
   if (g < N) {
     const int a = d.cell_ann[g];
     const Annulus A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
     inst = A.inst;
     double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    auto slopes = [&](const RFace &F, double *S) {
-      double pL = d.tiphw[F.cL] - .5 * d.dphi[F.cL];
-      double pR = d.tiphw[F.cR] - .5 * d.dphi[F.cR];
-      double dpL = F.cm - pL;
-      dpL = wrap_pm(dpL, d.err);
-      double dpR = pR - F.cm;
-      dpR = wrap_pm(dpR, d.err);
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        double WL = ld(d.prim, q, N, F.cL) + dpL * ld(d.gradp, q, N, F.cL);
-        double WR = ld(d.prim, q, N, F.cR) - dpR * ld(d.gradp, q, N, F.cR);
-        S[q] = (WR - WL) / (F.dr + F.dl);
-      }
-    };
-    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int) {
-      double S[5];
-      slopes(F, S);
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
       double dA = F.r * F.dphi * F.dperp;
 #pragma unroll
-      for (int q = 0; q < 5; ++q) gq[q] += S[q] * dA;
+      for (int q = 0; q < 5; ++q) gq[q] += d.fS[(size_t)q * NS + slot] * dA;
     });
     {
       double dz = P.dz, dp = d.dphi[g], dAtot;
@@ -714,13 +778,12 @@ __global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
 #pragma unroll
       for (int q = 0; q < 5; ++q) gq[q] /= dAtot;
     }
-    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int) {
-      double S[5];
-      slopes(F, S);
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        if (S[q] * gq[q] < 0.0) gq[q] = 0.0;
-        else if (fabs(P.plm * S[q]) < fabs(gq[q])) gq[q] = P.plm * S[q];
+        double Sq = d.fS[(size_t)q * NS + slot];
+        if (Sq * gq[q] < 0.0) gq[q] = 0.0;
+        else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
       }
     });
 #pragma unroll
@@ -754,13 +817,11 @@ __global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
             nu = P.visc * P.gamma * Pp / rho * dpow(fabs(r * cos(tc)), 2.0);
             if (r * cos(tc) > 20.) nu = 0.000000001;
           } else {
-            double xb0 = S.grk_r[0] * cos(S.grk_phi[0]), yb0 = S.grk_r[0] * sin(S.grk_phi[0]);
-            double xb1 = S.grk_r[1] * cos(S.grk_phi[1]), yb1 = S.grk_r[1] * sin(S.grk_phi[1]);
-            double d0 = gm_dist(xb0, yb0, r, tc);
-            double d1 = gm_dist(xb1, yb1, r, tc);
+            double d0 = gm_dist(S.rkx[0], S.rky[0], r, tc);
+            double d1 = gm_dist(S.rkx[1], S.rky[1], r, tc);
             double eps = P.g_eps;
             nu = P.visc * Pp / rho /
-                 sqrt(pow(d0 * d0 + eps * eps, -1.5) * S.grk_M[0] + pow(d1 * d1 + eps * eps, -1.5) * S.grk_M[1]);
+                 sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.grk_M[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.grk_M[1]);
           }
         }
         double dt_visc = .25 * dx * dx / nu;
@@ -812,6 +873,33 @@ __global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
+  if (t < d.n_ann) {
+    // per-annulus constants of this substep for k_update: the epicyclic rotation
+    // of cell_add_split_fictitious (cell_add_split_fictitious.c:26-38) and the
+    // relaxation factor of cell_bc_damp (cell_misc.c:121), identical for every
+    // cell of the annulus
+    const Annulus &A = d.ann[t];
+    const DiskParams &P = d.par[A.inst];
+    const InstState &S = d.ist[A.inst];
+    const double dt = fac * S.dt;
+    const double r = 0.5 * (A.rm + A.rp);
+    const double a_sep = S.gr[0] + S.gr[1];
+    const double rom = frame_rom(P, A.rom, r, a_sep);
+    const double Omega = rom / r;
+    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
+    const double kappa2 = 2. * Omega / r * dr_r2Om;
+    double kappa = 0.0, ck = 1.0, sk = 0.0;
+    if (kappa2 > 0.) {
+      kappa = sqrt(kappa2);
+      ck = cos(kappa * dt);
+      sk = sin(kappa * dt);
+    }
+    const int NA = d.n_ann;
+    d.ann_c[t] = kappa;
+    d.ann_c[NA + t] = ck;
+    d.ann_c[2 * NA + t] = sk;
+    d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
+  }
   if (t < N) {
     // phi face (j, j+1): riemann_setup_p (Riemann_setup.c:46-80)
     const int g = t;
@@ -855,21 +943,15 @@ __global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
       }
       v.tL = d.tiphw[cL];
       v.tR = d.tiphw[cR];
-      v.dL = dpL;
-      v.dR = dpR;
+      v.dpL = v.dpR = 0.0;
       v.r = r;
       v.cm = d.tiphw[cL];
       v.r_cell_L = r;
       v.r_cell_R = r;
       double a_sep = S.gr[0] + S.gr[1];
       v.rdr_om = frame_rdrom(P, A.rdrom, r, a_sep);
-      double gx[2], gy[2];
-      for (int p = 0; p < 2; ++p) {
-        gx[p] = S.gr[p] * cos(S.gphi[p]);
-        gy[p] = S.gr[p] * sin(S.gphi[p]);
-      }
       double Fv[3];
-      visc_flux(v, 1, P, S, gx, gy, Fv, d.err);
+      visc_flux(v, 1, P, S, S.gx, S.gy, Fv, d.err);
 #pragma unroll
       for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * N + g] = k * Fv[q];
     }
@@ -890,12 +972,8 @@ __global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
   const int cR = B.cell_off + d.fR[slot];
   const double fdphi = d.fdphi[slot], cm = d.fcm[slot];
   const double deltaL = A.f_dl, deltaR = A.f_dr;
-  double pLc = d.tiphw[cL] - .5 * d.dphi[cL];
-  double pRc = d.tiphw[cR] - .5 * d.dphi[cR];
-  double dpL = cm - pLc;
-  double dpR = -cm + pRc;
-  dpL = wrap_pm(dpL, d.err);
-  dpR = wrap_pm(dpR, d.err);
+  const double dpL = d.fdp[slot];
+  const double dpR = d.fdp[(size_t)d.n_slots + slot];
   const double r = A.f_r;
   const double dA = r * fdphi * A.f_dperp;
   const double r_cell_L = r - deltaL;
@@ -929,21 +1007,16 @@ __global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
     }
     v.tL = d.tiphw[cL];
     v.tR = d.tiphw[cR];
-    v.dL = d.dphi[cL];
-    v.dR = d.dphi[cR];
+    v.dpL = dpL;
+    v.dpR = dpR;
     v.r = r;
     v.cm = cm;
     v.r_cell_L = r_cell_L;
     v.r_cell_R = r_cell_R;
     double a_sep = S.gr[0] + S.gr[1];
     v.rdr_om = frame_rdrom(P, A.f_rdrom, r, a_sep);
-    double gx[2], gy[2];
-    for (int p = 0; p < 2; ++p) {
-      gx[p] = S.gr[p] * cos(S.gphi[p]);
-      gy[p] = S.gr[p] * sin(S.gphi[p]);
-    }
     double Fv[3];
-    visc_flux(v, 0, P, S, gx, gy, Fv, d.err);
+    visc_flux(v, 0, P, S, S.gx, S.gy, Fv, d.err);
 #pragma unroll
     for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * NS + slot] = k * Fv[q];
   }
@@ -954,7 +1027,7 @@ __global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
 // ---------------------------------------------------------------------------
 // fgrav (src/Cell/cell_source.c:11-13)
 __device__ __forceinline__ double fgrav(double M, double r, double eps, int n) {
-  return (M * dpow(r, n - 1.) / pow(dpow(r, n) + dpow(eps, n), 1. + 1. / n));
+  return (M * dpow(r, n - 1.) / dpow(dpow(r, n) + dpow(eps, n), 1. + 1. / n));
 }
 
 // Advanced phi edge of a cell (cell_update_phi, src/Cell/cell_misc.c:59-79).
@@ -1087,12 +1160,11 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
       double Fr = 0.0, Fp = 0.0;
       double xb[2], yb[2];
       for (int p = 0; p < 2; ++p) {
-        double cpp = cos(S.gphi[p]), spp = sin(S.gphi[p]);
-        xb[p] = S.gr[p] * cpp;
-        yb[p] = S.gr[p] * spp;
+        xb[p] = S.gx[p];
+        yb[p] = S.gy[p];
         // gravMassForce (src/Cell/cell_source.c:49-71)
-        double dx = gravdist * cosp - S.gr[p] * cpp;
-        double dy = gravdist * sinp - S.gr[p] * spp;
+        double dx = gravdist * cosp - S.gx[p];
+        double dy = gravdist * sinp - S.gy[p];
         double script_r = sqrt(dx * dx + dy * dy);
         double cosa = dx / script_r;
         double sina = dy / script_r;
@@ -1161,8 +1233,8 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
           Sigma_nu = rho * alpha;
         } else {
           Sigma_nu = alpha * Pp /
-                     sqrt(pow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
-                          pow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
+                     sqrt(dpow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
+                          dpow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
         }
         c[D_TAU] += dt * dV * Sigma_nu * rdrOm_a * (rdrOm_a + r * ld(d.grad, D_UPP, N, g) + ld(d.gradp, D_URR, N, g));
       }
@@ -1171,12 +1243,12 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
         double rom = w_a;
         double Omega = rom / r;
         double dr_r2Om = 2. * rom + r * rdrOm_a;
-        double kappa2 = 2. * Omega / r * dr_r2Om;
-        if (kappa2 > 0.) {
-          double kappa = sqrt(kappa2);
+        const int NA = d.n_ann;
+        const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_flux)
+        if (kappa > 0.) {
           double l0 = c[D_LLL];
           double rhov0 = c[D_SRR];
-          double ck = cos(kappa * dt), sk = sin(kappa * dt);
+          double ck = d.ann_c[NA + a], sk = d.ann_c[2 * NA + a];
           double l = l0 * ck - c[D_SRR] * dr_r2Om / kappa * sk;
           double rhov = rhov0 * ck + 2.0 * Omega * c[D_LLL] / r / kappa * sk;
           c[D_LLL] = l;
@@ -1243,7 +1315,7 @@ __global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop
         }
         // cell_bc_damp (src/Cell/cell_misc.c:98-132)
         if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
-          double f = (1. - exp(-A.damp_rate * dt));
+          double f = d.ann_c[3 * d.n_ann + a];  // 1.-exp(-rate*dt), k_flux
 #pragma unroll
           for (int q = 0; q < 5; ++q) {
             double dprim = A.ic[q] - pr[q];
@@ -1456,7 +1528,12 @@ int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa,
 int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
 
 int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream) {
-  k_face<<<d->n_ann, BLK, 0, (cudaStream_t)stream>>>(*d, substep, gm_ops);
+  k_face<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep, gm_ops);
+  return (int)cudaGetLastError();
+}
+int dgk_rslope(const DevPtrs *d, void *stream) {
+  if (d->n_slots <= 0) return 0;
+  k_rslope<<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
   return (int)cudaGetLastError();
 }
 int dgk_plm_r(const DevPtrs *d, int substep, void *stream) {

@@ -214,9 +214,12 @@ class Context:
         if sync:
             self.synchronize()
 
+    KERNELS = ("face", "rslope", "plm_r", "flux", "update")
+
     def step_timed(self, nsteps: int = 1) -> np.ndarray:
-        """Per-kernel device milliseconds summed over nsteps (8 kernels per step)."""
-        ms = np.zeros(8)
+        """Per-kernel device milliseconds summed over nsteps (KERNELS of substep 1,
+        then of substep 2)."""
+        ms = np.zeros(2 * len(self.KERNELS))
         self._ck(load().dgpu_step_rk2_timed(self._h, nsteps, _dptr(ms)))
         return ms
 

@@ -1,0 +1,45 @@
+"""Run a named workload for a few RK2 steps on cuda:0.
+
+    python -m disco2_b200.run --workload circumbinary --steps 3 [--timed] [--batch N]
+
+Used for profiling (ncu attaches to this process) and as a minimal example of
+the C ABI from Python.  --timed adds one step launched kernel by kernel
+with CUDA events and prints the per-kernel device times.  --batch N steps N
+copies of the disk in one context.
+"""
+from __future__ import annotations
+
+import argparse
+
+from . import configs, lib
+
+WORKLOADS = {"circumbinary": configs.circumbinary, "kepler_ring": configs.kepler_ring,
+             "gresho": configs.gresho}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="circumbinary", choices=sorted(WORKLOADS))
+    ap.add_argument("--num-r", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--timed", action="store_true")
+    ap.add_argument("--batch", type=int, default=1)
+    args = ap.parse_args()
+    p = WORKLOADS[args.workload]() if args.num_r is None else WORKLOADS[args.workload](num_r=args.num_r)
+    sims = [lib.Sim(p) for _ in range(args.batch)]
+    ctx = lib.Context(sims)
+    for k in range(args.batch):
+        ctx.init_state(k)
+    ctx.step(args.steps)
+    if args.timed:
+        ms = ctx.step_timed(1)
+        names = lib.Context.KERNELS
+        k = len(names)
+        print(" ".join(f"{n}{s}={ms[k * (s - 1) + i]:.4f}ms" for s in (1, 2) for i, n in enumerate(names)))
+    t, dt = ctx.time(0)
+    print(f"{args.workload}: {sims[0].num_cells} cells x {args.batch}, t={t:.6g} dt={dt:.6g}")
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
