@@ -29,7 +29,7 @@ HEADERS = ["dgpu_internal.h", "dgpu_sim.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false",
     "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-]
+] + os.environ.get("DGPU_NVCC_EXTRA", "").split()
 C_FLAGS = ["-O2", "-std=gnu99", "-fPIC", "-ffp-contract=off", "-Wall",
            "-Wno-unused-function", f"-I{CUDA_HOME}/include", f"-I{ROOT}/include"]
 

@@ -28,6 +28,21 @@
 
 #define PHIMAX (2.0 * M_PI)
 #define BLK 256
+// minimum resident blocks per SM requested from the register allocator
+// (measured on B200, circumbinary disk: these kernels are latency-bound, so
+// occupancy beats the extra spills)
+#ifndef DGPU_MINB_FACE
+#define DGPU_MINB_FACE 4
+#endif
+#ifndef DGPU_MINB_PLM
+#define DGPU_MINB_PLM 4
+#endif
+#ifndef DGPU_MINB_FLUX
+#define DGPU_MINB_FLUX 4
+#endif
+#ifndef DGPU_MINB_UPDATE
+#define DGPU_MINB_UPDATE 3
+#endif
 
 namespace {
 
@@ -423,7 +438,7 @@ __device__ T block_excl_scan(T v, T *sh, T &total) {
   return pre + x - v;
 }
 
-__global__ void __launch_bounds__(BLK) k_face(DevPtrs d, int substep, int gm_ops) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_face(DevPtrs d, int substep, int gm_ops) {
   __shared__ int sh_i[BLK];
   __shared__ int sh_j[BLK];
   __shared__ double sh_v[BLK];
@@ -744,7 +759,7 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d) {
   }
 }
 
-__global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells, NS = d.n_slots;
   unsigned long long key = ~0ull;
@@ -869,7 +884,7 @@ __global__ void __launch_bounds__(BLK) k_plm_r(DevPtrs d, int substep) {
 // ---------------------------------------------------------------------------
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLK) k_flux(DevPtrs d, int substep) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux(DevPtrs d, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
@@ -1039,7 +1054,7 @@ __device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, dou
   return t;
 }
 
-__global__ void __launch_bounds__(BLK) k_update(DevPtrs d, int substep, int stop, int tail) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int substep, int stop, int tail) {
   __shared__ double sh_md[2][BLK / 32];
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
