@@ -23,6 +23,8 @@ struct dgpu_ctx {
   int device;
   cudaStream_t stream;
   int own_stream;
+  cudaStream_t side;        /* second stream: concurrent branches inside the step graph */
+  cudaEvent_t fork[4];
   int n_inst;
   struct dgpu_sim **sims;
   DiskParams *h_par;
@@ -227,13 +229,16 @@ void dgpu_destroy(dgpu_ctx *c) {
   {
     void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
-                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
+                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
                   c->d.mdot_part, c->d.counters, c->d.err, c->d_stage, c->d_torque};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
       if (ps[k]) cudaFree(ps[k]);
   }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->side) cudaStreamDestroy(c->side);
+  for (k = 0; k < 4; ++k)
+    if (c->fork[k]) cudaEventDestroy(c->fork[k]);
   if (c->sims) {
     for (k = 0; k < c->n_inst; ++k) dsim_free(c->sims[k]);
     free(c->sims);
@@ -334,6 +339,17 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->own_stream = 1;
   }
   {
+    int k, bad = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess;
+    for (k = 0; k < 4 && !bad; ++k)
+      bad = cudaEventCreateWithFlags(&c->fork[k], cudaEventDisableTiming) != cudaSuccess;
+    if (bad) {
+      free(h_cell_ann);
+      free(h_slot_ann);
+      dgpu_destroy(c);
+      return fail(NULL, DGPU_ERR_CUDA, "stream/event creation failed");
+    }
+  }
+  {
     size_t N = (size_t)c->n_cells, S = (size_t)c->n_slots, A = (size_t)c->n_ann;
     c->d_par = (DiskParams *)dmalloc(sizeof(DiskParams) * (size_t)n, &ok);
     c->d_ist = (InstState *)dmalloc(sizeof(InstState) * (size_t)n, &ok);
@@ -354,6 +370,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.fphi = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
     c->d.frf = (double *)dmalloc(sizeof(double) * 8 * (S ? S : 1), &ok);
     c->d.fS = (double *)dmalloc(sizeof(double) * 5 * (S ? S : 1), &ok);
+    c->d.src = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
     c->d.fdp = (double *)dmalloc(sizeof(double) * 2 * (S ? S : 1), &ok);
     c->d.ann_c = (double *)dmalloc(sizeof(double) * 4 * A, &ok);
     c->d.fstart = (int *)dmalloc(sizeof(int) * N, &ok);
@@ -632,10 +649,22 @@ int dgpu_init_state(dgpu_ctx *c, int inst) {
 static int launch_step(struct dgpu_ctx *c) {
   int sub;
   for (sub = 1; sub <= 2; ++sub) {
-    CKK(dgk_face(&c->d, sub, 1, c->stream));
+    /* k_merge (per annulus pair) alongside k_cellprep (per cell) */
+    CK(cudaEventRecord(c->fork[0], c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
+    CKK(dgk_merge(&c->d, sub, c->side));
+    CKK(dgk_cellprep(&c->d, sub, c->stream));
+    CK(cudaEventRecord(c->fork[1], c->side));
+    CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
     CKK(dgk_rslope(&c->d, c->stream));
     CKK(dgk_plm_r(&c->d, sub, c->stream));
+    /* k_source (per cell) alongside k_flux (per face) */
+    CK(cudaEventRecord(c->fork[2], c->stream));
+    CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
+    CKK(dgk_source(&c->d, sub, c->side));
     CKK(dgk_flux(&c->d, sub, c->stream));
+    CK(cudaEventRecord(c->fork[3], c->side));
+    CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
     CKK(dgk_update(&c->d, sub, 7, c->stream));
   }
   return DGPU_OK;
@@ -676,11 +705,15 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
     int e = 0;
     CK(cudaEventRecord(ev[e++], c->stream));
     for (sub = 1; sub <= 2; ++sub) {
-      CKK(dgk_face(&c->d, sub, 1, c->stream));
+      CKK(dgk_cellprep(&c->d, sub, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_merge(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_rslope(&c->d, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_plm_r(&c->d, sub, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_source(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_flux(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
@@ -701,10 +734,12 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
 int dgpu_stage(dgpu_ctx *c, int phase) {
   if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
-  CKK(dgk_face(&c->d, 1, 1, c->stream));
+  CKK(dgk_cellprep(&c->d, 1, c->stream));
+  CKK(dgk_merge(&c->d, 1, c->stream));
   /* the CFL minimum (and dt) come from k_plm_r; PLM results are kept only from phase 1 on */
   CKK(dgk_rslope(&c->d, c->stream));
   CKK(dgk_plm_r(&c->d, 1, c->stream));
+  CKK(dgk_source(&c->d, 1, c->stream));
   if (phase >= 2) CKK(dgk_flux(&c->d, 1, c->stream));
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
   /* from phase 5 on the advanced phi edges live in the substep's output buffer */
@@ -725,7 +760,7 @@ int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, dou
   s = c->sims[inst];
   p = &c->h_par[inst];
   /* build the list of the current state: one k_face pass (substep-1 buffers) */
-  CKK(dgk_face(&c->d, 1, 0, c->stream));
+  CKK(dgk_merge(&c->d, 1, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
   nf = (int *)malloc(sizeof(int) * (size_t)s->NR);
   fL = (int *)malloc(sizeof(int) * (size_t)c->n_slots);

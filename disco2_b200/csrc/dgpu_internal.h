@@ -18,7 +18,7 @@
 #define DGPU_FACE_SLACK 8
 #define DGPU_RUN_SLACK 8
 #define DGPU_WRAP_LIMIT 64
-#define DGPU_STEP_KERNELS 10 /* launches per RK2 step: 5 per substep */
+#define DGPU_STEP_KERNELS 14 /* launches per RK2 step: 7 per substep */
 
 /* enums of src/Headers/header.h:1-13 */
 enum { D_RHO, D_PPP, D_URR, D_UPP, D_UZZ };
@@ -122,6 +122,7 @@ typedef struct {
   double *w_ann;          /* wiph per annulus */
   double *fphi;           /* [8][n_cells] phi-face increments, face (j, j+1) at cell j */
   double *frf;            /* [8][n_slots] r-face increments */
+  double *src;            /* [8][n_cells] source increments of the substep (k_source) */
   double *fS;             /* [5][n_slots] r-face slopes (WR - WL)/(deltaR + deltaL) */
   double *fdp;            /* [2][n_slots] r-face offsets dpL, dpR (wrapped to [-pi, pi]) */
   double *ann_c;          /* [4][n_ann] per substep: kappa, cos(kappa dt), sin(kappa dt), 1-exp(-rate dt) */
@@ -140,7 +141,9 @@ typedef struct {
 extern "C" {
 #endif
 /* kernel launchers (dgpu_kernels.cu); return cudaError_t as int */
-int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream);
+int dgk_cellprep(const DevPtrs *d, int substep, void *stream);
+int dgk_merge(const DevPtrs *d, int substep, void *stream);
+int dgk_source(const DevPtrs *d, int substep, void *stream);
 int dgk_rslope(const DevPtrs *d, void *stream);
 int dgk_plm_r(const DevPtrs *d, int substep, void *stream);
 int dgk_flux(const DevPtrs *d, int substep, void *stream);

@@ -133,10 +133,9 @@ __device__ __forceinline__ double frame_dtom(const DiskParams &P, double tab, do
   return P.w_analytic == DA_MILOS ? milos_dtom(r, a, P.orb_tscale) : tab;
 }
 
-// gravMass_dist (src/GravMass/GravMass_access.c:25-31) with (xbh, ybh) given.
-__device__ __forceinline__ double gm_dist(double xbh, double ybh, double r, double phi) {
-  double x = r * cos(phi);
-  double y = r * sin(phi);
+// gravMass_dist (src/GravMass/GravMass_access.c:25-31) from the point's
+// x = r cos(phi), y = r sin(phi) and the mass position (xbh, ybh).
+__device__ __forceinline__ double gm_dist_xy(double x, double y, double xbh, double ybh) {
   double z = 0.;
   return sqrt((x - xbh) * (x - xbh) + (y - ybh) * (y - ybh) + z * z);
 }
@@ -314,8 +313,11 @@ __device__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const I
     nu = alpha * P.gamma * Avg[D_PPP] / Avg[D_RHO] * dpow(fabs(r * cos(v.cm)), 2.0);
     if (r * cos(v.cm) > 20.) nu = 0.0;
   } else {
-    double d0 = gm_dist(gx[0], gy[0], r, v.cm);
-    double d1 = gm_dist(gx[1], gy[1], r, v.cm);
+    double sc, cc;
+    sincos(v.cm, &sc, &cc);
+    const double x = r * cc, y = r * sc;
+    double d0 = gm_dist_xy(x, y, gx[0], gy[0]);
+    double d1 = gm_dist_xy(x, y, gx[1], gy[1]);
     double eps = P.g_eps;
     nu = alpha * Avg[D_PPP] / Avg[D_RHO] /
          sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.gM[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.gM[1]);
@@ -438,86 +440,40 @@ __device__ T block_excl_scan(T v, T *sh, T &total) {
   return pre + x - v;
 }
 
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_face(DevPtrs d, int substep, int gm_ops) {
-  __shared__ int sh_i[BLK];
-  __shared__ int sh_j[BLK];
-  __shared__ double sh_v[BLK];
-  __shared__ int sh_flag;
-  extern __shared__ double sm[];  // staged phi edges and widths of the pair
-  const int a = blockIdx.x;
-  const Annulus A = d.ann[a];
-  const DiskParams &P = d.par[A.inst];
-  const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int np = A.np, off = A.cell_off;
+// Per cell, once per substep: cell_clean_pi (src/Cell/cell_misc.c:12-26),
+// cell_plm_p (src/Cell/cell_plm.c:116-161) and, for the first cell of each disk,
+// gravMass_copy at the start of a step (GravMass_misc.c:20-28) and
+// gravMass_clean_pi (GravMass_misc.c:9-17).  Runs concurrently with k_merge.
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, int substep) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
-  const bool pair = A.i < P.NR - 1;
-  const int npo = pair ? d.ann[a + 1].np : 0;
-  const int offo = pair ? d.ann[a + 1].cell_off : 0;
-  const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo);
-  const double *tin = traw + off, *din = d.dphi + off;
-  const double *tout = traw + offo, *dout = d.dphi + offo;
-  if (staged) {
-    double *s_tin = sm, *s_din = sm + np, *s_tout = sm + 2 * np, *s_dout = sm + 2 * np + npo;
-    for (int j = tid; j < np; j += nt) {
-      s_tin[j] = tin[j];
-      s_din[j] = din[j];
-    }
-    for (int j = tid; j < npo; j += nt) {
-      s_tout[j] = tout[j];
-      s_dout[j] = dout[j];
-    }
-    __syncthreads();
-    tin = s_tin;
-    din = s_din;
-    tout = s_tout;
-    dout = s_dout;
-  }
-
-  // cell_clean_pi (src/Cell/cell_misc.c:12-26)
-  for (int j = tid; j < np; j += nt) d.tiphw[off + j] = wrap_pos(tin[j], d.err);
-
-  // cell_plm_p (src/Cell/cell_plm.c:116-161)
-  for (int j = tid; j < np; j += nt) {
-    int g = off + j;
-    int jl = j == 0 ? np - 1 : j - 1;
-    int jr = j == np - 1 ? 0 : j + 1;
-    int gl = off + jl;
-    int gr = off + jr;
-    double dpL = .5 * (din[j] + din[jl]);
-    double dpR = .5 * (din[j] + din[jr]);
+  if (g >= N) return;
+  const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
+  const int a = d.cell_ann[g];
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  const int np = A.np, off = A.cell_off, j = g - off;
+  d.tiphw[g] = wrap_pos(traw[g], d.err);
+  {
+    const int gl = off + (j == 0 ? np - 1 : j - 1);
+    const int gr = off + (j == np - 1 ? 0 : j + 1);
+    const double dc = d.dphi[g];
+    const double dpL = .5 * (dc + d.dphi[gl]);
+    const double dpR = .5 * (dc + d.dphi[gr]);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       double pc = ld(d.prim, q, N, g), pl = ld(d.prim, q, N, gl), pr = ld(d.prim, q, N, gr);
       double sL = (pc - pl) / dpL;
       double sR = (pr - pc) / dpR;
       double sM = (pr - pl) / (dpL + dpR);
-      double s = P.plm * sL;
-      if (fabs(s) > P.plm * fabs(sR)) s = P.plm * sR;
-      if (fabs(s) > fabs(sM)) s = sM;
-      if (sL * sR < 0.0) s = 0.0;
-      d.gradp[(size_t)q * N + g] = s;
+      double sv = P.plm * sL;
+      if (fabs(sv) > P.plm * fabs(sR)) sv = P.plm * sR;
+      if (fabs(sv) > fabs(sM)) sv = sM;
+      if (sL * sR < 0.0) sv = 0.0;
+      d.gradp[(size_t)q * N + g] = sv;
     }
   }
-
-  // cell_clear_w + cell_set_w (src/Cell/cell_set_w.c:12-102): one value per annulus
-  if (tid == 0) {
-    if (P.w_numeric == DC_RIGID) {
-      double w = 0.0, Mring = 0.0;
-      for (int j = 0; j < np; ++j) {
-        double vp = A.r * ld(d.prim, D_UPP, N, off + j);
-        double m = ld(d.cons, D_DDD, N, off + j);
-        Mring += m;
-        w += vp * m;
-      }
-      d.w_ann[a] = w / Mring;
-    } else {
-      d.w_ann[a] = A.wnum;
-    }
-  }
-
-  // GravMass: gravMass_copy at the start of a step, then gravMass_clean_pi
-  if (gm_ops && A.i == 0 && tid == 0) {
+  if (g == P.cell_base) {
     InstState &S = d.ist[A.inst];
     if (substep == 1) {
       for (int p = 0; p < 2; ++p) {
@@ -531,136 +487,184 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_face(DevPtrs d, int sub
       }
       S.dtkey = (unsigned long long)__double_as_longlong(1.e100);
     }
-    for (int p = 0; p < 2; ++p) {
-      // gravMass_clean_pi: same loops as cell_clean_pi with 2.*M_PI == PHIMAX
-      S.gphi[p] = wrap_pos(S.gphi[p], d.err);
-    }
+    for (int p = 0; p < 2; ++p) S.gphi[p] = wrap_pos(S.gphi[p], d.err);  // 2.*M_PI == PHIMAX
   }
+}
 
-  if (!pair) return;
-
-  // ---- r faces of the pair (a, a+1) ----
-  FaceCtx c;
-  c.tin = tin;
-  c.din = din;
-  c.tout = tout;
-  c.dout = dout;
-  c.Nin = np;
-  c.Nout = npo;
-  c.fL = d.fL + A.face_base;
-  c.fR = d.fR + A.face_base;
-  c.fdphi = d.fdphi + A.face_base;
-  c.fcm = d.fcm + A.face_base;
-  c.runs = d.runs + A.run_base;
-  c.fstart = d.fstart + off;
-  c.cap = A.face_cap;
-  c.rcap = A.run_cap;
-  c.err = d.err;
-  const double p0 = c.tin[np - 1];
-
-  // jpmin: first outer cell with the smallest wrap(tiph - p0), start (PHIMAX, 0)
-  {
-    double bv = PHIMAX;
-    int bi = 0;
-    for (int jp = tid; jp < c.Nout; jp += nt) {
-      double dp = wrap_pos(c.tout[jp] - p0, d.err);
-      if (dp < bv || (dp == bv && jp < bi)) {
-        bv = dp;
-        bi = jp;
+// Per annulus pair (i, i+1) of a disk: the r-face list of face_create/
+// build_jloop (src/Face/face_create_destroy.c:22-193) as a checked parallel
+// merge, and cell_set_w (src/Cell/cell_set_w.c:12-102) of annulus i.
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int substep) {
+  __shared__ int sh_i[BLK];
+  __shared__ int sh_j[BLK];
+  __shared__ double sh_v[BLK];
+  __shared__ int sh_flag;
+  extern __shared__ double sm[];  // staged phi edges and widths of the pair
+  const int a = blockIdx.x;
+  const Annulus A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int np = A.np, off = A.cell_off;
+  const int N = d.n_cells;
+  const bool rigid = P.w_numeric == DC_RIGID;
+  if (tid == 0 && !rigid) d.w_ann[a] = A.wnum;
+  if (A.i < P.NR - 1) {
+    const int npo = d.ann[a + 1].np;
+    const int offo = d.ann[a + 1].cell_off;
+    const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo);
+    const double *tin = traw + off, *din = d.dphi + off;
+    const double *tout = traw + offo, *dout = d.dphi + offo;
+    if (staged) {
+      double *s_tin = sm, *s_din = sm + np, *s_tout = sm + 2 * np, *s_dout = sm + 2 * np + npo;
+      for (int j = tid; j < np; j += nt) {
+        s_tin[j] = tin[j];
+        s_din[j] = din[j];
       }
-    }
-    sh_v[tid] = bv;
-    sh_i[tid] = bi;
-    __syncthreads();
-    for (int o = nt / 2; o > 0; o >>= 1) {
-      if (tid < o) {
-        double v2 = sh_v[tid + o];
-        int i2 = sh_i[tid + o];
-        if (v2 < sh_v[tid] || (v2 == sh_v[tid] && i2 < sh_i[tid])) {
-          sh_v[tid] = v2;
-          sh_i[tid] = i2;
-        }
+      for (int j = tid; j < npo; j += nt) {
+        s_tout[j] = tout[j];
+        s_dout[j] = dout[j];
       }
       __syncthreads();
+      tin = s_tin;
+      din = s_din;
+      tout = s_tout;
+      dout = s_dout;
     }
-  }
-  const int jpmin = sh_i[0];
-  __syncthreads();
+    FaceCtx c;
+    c.tin = tin;
+    c.din = din;
+    c.tout = tout;
+    c.dout = dout;
+    c.Nin = np;
+    c.Nout = npo;
+    c.fL = d.fL + A.face_base;
+    c.fR = d.fR + A.face_base;
+    c.fdphi = d.fdphi + A.face_base;
+    c.fcm = d.fcm + A.face_base;
+    c.runs = d.runs + A.run_base;
+    c.fstart = d.fstart + off;
+    c.cap = A.face_cap;
+    c.rcap = A.run_cap;
+    c.err = d.err;
+    const double p0 = c.tin[np - 1];
 
-  // contiguous chunk of inner cells per thread; speculative start outer cell
-  const int chunk = (np + nt - 1) / nt;
-  const int j0 = min(np, tid * chunk), j1 = min(np, j0 + chunk);
-  int jp_start = jpmin;
-  if (j0 > 0 && j0 < np) {
-    // lower bound of the left edge of inner cell j0 among the outer edges,
-    // both measured as wrap(edge - p0); verified below
-    double L = wrap_pos(c.tin[j0 - 1] - p0, d.err);
-    int lo = 0, hi = c.Nout;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      int k = jpmin + mid;
-      if (k >= c.Nout) k -= c.Nout;
-      double e = wrap_pos(c.tout[k] - p0, d.err);
-      if (e < L) lo = mid + 1;
-      else hi = mid;
+    // jpmin: first outer cell with the smallest wrap(tiph - p0), start (PHIMAX, 0)
+    {
+      double bv = PHIMAX;
+      int bi = 0;
+      for (int jp = tid; jp < c.Nout; jp += nt) {
+        double dp = wrap_pos(c.tout[jp] - p0, d.err);
+        if (dp < bv || (dp == bv && jp < bi)) {
+          bv = dp;
+          bi = jp;
+        }
+      }
+      sh_v[tid] = bv;
+      sh_i[tid] = bi;
+      __syncthreads();
+      for (int o = nt / 2; o > 0; o >>= 1) {
+        if (tid < o) {
+          double v2 = sh_v[tid + o];
+          int i2 = sh_i[tid + o];
+          if (v2 < sh_v[tid] || (v2 == sh_v[tid] && i2 < sh_i[tid])) {
+            sh_v[tid] = v2;
+            sh_i[tid] = i2;
+          }
+        }
+        __syncthreads();
+      }
     }
-    jp_start = jpmin + lo;
-    if (jp_start >= c.Nout) jp_start -= c.Nout;
-  }
-  int cnt = 0, steps = 0, jp = jp_start;
-  {
-    int n = 0, s = 0;
-    for (int j = j0; j < j1; ++j) face_cell<false>(c, j, jp, n, s);
-    cnt = n;
-    steps = s;
-  }
-  if (tid == 0) sh_flag = 0;
-  sh_j[tid] = (j0 < j1) ? jp_start : -1;
-  __syncthreads();
-  if (j0 < j1 && tid + 1 < nt && sh_j[tid + 1] >= 0 && sh_j[tid + 1] != jp) sh_flag = 1;
-  __syncthreads();
-  const bool sequential = sh_flag != 0;
+    const int jpmin = sh_i[0];
+    __syncthreads();
 
-  if (!sequential) {
-    int ntot, stot;
-    int fo = block_excl_scan<int>(cnt, sh_i, ntot);
-    int so = block_excl_scan<int>(steps, sh_j, stot);
-    if (ntot > c.cap || stot + 2 > c.rcap) {
-      if (tid == 0) {
+    // contiguous chunk of inner cells per thread; speculative start outer cell
+    const int chunk = (np + nt - 1) / nt;
+    const int j0 = min(np, tid * chunk), j1 = min(np, j0 + chunk);
+    int jp_start = jpmin;
+    if (j0 > 0 && j0 < np) {
+      // lower bound of the left edge of inner cell j0 among the outer edges,
+      // both measured as wrap(edge - p0); verified below
+      double L = wrap_pos(c.tin[j0 - 1] - p0, d.err);
+      int lo = 0, hi = c.Nout;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        int k = jpmin + mid;
+        if (k >= c.Nout) k -= c.Nout;
+        double e = wrap_pos(c.tout[k] - p0, d.err);
+        if (e < L) lo = mid + 1;
+        else hi = mid;
+      }
+      jp_start = jpmin + lo;
+      if (jp_start >= c.Nout) jp_start -= c.Nout;
+    }
+    int cnt = 0, steps = 0, jp = jp_start;
+    {
+      int n = 0, s = 0;
+      for (int j = j0; j < j1; ++j) face_cell<false>(c, j, jp, n, s);
+      cnt = n;
+      steps = s;
+    }
+    if (tid == 0) sh_flag = 0;
+    sh_j[tid] = (j0 < j1) ? jp_start : -1;
+    __syncthreads();
+    if (j0 < j1 && tid + 1 < nt && sh_j[tid + 1] >= 0 && sh_j[tid + 1] != jp) sh_flag = 1;
+    __syncthreads();
+    const bool sequential = sh_flag != 0;
+
+    if (!sequential) {
+      int ntot, stot;
+      int fo = block_excl_scan<int>(cnt, sh_i, ntot);
+      int so = block_excl_scan<int>(steps, sh_j, stot);
+      if (ntot > c.cap || stot + 2 > c.rcap) {
+        if (tid == 0) {
+          set_err(d.err, DGPU_EF_FACE_OVERFLOW);
+          d.pair_nf[a] = 0;
+          d.pair_T[a] = 0;
+        }
+      } else {
+        int n = fo, s = so;
+        jp = jp_start;
+        for (int j = j0; j < j1; ++j) face_cell<true>(c, j, jp, n, s);
+        if (tid == 0) {
+          c.runs[0] = 0;
+          c.runs[stot + 1] = ntot;
+          d.pair_nf[a] = ntot;
+          d.pair_jpmin[a] = jpmin;
+          d.pair_T[a] = stot;
+          d.pair_seq[a] = 0;
+        }
+      }
+    } else if (tid == 0) {
+      // exact sequential replay of build_jloop from jpmin
+      int n = 0, s = 0;
+      jp = jpmin;
+      for (int j = 0; j < np; ++j) face_cell<true>(c, j, jp, n, s);
+      if (n > c.cap || s + 2 > c.rcap) {
         set_err(d.err, DGPU_EF_FACE_OVERFLOW);
         d.pair_nf[a] = 0;
         d.pair_T[a] = 0;
+      } else {
+        c.runs[0] = 0;
+        c.runs[s + 1] = n;
+        d.pair_nf[a] = n;
+        d.pair_jpmin[a] = jpmin;
+        d.pair_T[a] = s;
+        d.pair_seq[a] = 1;
       }
-      return;
     }
-    int n = fo, s = so;
-    jp = jp_start;
-    for (int j = j0; j < j1; ++j) face_cell<true>(c, j, jp, n, s);
-    if (tid == 0) {
-      c.runs[0] = 0;
-      c.runs[stot + 1] = ntot;
-      d.pair_nf[a] = ntot;
-      d.pair_jpmin[a] = jpmin;
-      d.pair_T[a] = stot;
-      d.pair_seq[a] = 0;
+  }
+  // C_RIGID: the mass-weighted mean v_phi of the annulus, summed in j order
+  // like the reference (cell_set_w.c:41-49); one lane, after the merge
+  if (rigid && tid == nt - 32) {
+    double w = 0.0, Mring = 0.0;
+    for (int j = 0; j < np; ++j) {
+      double vp = A.r * ld(d.prim, D_UPP, N, off + j);
+      double m = ld(d.cons, D_DDD, N, off + j);
+      Mring += m;
+      w += vp * m;
     }
-  } else if (tid == 0) {
-    // exact sequential replay of build_jloop from jpmin
-    int n = 0, s = 0;
-    jp = jpmin;
-    for (int j = 0; j < np; ++j) face_cell<true>(c, j, jp, n, s);
-    if (n > c.cap || s + 2 > c.rcap) {
-      set_err(d.err, DGPU_EF_FACE_OVERFLOW);
-      d.pair_nf[a] = 0;
-      d.pair_T[a] = 0;
-      return;
-    }
-    c.runs[0] = 0;
-    c.runs[s + 1] = n;
-    d.pair_nf[a] = n;
-    d.pair_jpmin[a] = jpmin;
-    d.pair_T[a] = s;
-    d.pair_seq[a] = 1;
+    d.w_ann[a] = w / Mring;
   }
 }
 
@@ -832,8 +836,11 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int sub
             nu = P.visc * P.gamma * Pp / rho * dpow(fabs(r * cos(tc)), 2.0);
             if (r * cos(tc) > 20.) nu = 0.000000001;
           } else {
-            double d0 = gm_dist(S.rkx[0], S.rky[0], r, tc);
-            double d1 = gm_dist(S.rkx[1], S.rky[1], r, tc);
+            double sc, cc;
+            sincos(tc, &sc, &cc);
+            const double x = r * cc, y = r * sc;
+            double d0 = gm_dist_xy(x, y, S.rkx[0], S.rky[0]);
+            double d1 = gm_dist_xy(x, y, S.rkx[1], S.rky[1]);
             double eps = P.g_eps;
             nu = P.visc * Pp / rho /
                  sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.grk_M[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.grk_M[1]);
@@ -888,33 +895,6 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux(DevPtrs d, int sub
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
-  if (t < d.n_ann) {
-    // per-annulus constants of this substep for k_update: the epicyclic rotation
-    // of cell_add_split_fictitious (cell_add_split_fictitious.c:26-38) and the
-    // relaxation factor of cell_bc_damp (cell_misc.c:121), identical for every
-    // cell of the annulus
-    const Annulus &A = d.ann[t];
-    const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const double dt = fac * S.dt;
-    const double r = 0.5 * (A.rm + A.rp);
-    const double a_sep = S.gr[0] + S.gr[1];
-    const double rom = frame_rom(P, A.rom, r, a_sep);
-    const double Omega = rom / r;
-    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
-    const double kappa2 = 2. * Omega / r * dr_r2Om;
-    double kappa = 0.0, ck = 1.0, sk = 0.0;
-    if (kappa2 > 0.) {
-      kappa = sqrt(kappa2);
-      ck = cos(kappa * dt);
-      sk = sin(kappa * dt);
-    }
-    const int NA = d.n_ann;
-    d.ann_c[t] = kappa;
-    d.ann_c[NA + t] = ck;
-    d.ann_c[2 * NA + t] = sk;
-    d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
-  }
   if (t < N) {
     // phi face (j, j+1): riemann_setup_p (Riemann_setup.c:46-80)
     const int g = t;
@@ -1054,14 +1034,178 @@ __device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, dou
   return t;
 }
 
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int substep, int stop, int tail) {
+// Source increments of cell_add_src (src/Cell/cell_source.c:73-214) and
+// cell_add_visc_src (cell_source.c:216-277), per cell, for k_update to add in
+// the reference's order: src[0..4] = S_r (pressure/centrifugal), S_r (gravity
+// + frame), L, S_z, tau; src[5] = viscous heating; src[6+p] = sink mass of mass
+// p.  They read only the substep's primitives, slopes and GravMass positions,
+// so this kernel runs concurrently with k_flux.  Its first n_ann threads also
+// form the per-annulus constants of the substep (epicyclic rotation of
+// cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, int substep) {
   __shared__ double sh_md[2][BLK / 32];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  if (t < d.n_ann) {
+    // per-annulus constants of this substep for k_update: the epicyclic rotation
+    // of cell_add_split_fictitious (cell_add_split_fictitious.c:26-38) and the
+    // relaxation factor of cell_bc_damp (cell_misc.c:121), identical for every
+    // cell of the annulus
+    const Annulus &A = d.ann[t];
+    const DiskParams &P = d.par[A.inst];
+    const InstState &S = d.ist[A.inst];
+    const double dt = fac * S.dt;
+    const double r = 0.5 * (A.rm + A.rp);
+    const double a_sep = S.gr[0] + S.gr[1];
+    const double rom = frame_rom(P, A.rom, r, a_sep);
+    const double Omega = rom / r;
+    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
+    const double kappa2 = 2. * Omega / r * dr_r2Om;
+    double kappa = 0.0, ck = 1.0, sk = 0.0;
+    if (kappa2 > 0.) {
+      kappa = sqrt(kappa2);
+      ck = cos(kappa * dt);
+      sk = sin(kappa * dt);
+    }
+    const int NA = d.n_ann;
+    d.ann_c[t] = kappa;
+    d.ann_c[NA + t] = ck;
+    d.ann_c[2 * NA + t] = sk;
+    d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
+  }
+  double md0 = 0.0, md1 = 0.0;
+  if (t < N) {
+    const int g = t;
+    const int a = d.cell_ann[g];
+    const Annulus &A = d.ann[a];
+    const DiskParams &P = d.par[A.inst];
+    const InstState &S = d.ist[A.inst];
+    const double dt = fac * S.dt;
+    const double a_sep = S.gr[0] + S.gr[1];
+    const double dphi = d.dphi[g];
+    const double rm = A.rm, rp = A.rp;
+    double phi = d.tiphw[g] - .5 * dphi;
+    double rho = ld(d.prim, D_RHO, N, g);
+    double Pp = ld(d.prim, D_PPP, N, g);
+    double r = .5 * (rp + rm);
+    double vr = ld(d.prim, D_URR, N, g);
+    double vz = ld(d.prim, D_UZZ, N, g);
+    double vp = ld(d.prim, D_UPP, N, g) * r;
+    double dz = P.dz;
+    double dV = dphi * .5 * A.dv_diff * dz;
+    double sinp, cosp;
+    sincos(phi, &sinp, &cosp);
+    double xpos = r * cosp;
+    double ypos = r * sinp;
+    double z = P.z;
+    double R = sqrt(r * r + z * z);
+    double sint, cost, gravdist;
+    if (P.grav2d == 1) {
+      sint = 1.0;
+      cost = 0.0;
+      gravdist = r;
+    } else {
+      sint = r / R;
+      cost = z / R;
+      gravdist = R;
+    }
+    double Fr = 0.0, Fp = 0.0;
+    for (int p = 0; p < 2; ++p) {
+      // gravMassForce (src/Cell/cell_source.c:49-71)
+      double dx = gravdist * cosp - S.gx[p];
+      double dy = gravdist * sinp - S.gy[p];
+      double script_r = sqrt(dx * dx + dy * dy);
+      double cosa = dx / script_r;
+      double sina = dy / script_r;
+      double cosap = cosa * cosp + sina * sinp;
+      double sinap = sina * cosp - cosa * sinp;
+      double f1 = -fgrav(S.gM[p], script_r, P.g_eps, P.phi_order);
+      Fr += cosap * f1;
+      Fp += sinap * f1;
+    }
+    double w_a = frame_rom(P, A.rom, r, a_sep);
+    double rdrOm_a = frame_rdrom(P, A.rdrom, r, a_sep);
+    double F_centrifugal_r = w_a * w_a / r;
+    double dtOm_a = frame_dtom(P, A.dtom, r, a_sep);
+    double F_euler_phi = -(r * dtOm_a + vr * rdrOm_a);
+    double *src = d.src;
+    src[g] = dt * dV * (rho * vp * vp + Pp) / r;
+    src[(size_t)N + g] = dt * dV * rho * (Fr * sint + F_centrifugal_r);
+    src[2 * (size_t)N + g] = dt * dV * rho * (Fp - r * dtOm_a) * r;
+    src[3 * (size_t)N + g] = dt * dV * rho * Fr * cost;
+    src[4 * (size_t)N + g] =
+        dt * dV * rho * ((Fr * sint + F_centrifugal_r) * vr + Fr * vz * cost + (Fp + F_euler_phi) * vp);
+    if (P.rho_sink_on == 1) {
+      // get_rho_sink (src/Cell/cell_source.c:15-47)
+      double r0 = sqrt((xpos - S.gx[0]) * (xpos - S.gx[0]) + (ypos - S.gy[0]) * (ypos - S.gy[0]));
+      double r1 = sqrt((xpos - S.gx[1]) * (xpos - S.gx[1]) + (ypos - S.gy[1]) * (ypos - S.gy[1]));
+      double M0 = S.gM[0], M1 = S.gM[1];
+      double Mtotal = M0 + M1;
+      double alpha = P.visc;
+      double one_o_nu = 1.0 / (alpha * Pp / rho) * sqrt(pow(r0, -3) * M0 / Mtotal + pow(r1, -3) * M1 / Mtotal);
+      double t_visc0 = 1.0 * 2. / 3. * r0 * r0 * one_o_nu;
+      double t_visc1 = 1.0 * 2. / 3. * r1 * r1 * one_o_nu;
+      if (t_visc0 < 10. * dt) t_visc0 = 10. * dt;
+      if (t_visc1 < 10. * dt) t_visc1 = 10. * dt;
+      double sink_size = 0.5;
+      for (int p = 0; p < P.num_sinks && p < 2; ++p) {
+        double drho = 0.0;
+        if (p == 0) { if (r0 < sink_size) drho = rho / t_visc0; }
+        else { if (r1 < sink_size) drho = rho / t_visc1; }
+        src[(6 + (size_t)p) * N + g] = drho * dt * dV;
+        if (A.kind & DGPU_AK_SINK_SUM) {
+          if (p == 0) md0 += drho * dV;
+          else md1 += drho * dV;
+        }
+      }
+    }
+    if (P.has_visc) {
+      double dist_bh0 = sqrt((xpos - S.gx[0]) * (xpos - S.gx[0]) + (ypos - S.gy[0]) * (ypos - S.gy[0]));
+      double dist_bh1 = sqrt((xpos - S.gx[1]) * (xpos - S.gx[1]) + (ypos - S.gy[1]) * (ypos - S.gy[1]));
+      double alpha = P.visc;
+      double eps = P.g_eps;
+      double Sigma_nu;
+      if (P.visc_const == 1) {
+        Sigma_nu = rho * alpha;
+      } else {
+        Sigma_nu = alpha * Pp /
+                   sqrt(dpow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
+                        dpow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
+      }
+      src[5 * (size_t)N + g] =
+          dt * dV * Sigma_nu * rdrOm_a * (rdrOm_a + r * ld(d.grad, D_UPP, N, g) + ld(d.gradp, D_URR, N, g));
+    }
+  }
+  // deterministic per-block Mdot partial sums (reduced in block order by k_update)
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    md0 += __shfl_down_sync(full, md0, o);
+    md1 += __shfl_down_sync(full, md1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh_md[0][threadIdx.x >> 5] = md0;
+    sh_md[1][threadIdx.x >> 5] = md1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (size_t)blockIdx.x * BLK < (size_t)N) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < BLK / 32; ++w) {
+      s0 += sh_md[0][w];
+      s1 += sh_md[1][w];
+    }
+    d.mdot_part[2 * blockIdx.x] = s0;
+    d.mdot_part[2 * blockIdx.x + 1] = s1;
+  }
+}
+
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int substep, int stop, int tail) {
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double RK = substep == 1 ? 0.0 : 0.5;
   const double fac = substep == 1 ? 1.0 : 0.5;
-  double md0 = 0.0, md1 = 0.0;
   if (g < N) {
     const int a = d.cell_ann[g];
     const Annulus A = d.ann[a];
@@ -1147,83 +1291,22 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
     const double rm = A.rm, rp = A.rp;
     const double a_sep = S.gr[0] + S.gr[1];
     if (!done) {
-      // cell_add_src (src/Cell/cell_source.c:73-214)
-      double phi = tw - .5 * dphi;
-      double rho = ld(d.prim, D_RHO, N, g);
-      double Pp = ld(d.prim, D_PPP, N, g);
-      double r = .5 * (rp + rm);
-      double vr = ld(d.prim, D_URR, N, g);
-      double vz = ld(d.prim, D_UZZ, N, g);
-      double vp = ld(d.prim, D_UPP, N, g) * r;
-      double dz = P.dz;
-      double dV = dphi * .5 * A.dv_diff * dz;
-      double cosp = cos(phi), sinp = sin(phi);
-      double xpos = r * cosp;
-      double ypos = r * sinp;
-      double z = P.z;
-      double R = sqrt(r * r + z * z);
-      double sint, cost, gravdist;
-      if (P.grav2d == 1) {
-        sint = 1.0;
-        cost = 0.0;
-        gravdist = r;
-      } else {
-        sint = r / R;
-        cost = z / R;
-        gravdist = R;
-      }
-      double Fr = 0.0, Fp = 0.0;
-      double xb[2], yb[2];
-      for (int p = 0; p < 2; ++p) {
-        xb[p] = S.gx[p];
-        yb[p] = S.gy[p];
-        // gravMassForce (src/Cell/cell_source.c:49-71)
-        double dx = gravdist * cosp - S.gx[p];
-        double dy = gravdist * sinp - S.gy[p];
-        double script_r = sqrt(dx * dx + dy * dy);
-        double cosa = dx / script_r;
-        double sina = dy / script_r;
-        double cosap = cosa * cosp + sina * sinp;
-        double sinap = sina * cosp - cosa * sinp;
-        double f1 = -fgrav(S.gM[p], script_r, P.g_eps, P.phi_order);
-        Fr += cosap * f1;
-        Fp += sinap * f1;
-      }
-      double w_a = frame_rom(P, A.rom, r, a_sep);
-      double rdrOm_a = frame_rdrom(P, A.rdrom, r, a_sep);
-      double F_centrifugal_r = w_a * w_a / r;
-      double dtOm_a = frame_dtom(P, A.dtom, r, a_sep);
-      double F_euler_phi = -(r * dtOm_a + vr * rdrOm_a);
-      c[D_SRR] += dt * dV * (rho * vp * vp + Pp) / r;
-      c[D_SRR] += dt * dV * rho * (Fr * sint + F_centrifugal_r);
-      c[D_LLL] += dt * dV * rho * (Fp - r * dtOm_a) * r;
-      c[D_SZZ] += dt * dV * rho * Fr * cost;
-      c[D_TAU] += dt * dV * rho * ((Fr * sint + F_centrifugal_r) * vr + Fr * vz * cost + (Fp + F_euler_phi) * vp);
+      // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
+      // increments come from k_source; added here in the reference's order
+      const double *src = d.src;
+      c[D_SRR] += src[g];
+      c[D_SRR] += src[(size_t)N + g];
+      c[D_LLL] += src[2 * (size_t)N + g];
+      c[D_SZZ] += src[3 * (size_t)N + g];
+      c[D_TAU] += src[4 * (size_t)N + g];
       if (P.rho_sink_on == 1) {
-        // get_rho_sink (src/Cell/cell_source.c:15-47)
-        double r0 = sqrt((xpos - xb[0]) * (xpos - xb[0]) + (ypos - yb[0]) * (ypos - yb[0]));
-        double r1 = sqrt((xpos - xb[1]) * (xpos - xb[1]) + (ypos - yb[1]) * (ypos - yb[1]));
-        double M0 = S.gM[0], M1 = S.gM[1];
-        double Mtotal = M0 + M1;
-        double alpha = P.visc;
-        double one_o_nu = 1.0 / (alpha * Pp / rho) * sqrt(pow(r0, -3) * M0 / Mtotal + pow(r1, -3) * M1 / Mtotal);
-        double t_visc0 = 1.0 * 2. / 3. * r0 * r0 * one_o_nu;
-        double t_visc1 = 1.0 * 2. / 3. * r1 * r1 * one_o_nu;
-        if (t_visc0 < 10. * dt) t_visc0 = 10. * dt;
-        if (t_visc1 < 10. * dt) t_visc1 = 10. * dt;
-        double sink_size = 0.5;
-        for (int p = 0; p < P.num_sinks && p < 2; ++p) {
-          double drho = 0.0;
-          if (p == 0) { if (r0 < sink_size) drho = rho / t_visc0; }
-          else { if (r1 < sink_size) drho = rho / t_visc1; }
-          c[D_DDD] -= drho * dt * dV;
-          if (A.kind & DGPU_AK_SINK_SUM) {
-            if (p == 0) md0 += drho * dV;
-            else md1 += drho * dV;
-          }
-        }
+        for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= src[(6 + (size_t)p) * N + g];
       }
+      const double r = .5 * (rp + rm);
       if (P.cooling == 1) {
+        // cooling reads the running tau (cell_source.c:187-203)
+        const double rho = ld(d.prim, D_RHO, N, g), Pp = ld(d.prim, D_PPP, N, g);
+        const double dV = dphi * .5 * A.dv_diff * P.dz;
         if (P.init_type == DI_SHEAR) {
           double cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
           if (cooling_term < 0.0) cooling_term = 0.0;
@@ -1237,29 +1320,14 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
           c[D_TAU] -= cooling_term;
         }
       }
-      // cell_add_visc_src (src/Cell/cell_source.c:216-277)
-      if (P.has_visc) {
-        double dist_bh0 = sqrt((xpos - xb[0]) * (xpos - xb[0]) + (ypos - yb[0]) * (ypos - yb[0]));
-        double dist_bh1 = sqrt((xpos - xb[1]) * (xpos - xb[1]) + (ypos - yb[1]) * (ypos - yb[1]));
-        double alpha = P.visc;
-        double eps = P.g_eps;
-        double Sigma_nu;
-        if (P.visc_const == 1) {
-          Sigma_nu = rho * alpha;
-        } else {
-          Sigma_nu = alpha * Pp /
-                     sqrt(dpow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
-                          dpow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
-        }
-        c[D_TAU] += dt * dV * Sigma_nu * rdrOm_a * (rdrOm_a + r * ld(d.grad, D_UPP, N, g) + ld(d.gradp, D_URR, N, g));
-      }
+      if (P.has_visc) c[D_TAU] += src[5 * (size_t)N + g];
       // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
       {
-        double rom = w_a;
-        double Omega = rom / r;
-        double dr_r2Om = 2. * rom + r * rdrOm_a;
+        const double rom = frame_rom(P, A.rom, r, a_sep);
+        const double Omega = rom / r;
+        const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
         const int NA = d.n_ann;
-        const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_flux)
+        const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
         if (kappa > 0.) {
           double l0 = c[D_LLL];
           double rhov0 = c[D_SRR];
@@ -1350,30 +1418,6 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
     }
   }
   if (tail == 0) return;
-
-  // deterministic per-block Mdot partial sums
-  {
-    const unsigned full = 0xffffffffu;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      md0 += __shfl_down_sync(full, md0, o);
-      md1 += __shfl_down_sync(full, md1, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-      sh_md[0][threadIdx.x >> 5] = md0;
-      sh_md[1][threadIdx.x >> 5] = md1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s0 = 0.0, s1 = 0.0;
-      for (int w = 0; w < BLK / 32; ++w) {
-        s0 += sh_md[0][w];
-        s1 += sh_md[1][w];
-      }
-      d.mdot_part[2 * blockIdx.x] = s0;
-      d.mdot_part[2 * blockIdx.x + 1] = s1;
-    }
-  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(&d.counters[1], 1u) == gridDim.x - 1;
@@ -1542,8 +1586,12 @@ int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa,
 
 int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
 
-int dgk_face(const DevPtrs *d, int substep, int gm_ops, void *stream) {
-  k_face<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep, gm_ops);
+int dgk_cellprep(const DevPtrs *d, int substep, void *stream) {
+  k_cellprep<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_merge(const DevPtrs *d, int substep, void *stream) {
+  k_merge<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_rslope(const DevPtrs *d, void *stream) {
@@ -1558,6 +1606,11 @@ int dgk_plm_r(const DevPtrs *d, int substep, void *stream) {
 int dgk_flux(const DevPtrs *d, int substep, void *stream) {
   int n = d->n_cells + d->n_slots;
   k_flux<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_source(const DevPtrs *d, int substep, void *stream) {
+  int n = d->n_cells > d->n_ann ? d->n_cells : d->n_ann;
+  k_source<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_update(const DevPtrs *d, int substep, int stop, void *stream) {
