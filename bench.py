@@ -65,6 +65,25 @@ def workload_params(name: str):
     raise SystemExit(f"unknown workload {name}")
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary (one
+    --set full capture of the same workload), or None."""
+    import re
+    path = os.path.join(HERE, "profiles", "step_kernels_circumbinary.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_launch:([^`\n]*)", text)
+    if not m:
+        return None
+    for tok in m.group(1).split():
+        k, _, v = tok.partition("=")
+        if k == "k_" + kernel:
+            return float(v)
+    return None
+
+
 def load_peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -411,8 +430,10 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single disk"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "alg_bytes_per_launch": alg_bytes,
-                         "ms_per_launch": per_kernel[dom]},
+                         "traffic": profiled_traffic(dom) if args.workload == "circumbinary" else None,
+                         "alg_bytes_per_launch": alg_bytes,
+                         "ms_per_launch": per_kernel[dom],
+                         "traffic_source": "profiles/step_kernels_circumbinary.md (ncu dram__bytes_read+write, one launch)"},
             "step_roofline": {"alg_bytes_per_zone_update": STEP_ALG_BYTES,
                               "achieved_gbs": value / world * STEP_ALG_BYTES / 1e9,
                               "frac": value / world * STEP_ALG_BYTES / 1e9 / peak},
