@@ -36,7 +36,7 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Compulsory DRAM bytes per unit for each kernel as designed (each array
 # element touched once): per cell and per r-face of one substep.
-KERNELS = ["cellprep", "merge", "rslope", "plm_r", "source", "flux", "update"]
+KERNELS = ["cellprep", "merge", "rslope", "plm_r", "source", "flux_phi", "flux_r", "update"]
 ALG_BYTES = {
     # name: (bytes per cell, bytes per r-face)
     "cellprep": (8 + 8 + 40 + 8 + 40, 0),
@@ -44,7 +44,8 @@ ALG_BYTES = {
     "rslope": (40 + 40 + 8 + 8, 24 + 40 + 16),
     "plm_r": (8 + 4 + 40, 24 + 40),
     "source": (40 + 8 + 8 + 16 + 64, 0),
-    "flux": (40 + 40 + 40 + 8 + 8 + 64, 24 + 16 + 64),
+    "flux_phi": (40 + 40 + 40 + 8 + 8 + 64, 0),
+    "flux_r": (0, 8 + 16 + 16 + 64 + 2 * (40 + 40 + 40 + 8)),
     "update": (40 + 40 + 40 + 8 + 8 + 8 + 8 + 64 + 64 + 8 + 40 + 40 + 8 + 8 + 8, 64),
 }
 STEP_ALG_BYTES = 240  # per zone-update: 5 conserved + 1 phi edge, read/written across 2 stages

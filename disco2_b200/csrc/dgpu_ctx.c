@@ -229,7 +229,7 @@ void dgpu_destroy(dgpu_ctx *c) {
   {
     void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
-                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
+                  c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.rr, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
                   c->d.mdot_part, c->d.counters, c->d.err, c->d_stage, c->d_torque};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
@@ -374,6 +374,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.fdp = (double *)dmalloc(sizeof(double) * 2 * (S ? S : 1), &ok);
     c->d.ann_c = (double *)dmalloc(sizeof(double) * 4 * A, &ok);
     c->d.fstart = (int *)dmalloc(sizeof(int) * N, &ok);
+    c->d.rr = (int *)dmalloc(sizeof(int) * 4 * N, &ok);
     c->d.fL = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
     c->d.fR = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
     c->d.fdphi = (double *)dmalloc(sizeof(double) * (S ? S : 1), &ok);
@@ -658,11 +659,12 @@ static int launch_step(struct dgpu_ctx *c) {
     CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
     CKK(dgk_rslope(&c->d, c->stream));
     CKK(dgk_plm_r(&c->d, sub, c->stream));
-    /* k_source (per cell) alongside k_flux (per face) */
+    /* k_source and the phi faces (per cell) alongside the r faces (per face) */
     CK(cudaEventRecord(c->fork[2], c->stream));
     CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
     CKK(dgk_source(&c->d, sub, c->side));
-    CKK(dgk_flux(&c->d, sub, c->stream));
+    CKK(dgk_flux_phi(&c->d, sub, c->side));
+    CKK(dgk_flux_r(&c->d, sub, c->stream));
     CK(cudaEventRecord(c->fork[3], c->side));
     CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
     CKK(dgk_update(&c->d, sub, 7, c->stream));
@@ -715,7 +717,9 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_source(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_flux(&c->d, sub, c->stream));
+      CKK(dgk_flux_phi(&c->d, sub, c->stream));
+      CK(cudaEventRecord(ev[e++], c->stream));
+      CKK(dgk_flux_r(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_update(&c->d, sub, 7, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
@@ -740,7 +744,10 @@ int dgpu_stage(dgpu_ctx *c, int phase) {
   CKK(dgk_rslope(&c->d, c->stream));
   CKK(dgk_plm_r(&c->d, 1, c->stream));
   CKK(dgk_source(&c->d, 1, c->stream));
-  if (phase >= 2) CKK(dgk_flux(&c->d, 1, c->stream));
+  if (phase >= 2) {
+    CKK(dgk_flux_phi(&c->d, 1, c->stream));
+    CKK(dgk_flux_r(&c->d, 1, c->stream));
+  }
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
   /* from phase 5 on the advanced phi edges live in the substep's output buffer */
   if (phase >= 5)
@@ -789,13 +796,12 @@ int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, dou
     int n = 0;
     for (i = 0; i < s->NR - 1; ++i) {
       const Annulus *A = &c->h_ann[p->ann_base + i];
-      const Annulus *B = &c->h_ann[p->ann_base + i + 1];
       int f;
       if (nri) nri[i] = n;
       for (f = 0; f < nf[i]; ++f, ++n) {
         int slot = A->face_base + f;
-        if (L) L[n] = A->cell_off - p->cell_base + fL[slot];
-        if (R) R[n] = B->cell_off - p->cell_base + fR[slot];
+        if (L) L[n] = fL[slot] - p->cell_base;
+        if (R) R[n] = fR[slot] - p->cell_base;
         if (r) r[n] = A->f_r;
         if (dphi) dphi[n] = fd[slot];
         if (dA) dA[n] = A->f_r * fd[slot] * A->f_dperp;

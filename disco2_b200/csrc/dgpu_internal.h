@@ -18,7 +18,7 @@
 #define DGPU_FACE_SLACK 8
 #define DGPU_RUN_SLACK 8
 #define DGPU_WRAP_LIMIT 64
-#define DGPU_STEP_KERNELS 14 /* launches per RK2 step: 7 per substep */
+#define DGPU_STEP_KERNELS 16 /* launches per RK2 step: 8 per substep */
 
 /* enums of src/Headers/header.h:1-13 */
 enum { D_RHO, D_PPP, D_URR, D_UPP, D_UZZ };
@@ -128,7 +128,9 @@ typedef struct {
   double *ann_c;          /* [4][n_ann] per substep: kappa, cos(kappa dt), sin(kappa dt), 1-exp(-rate dt) */
   int smem_face;          /* dynamic shared bytes of k_face (0: merge reads global memory) */
   int *fstart;            /* first r-face (within the pair slab) of each inner cell */
-  int *fL, *fR;           /* r-face cells (local j of inner / outer annulus) */
+  int *rr;                /* [n_cells][4] r-face ranges (within the slab of pair i-1) of each outer cell:
+                             [x, y) and [z, w) for its two runs; z = INT_MIN: more runs */
+  int *fL, *fR;           /* r-face cells (global cell numbers); fL = -1 past the list of a pair */
   double *fdphi, *fcm;    /* r-face dphi and cm */
   int *pair_nf, *pair_jpmin, *pair_T, *pair_seq; /* per annulus (pair i, i+1) */
   int *runs;              /* run starts */
@@ -146,7 +148,8 @@ int dgk_merge(const DevPtrs *d, int substep, void *stream);
 int dgk_source(const DevPtrs *d, int substep, void *stream);
 int dgk_rslope(const DevPtrs *d, void *stream);
 int dgk_plm_r(const DevPtrs *d, int substep, void *stream);
-int dgk_flux(const DevPtrs *d, int substep, void *stream);
+int dgk_flux_phi(const DevPtrs *d, int substep, void *stream);
+int dgk_flux_r(const DevPtrs *d, int substep, void *stream);
 int dgk_update(const DevPtrs *d, int substep, int stop, void *stream);
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
 int dgk_calc_cons(const DevPtrs *d, void *stream);

@@ -21,6 +21,7 @@
 // order and rounding (double '/' and sqrt are IEEE-rounded on the GPU), so
 // paths without transcendentals reproduce the reference bit for bit.
 #include <cuda_runtime.h>
+#include <climits>
 #include <math.h>
 #include <stdint.h>
 
@@ -177,7 +178,7 @@ __device__ __forceinline__ void prim2cons(const double *p, double *U, double r, 
   U[D_TAU] = (.5 * rho * v2 + rhoe) * dV;
 }
 
-__device__ void riemann_flux(const double *pL, const double *pR, double r, int dir, double w, double gam,
+__device__ __forceinline__ void riemann_flux(const double *pL, const double *pR, double r, int dir, double w, double gam,
                              int solver, double *F) {
   const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = 0.0;
   double vnL, cf2L, vnR, cf2R;
@@ -277,7 +278,7 @@ struct ViscIn {
   double rdr_om;                // sim_rdrOm_a at r
 };
 
-__device__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const InstState &S,
+__device__ __forceinline__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const InstState &S,
                           const double *gx, const double *gy, double *Fv, int *err) {
   const double r = v.r;
   double Avg[5], Gr[5], Gp[5];
@@ -355,6 +356,7 @@ struct FaceCtx {
   int *fstart;  // fstart of the inner annulus cells (indexed by j)
   int cap, rcap;
   int *err;
+  int offL, offR;  // global cell numbers of inner/outer cell 0 (face records hold global cells)
 };
 
 // The body of the reference's j loop for inner cell j starting at outer cell
@@ -368,8 +370,8 @@ __device__ void face_cell(const FaceCtx &c, int j, int &jp, int &n, int &s) {
   auto emit = [&](double dphi, double tp) {
     if (FILL) {
       if (n < c.cap) {
-        c.fL[n] = j;
-        c.fR[n] = jp;
+        c.fL[n] = c.offL + j;
+        c.fR[n] = c.offR + jp;
         c.fdphi[n] = dphi;
         c.fcm[n] = tp - .5 * dphi;
       }
@@ -547,6 +549,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
     c.cap = A.face_cap;
     c.rcap = A.run_cap;
     c.err = d.err;
+    c.offL = off;
+    c.offR = offo;
     const double p0 = c.tin[np - 1];
 
     // jpmin: first outer cell with the smallest wrap(tiph - p0), start (PHIMAX, 0)
@@ -653,6 +657,25 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
         d.pair_seq[a] = 1;
       }
     }
+    __syncthreads();
+    // per outer cell, the face ranges of its runs s = jp - jpmin (mod Nout) and
+    // s + Nout (the cell at the wrap point); z = INT_MIN flags a third run
+    {
+      const int nf = d.pair_nf[a], T = d.pair_T[a];
+      for (int jq = tid; jq < npo; jq += nt) {
+        int4 rr = make_int4(0, 0, 0, 0);
+        if (nf > 0) {
+          int s0 = jq - jpmin;
+          if (s0 < 0) s0 += npo;
+          if (s0 <= T) rr.x = c.runs[s0], rr.y = c.runs[s0 + 1];
+          if (s0 + npo <= T) rr.z = c.runs[s0 + npo], rr.w = c.runs[s0 + npo + 1];
+          if (s0 + 2 * npo <= T) rr.z = INT_MIN;
+        }
+        reinterpret_cast<int4 *>(d.rr)[offo + jq] = rr;
+      }
+      // slab slots past the list hold no face
+      for (int n = nf + tid; n < c.cap; n += nt) c.fL[n] = -1;
+    }
   }
   // C_RIGID: the mass-weighted mean v_phi of the annulus, summed in j order
   // like the reference (cell_set_w.c:41-49); one lane, after the merge
@@ -686,40 +709,42 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
   const int j = g - A.cell_off;
   if (A.i > 0) {
     const Annulus &Q = d.ann[a - 1];
-    const int nf = d.pair_nf[a - 1];
-    const int T = d.pair_T[a - 1];
-    const int jpmin = d.pair_jpmin[a - 1];
-    if (nf > 0) {
+    const int4 rr = reinterpret_cast<const int4 *>(d.rr)[g];
+    auto one = [&](int n) {
+      RFace F;
+      F.cL = d.fL[Q.face_base + n];
+      F.cR = g;
+      F.dphi = d.fdphi[Q.face_base + n];
+      F.cm = d.fcm[Q.face_base + n];
+      F.r = Q.f_r;
+      F.dl = Q.f_dl;
+      F.dr = Q.f_dr;
+      F.dperp = Q.f_dperp;
+      f(F, Q.face_base + n, 1);
+    };
+    if (rr.z != INT_MIN) {
+      for (int n = rr.x; n < rr.y; ++n) one(n);
+      for (int n = rr.z; n < rr.w; ++n) one(n);
+    } else {
+      // three or more runs (the outer pointer went round more than twice)
+      const int T = d.pair_T[a - 1];
+      const int jpmin = d.pair_jpmin[a - 1];
       int dd = j - jpmin;
       if (dd < 0) dd += A.np;
       const int *runs = d.runs + Q.run_base;
-      for (int s = dd; s <= T; s += A.np) {
-        int n0 = runs[s], n1 = runs[s + 1];
-        for (int n = n0; n < n1; ++n) {
-          RFace F;
-          F.cL = Q.cell_off + d.fL[Q.face_base + n];
-          F.cR = g;
-          F.dphi = d.fdphi[Q.face_base + n];
-          F.cm = d.fcm[Q.face_base + n];
-          F.r = Q.f_r;
-          F.dl = Q.f_dl;
-          F.dr = Q.f_dr;
-          F.dperp = Q.f_dperp;
-          f(F, Q.face_base + n, 1);
-        }
-      }
+      for (int s = dd; s <= T; s += A.np)
+        for (int n = runs[s]; n < runs[s + 1]; ++n) one(n);
     }
   }
   if (A.i < NR - 1) {
     const int nf = d.pair_nf[a];
-    const Annulus &B = d.ann[a + 1];
     int n0 = d.fstart[g];
     int n1 = (j + 1 < A.np) ? d.fstart[g + 1] : nf;
     if (nf <= 0) n1 = n0;
     for (int n = n0; n < n1; ++n) {
       RFace F;
       F.cL = g;
-      F.cR = B.cell_off + d.fR[A.face_base + n];
+      F.cR = d.fR[A.face_base + n];
       F.dphi = d.fdphi[A.face_base + n];
       F.cm = d.fcm[A.face_base + n];
       F.r = A.f_r;
@@ -738,13 +763,12 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
 __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= d.n_slots) return;
+  const int cL = d.fL[slot];
+  if (cL < 0) return;  // slot past the face list of its pair
+  const int cR = d.fR[slot];
   const int a = d.slot_ann[slot];
-  if (a < 0) return;
   const Annulus &A = d.ann[a];
-  if (slot - A.face_base >= d.pair_nf[a]) return;
   const int N = d.n_cells, NS = d.n_slots;
-  const int cL = A.cell_off + d.fL[slot];
-  const int cR = d.ann[a + 1].cell_off + d.fR[slot];
   const double cm = d.fcm[slot];
   double pL = d.tiphw[cL] - .5 * d.dphi[cL];
   double pR = d.tiphw[cR] - .5 * d.dphi[cR];
@@ -891,80 +915,82 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int sub
 // ---------------------------------------------------------------------------
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux(DevPtrs d, int substep) {
+// phi faces: thread per cell j, face (j, j+1) (riemann_setup_p, Riemann_setup.c:46-80)
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
-  if (t < N) {
+  if (t >= N) return;
     // phi face (j, j+1): riemann_setup_p (Riemann_setup.c:46-80)
-    const int g = t;
-    const int a = d.cell_ann[g];
-    const Annulus A = d.ann[a];
-    const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const int j = g - A.cell_off;
-    const int cL = g, cR = (j == A.np - 1) ? A.cell_off : g + 1;
-    const double dpL = d.dphi[cL], dpR = d.dphi[cR];
-    const double dz = P.dz;
-    const double dr = A.rp - A.rm;
-    const double r = .5 * (A.rp + A.rm);
-    const double dA = dr * dz;
-    double pL[5], pR[5];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      pL[q] = ld(d.prim, q, N, cL) + 0.5 * ld(d.gradp, q, N, cL) * dpL;
-      pR[q] = ld(d.prim, q, N, cR) - 0.5 * ld(d.gradp, q, N, cR) * dpR;
-    }
-    const double w = d.w_ann[a];
-    double F[5];
-    riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F);
-    const double dt = fac * S.dt;
-    const double k = dt * dA;
-    double *out = d.fphi;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) out[(size_t)q * N + g] = k * F[q];
-    if (P.has_visc) {
-      ViscIn v;
-      v.pL = pL;
-      v.pR = pR;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        v.cL[q] = ld(d.prim, q, N, cL);
-        v.cR[q] = ld(d.prim, q, N, cR);
-        v.gpL[q] = ld(d.gradp, q, N, cL);
-        v.gpR[q] = ld(d.gradp, q, N, cR);
-        v.grL[q] = ld(d.grad, q, N, cL);
-        v.grR[q] = ld(d.grad, q, N, cR);
-      }
-      v.tL = d.tiphw[cL];
-      v.tR = d.tiphw[cR];
-      v.dpL = v.dpR = 0.0;
-      v.r = r;
-      v.cm = d.tiphw[cL];
-      v.r_cell_L = r;
-      v.r_cell_R = r;
-      double a_sep = S.gr[0] + S.gr[1];
-      v.rdr_om = frame_rdrom(P, A.rdrom, r, a_sep);
-      double Fv[3];
-      visc_flux(v, 1, P, S, S.gx, S.gy, Fv, d.err);
-#pragma unroll
-      for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * N + g] = k * Fv[q];
-    }
-    return;
-  }
-  const int slot = t - N;
-  if (slot >= d.n_slots) return;
-  const int a = d.slot_ann[slot];
-  if (a < 0) return;
+  const int g = t;
+  const int a = d.cell_ann[g];
   const Annulus A = d.ann[a];
-  const int n = slot - A.face_base;
-  if (n >= d.pair_nf[a]) return;
-  // r face: riemann_setup_rz (Riemann_setup.c:11-44)
   const DiskParams &P = d.par[A.inst];
   const InstState &S = d.ist[A.inst];
-  const Annulus &B = d.ann[a + 1];
-  const int cL = A.cell_off + d.fL[slot];
-  const int cR = B.cell_off + d.fR[slot];
+  const int j = g - A.cell_off;
+  const int cL = g, cR = (j == A.np - 1) ? A.cell_off : g + 1;
+  const double dpL = d.dphi[cL], dpR = d.dphi[cR];
+  const double dz = P.dz;
+  const double dr = A.rp - A.rm;
+  const double r = .5 * (A.rp + A.rm);
+  const double dA = dr * dz;
+  double pL[5], pR[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    pL[q] = ld(d.prim, q, N, cL) + 0.5 * ld(d.gradp, q, N, cL) * dpL;
+    pR[q] = ld(d.prim, q, N, cR) - 0.5 * ld(d.gradp, q, N, cR) * dpR;
+  }
+  const double w = d.w_ann[a];
+  double F[5];
+  riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F);
+  const double dt = fac * S.dt;
+  const double k = dt * dA;
+  double *out = d.fphi;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) out[(size_t)q * N + g] = k * F[q];
+  if (P.has_visc) {
+    ViscIn v;
+    v.pL = pL;
+    v.pR = pR;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      v.cL[q] = ld(d.prim, q, N, cL);
+      v.cR[q] = ld(d.prim, q, N, cR);
+      v.gpL[q] = ld(d.gradp, q, N, cL);
+      v.gpR[q] = ld(d.gradp, q, N, cR);
+      v.grL[q] = ld(d.grad, q, N, cL);
+      v.grR[q] = ld(d.grad, q, N, cR);
+    }
+    v.tL = d.tiphw[cL];
+    v.tR = d.tiphw[cR];
+    v.dpL = v.dpR = 0.0;
+    v.r = r;
+    v.cm = d.tiphw[cL];
+    v.r_cell_L = r;
+    v.r_cell_R = r;
+    double a_sep = S.gr[0] + S.gr[1];
+    v.rdr_om = frame_rdrom(P, A.rdrom, r, a_sep);
+    double Fv[3];
+    visc_flux(v, 1, P, S, S.gx, S.gy, Fv, d.err);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * N + g] = k * Fv[q];
+  }
+}
+
+// r faces: thread per face slot (riemann_setup_rz, Riemann_setup.c:11-44)
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, int substep) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  const int slot = t;
+  if (slot >= d.n_slots) return;
+  const int cL = d.fL[slot];
+  if (cL < 0) return;  // slot past the face list of its pair
+  const int cR = d.fR[slot];
+  const int a = d.slot_ann[slot];
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  const InstState &S = d.ist[A.inst];
   const double fdphi = d.fdphi[slot], cm = d.fcm[slot];
   const double deltaL = A.f_dl, deltaR = A.f_dr;
   const double dpL = d.fdp[slot];
@@ -1603,9 +1629,13 @@ int dgk_plm_r(const DevPtrs *d, int substep, void *stream) {
   k_plm_r<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
-int dgk_flux(const DevPtrs *d, int substep, void *stream) {
-  int n = d->n_cells + d->n_slots;
-  k_flux<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+int dgk_flux_phi(const DevPtrs *d, int substep, void *stream) {
+  k_flux_phi<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_flux_r(const DevPtrs *d, int substep, void *stream) {
+  if (d->n_slots <= 0) return 0;
+  k_flux_r<<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_source(const DevPtrs *d, int substep, void *stream) {
@@ -1760,6 +1790,7 @@ __device__ FaceCtx noalloc_ctx(const NoallocScratch *S, int i, const double *tip
   c.runs = c.fstart = nullptr;
   c.cap = c.rcap = 0;
   c.err = err;
+  c.offL = c.offR = 0;
   return c;
 }
 

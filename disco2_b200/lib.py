@@ -214,7 +214,7 @@ class Context:
         if sync:
             self.synchronize()
 
-    KERNELS = ("cellprep", "merge", "rslope", "plm_r", "source", "flux", "update")
+    KERNELS = ("cellprep", "merge", "rslope", "plm_r", "source", "flux_phi", "flux_r", "update")
 
     def step_timed(self, nsteps: int = 1) -> np.ndarray:
         """Per-kernel device milliseconds summed over nsteps (KERNELS of substep 1,

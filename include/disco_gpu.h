@@ -109,10 +109,10 @@ int dgpu_step_rk2(dgpu_ctx *ctx, int nsteps);
 int dgpu_synchronize(dgpu_ctx *ctx);
 /* The same steps launched one kernel at a time with CUDA events between the
  * kernels on the context's stream (no graph); adds each kernel's device time in
- * milliseconds to kernel_ms[14] (cellprep, merge, rslope, plm_r, source, flux,
- * update of substep 1, then of substep 2).  Synchronous.  For measurement
- * only: inside the step graph merge runs beside cellprep and source beside
- * flux. */
+ * milliseconds to kernel_ms[16] (cellprep, merge, rslope, plm_r, source,
+ * flux_phi, flux_r, update of substep 1, then of substep 2).  Synchronous.
+ * For measurement only: inside the step graph merge runs beside cellprep, and
+ * source and flux_phi beside flux_r. */
 int dgpu_step_rk2_timed(dgpu_ctx *ctx, int nsteps, double *kernel_ms);
 /* Stage parity: the prologue of timestep_rk2 and the first substep
  * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`
