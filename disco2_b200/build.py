@@ -24,7 +24,7 @@ CC = shutil.which("gcc") or "gcc"
 
 C_SOURCES = ["dgpu_sim.c", "dgpu_ctx.c"]
 CU_SOURCES = ["dgpu_kernels.cu"]
-HEADERS = ["dgpu_internal.h", "dgpu_sim.h"]
+HEADERS = ["dgpu_internal.h", "dgpu_sim.h", "dgpu_device.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false",

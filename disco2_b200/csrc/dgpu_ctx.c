@@ -475,7 +475,7 @@ static int upload_disk(struct dgpu_ctx *c, int inst, const double *prim, const d
   }
   if (tiph) CK(cudaMemcpyAsync(c->d.tiph0 + base, tiph, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
   if (dphi) CK(cudaMemcpyAsync(c->d.dphi + base, dphi, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-  CKK(dgk_calc_cons(&c->d, c->stream));
+  CKK(dgk_calc_cons(&c->d, NULL, c->stream));
   return DGPU_OK;
 }
 
@@ -654,20 +654,20 @@ static int launch_step(struct dgpu_ctx *c) {
     CK(cudaEventRecord(c->fork[0], c->stream));
     CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
     CKK(dgk_merge(&c->d, sub, c->side));
-    CKK(dgk_cellprep(&c->d, sub, c->stream));
+    CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
     CK(cudaEventRecord(c->fork[1], c->side));
     CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
-    CKK(dgk_rslope(&c->d, c->stream));
-    CKK(dgk_plm_r(&c->d, sub, c->stream));
+    CKK(dgk_rslope(&c->d, NULL, c->stream));
+    CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
     /* k_source and the phi faces (per cell) alongside the r faces (per face) */
     CK(cudaEventRecord(c->fork[2], c->stream));
     CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
-    CKK(dgk_source(&c->d, sub, c->side));
-    CKK(dgk_flux_phi(&c->d, sub, c->side));
-    CKK(dgk_flux_r(&c->d, sub, c->stream));
+    CKK(dgk_source(&c->d, NULL, sub, c->side));
+    CKK(dgk_flux_phi(&c->d, NULL, sub, c->side));
+    CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
     CK(cudaEventRecord(c->fork[3], c->side));
     CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
-    CKK(dgk_update(&c->d, sub, 7, c->stream));
+    CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
   }
   return DGPU_OK;
 }
@@ -707,21 +707,21 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
     int e = 0;
     CK(cudaEventRecord(ev[e++], c->stream));
     for (sub = 1; sub <= 2; ++sub) {
-      CKK(dgk_cellprep(&c->d, sub, c->stream));
+      CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_merge(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_rslope(&c->d, c->stream));
+      CKK(dgk_rslope(&c->d, NULL, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_plm_r(&c->d, sub, c->stream));
+      CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_source(&c->d, sub, c->stream));
+      CKK(dgk_source(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_flux_phi(&c->d, sub, c->stream));
+      CKK(dgk_flux_phi(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_flux_r(&c->d, sub, c->stream));
+      CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
-      CKK(dgk_update(&c->d, sub, 7, c->stream));
+      CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
     }
     CK(cudaEventSynchronize(ev[DGPU_STEP_KERNELS]));
@@ -738,15 +738,15 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
 int dgpu_stage(dgpu_ctx *c, int phase) {
   if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
-  CKK(dgk_cellprep(&c->d, 1, c->stream));
+  CKK(dgk_cellprep(&c->d, NULL, 1, c->stream));
   CKK(dgk_merge(&c->d, 1, c->stream));
   /* the CFL minimum (and dt) come from k_plm_r; PLM results are kept only from phase 1 on */
-  CKK(dgk_rslope(&c->d, c->stream));
-  CKK(dgk_plm_r(&c->d, 1, c->stream));
-  CKK(dgk_source(&c->d, 1, c->stream));
+  CKK(dgk_rslope(&c->d, NULL, c->stream));
+  CKK(dgk_plm_r(&c->d, NULL, 1, c->stream));
+  CKK(dgk_source(&c->d, NULL, 1, c->stream));
   if (phase >= 2) {
-    CKK(dgk_flux_phi(&c->d, 1, c->stream));
-    CKK(dgk_flux_r(&c->d, 1, c->stream));
+    CKK(dgk_flux_phi(&c->d, NULL, 1, c->stream));
+    CKK(dgk_flux_r(&c->d, NULL, 1, c->stream));
   }
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
   /* from phase 5 on the advanced phi edges live in the substep's output buffer */

@@ -43,6 +43,7 @@ enum { DR_HLLC, DR_HLL };
 #define DGPU_AK_DAMP 4       /* inside a damping zone (cell_misc.c:98-132) */
 #define DGPU_AK_SINK_SUM 8   /* counted in the Mdot sum (cell_source.c:80-88,181) */
 #define DGPU_AK_IC 16        /* boundary profile ic[] is defined for this annulus */
+#define DGPU_AK_MDOT 32      /* innermost non-ghost annulus: the accretion-rate objective */
 
 /* Per-disk parameters (constant during a run). */
 typedef struct {
@@ -139,20 +140,40 @@ typedef struct {
   int *err;               /* error flags */
 } DevPtrs;
 
+/* Forward-mode tangent: d/de of the state and of the substep intermediates
+ * along one direction e, in the layouts of the matching DevPtrs arrays.
+ * Only the arrays that depend on the state, on the mass ratio q or on alpha
+ * have tangents: the mesh (phi edges, face list, geometry), the frozen dt and
+ * the GravMass orbit phases do not. */
+#define DGPU_TP_DM0 0   /* dM_0/de  */
+#define DGPU_TP_DM1 1   /* dM_1/de  */
+#define DGPU_TP_DR0 2   /* dr_0/de (orbit radius of mass 0) */
+#define DGPU_TP_DR1 3   /* dr_1/de  */
+#define DGPU_TP_DALPHA 4/* dalpha/de */
+#define DGPU_TP_N 8     /* per-disk stride of TanPtrs.seed */
+typedef struct {
+  double *prim, *cons, *rkcons, *grad, *gradp; /* [5][n_cells] */
+  double *fS;                                  /* [5][n_slots] */
+  double *fphi, *src;                          /* [8][n_cells] */
+  double *frf;                                 /* [8][n_slots] */
+  const double *seed;                          /* [n_inst][DGPU_TP_N] */
+} TanPtrs;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
-/* kernel launchers (dgpu_kernels.cu); return cudaError_t as int */
-int dgk_cellprep(const DevPtrs *d, int substep, void *stream);
+/* kernel launchers (dgpu_kernels.cu); return cudaError_t as int.  t = NULL
+ * launches the forward kernels, t != NULL their tangent instances. */
+int dgk_cellprep(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_merge(const DevPtrs *d, int substep, void *stream);
-int dgk_source(const DevPtrs *d, int substep, void *stream);
-int dgk_rslope(const DevPtrs *d, void *stream);
-int dgk_plm_r(const DevPtrs *d, int substep, void *stream);
-int dgk_flux_phi(const DevPtrs *d, int substep, void *stream);
-int dgk_flux_r(const DevPtrs *d, int substep, void *stream);
-int dgk_update(const DevPtrs *d, int substep, int stop, void *stream);
+int dgk_source(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
+int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream);
+int dgk_plm_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
+int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
+int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
+int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream);
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
-int dgk_calc_cons(const DevPtrs *d, void *stream);
+int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream);
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
 int dgk_update_blocks(int n_cells);
 int dgk_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n, void *stream);

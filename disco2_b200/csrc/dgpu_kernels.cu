@@ -25,10 +25,10 @@
 #include <math.h>
 #include <stdint.h>
 
-#include "dgpu_internal.h"
+#include <type_traits>
 
-#define PHIMAX (2.0 * M_PI)
-#define BLK 256
+#include "dgpu_device.cuh"
+
 // minimum resident blocks per SM requested from the register allocator
 // (measured on B200, circumbinary disk: these kernels are latency-bound, so
 // occupancy beats the extra spills)
@@ -47,302 +47,6 @@
 
 namespace {
 
-__device__ __forceinline__ void set_err(int *err, int flag) { atomicOr(err, flag); }
-
-// while(dp > PHIMAX) dp -= PHIMAX; while(dp < 0.0) dp += PHIMAX;  (bounded)
-__device__ __forceinline__ double wrap_pos(double dp, int *err) {
-  int it = 0;
-  while (dp > PHIMAX) {
-    dp -= PHIMAX;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
-  }
-  while (dp < 0.0) {
-    dp += PHIMAX;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
-  }
-  return dp;
-}
-// while(dp > PHIMAX/2.) dp -= PHIMAX; while(dp < -PHIMAX/2.) dp += PHIMAX;  (bounded)
-__device__ __forceinline__ double wrap_pm(double dp, int *err) {
-  int it = 0;
-  while (dp > PHIMAX / 2.) {
-    dp -= PHIMAX;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
-  }
-  while (dp < -PHIMAX / 2.) {
-    dp += PHIMAX;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return dp; }
-  }
-  return dp;
-}
-
-// while (x - y > h) y += p; while (x - y < -h) y -= p;  (bounded: the RK phase
-// adjustments of cell_update_phi and gravMass_update_RK)
-__device__ __forceinline__ double adjust_toward(double x, double y, double h, double per, int *err) {
-  int it = 0;
-  while (x - y > h) {
-    y += per;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return y; }
-  }
-  while (x - y < -h) {
-    y -= per;
-    if (++it > DGPU_WRAP_LIMIT) { set_err(err, DGPU_EF_WRAP_LIMIT); return y; }
-  }
-  return y;
-}
-
-// pow for the exponents the step uses: x^1 = x and x^2 = x*x are the correctly
-// rounded values; x^1.5 = x*sqrt(x) and x^-1.5 = 1/(x*sqrt(x)) are within 2 ulp
-// (like CUDA's pow, which also differs from the host libm in the last ulp).
-__device__ __forceinline__ double dpow(double x, double y) {
-  if (y == 1.0) return x;
-  if (y == 2.0) return x * x;
-  if (y == 1.5) return x * sqrt(x);
-  if (y == -1.5) return 1.0 / (x * sqrt(x));
-  return pow(x, y);
-}
-
-// sim_rOm_a / sim_rdrOm_a / sim_dtOm_a for A_MILOS (src/Sim/sim_w_a.c:8-72);
-// other frame types use the host-computed annulus tables.
-__device__ double milos_rom(double r, double a) {
-  const int n = 8;
-  return r * (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
-}
-__device__ double milos_rdrom(double r, double a) {
-  const int n = 8;
-  double Omega_a = (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
-  double arn = pow(a / r, n);
-  return ((-1.5 + n * arn / (1. + arn)) * Omega_a +
-          (1.5 - n) * pow(a / r, n - 1.5) / (1. + arn) * pow(r, -1.5));
-}
-__device__ double milos_dtom(double r, double a, double tau) {
-  const int n = 8;
-  double a0 = 1.0;
-  double dta_o_a = -.25 * pow(a / a0, -4) / tau;
-  double Omega_a = (pow(r, n - 1.5) + pow(a, n - 1.5)) / (pow(r, n) + pow(a, n));
-  double arn = pow(a / r, n);
-  if (a > 0.0) return (dta_o_a * (Omega_a * (-1.5 + n / (1. + arn)) + (1.5 - n) * pow(r, -1.5) / (1. + arn)));
-  return 0.0;
-}
-__device__ __forceinline__ double frame_rom(const DiskParams &P, double tab, double r, double a) {
-  return P.w_analytic == DA_MILOS ? milos_rom(r, a) : tab;
-}
-__device__ __forceinline__ double frame_rdrom(const DiskParams &P, double tab, double r, double a) {
-  return P.w_analytic == DA_MILOS ? milos_rdrom(r, a) : tab;
-}
-__device__ __forceinline__ double frame_dtom(const DiskParams &P, double tab, double r, double a) {
-  return P.w_analytic == DA_MILOS ? milos_dtom(r, a, P.orb_tscale) : tab;
-}
-
-// gravMass_dist (src/GravMass/GravMass_access.c:25-31) from the point's
-// x = r cos(phi), y = r sin(phi) and the mass position (xbh, ybh).
-__device__ __forceinline__ double gm_dist_xy(double x, double y, double xbh, double ybh) {
-  double z = 0.;
-  return sqrt((x - xbh) * (x - xbh) + (y - ybh) * (y - ybh) + z * z);
-}
-
-// ---------------------------------------------------------------------------
-// Riemann solver: riemann_set_vel / _set_state / _set_flux / _set_star_hll /
-// _set_star_hllc and the flux choice of riemann_AddFlux
-// (src/Riemann/Riemann_routines.c:14-191,314-371).  dir 0 = r face, 1 = phi.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void phys_flux(const double *p, double r, double n0, double n1, double n2,
-                                          double gam, double *F) {
-  double rho = p[D_RHO];
-  double Pp = p[D_PPP];
-  double vr = p[D_URR];
-  double vp = p[D_UPP] * r;
-  double vz = p[D_UZZ];
-  double vn = vr * n0 + vp * n1 + vz * n2;
-  double rhoe = Pp / (gam - 1.);
-  double v2 = vr * vr + vp * vp + vz * vz;
-  F[D_DDD] = rho * vn;
-  F[D_SRR] = rho * vr * vn + Pp * n0;
-  F[D_LLL] = r * (rho * vp * vn + Pp * n1);
-  F[D_SZZ] = rho * vz * vn + Pp * n2;
-  F[D_TAU] = (.5 * rho * v2 + rhoe + Pp) * vn;
-}
-// cell_prim2cons with dV = 1 (src/Cell/cell_conversion.c:11-33)
-__device__ __forceinline__ void prim2cons(const double *p, double *U, double r, double dV, double gam) {
-  double rho = p[D_RHO];
-  double Pp = p[D_PPP];
-  double vr = p[D_URR];
-  double vp = p[D_UPP] * r;
-  double vz = p[D_UZZ];
-  double v2 = vr * vr + vp * vp + vz * vz;
-  double rhoe = Pp / (gam - 1.);
-  U[D_DDD] = rho * dV;
-  U[D_SRR] = rho * vr * dV;
-  U[D_LLL] = r * rho * vp * dV;
-  U[D_SZZ] = rho * vz * dV;
-  U[D_TAU] = (.5 * rho * v2 + rhoe) * dV;
-}
-
-__device__ __forceinline__ void riemann_flux(const double *pL, const double *pR, double r, int dir, double w, double gam,
-                             int solver, double *F) {
-  const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = 0.0;
-  double vnL, cf2L, vnR, cf2R;
-  {
-    double P = pL[D_PPP], rho = pL[D_RHO], vr = pL[D_URR], vp = r * pL[D_UPP], vz = pL[D_UZZ];
-    vnL = vr * n0 + vp * n1 + vz * n2;
-    cf2L = gam * (P / rho);
-  }
-  {
-    double P = pR[D_PPP], rho = pR[D_RHO], vr = pR[D_URR], vp = r * pR[D_UPP], vz = pR[D_UZZ];
-    vnR = vr * n0 + vp * n1 + vz * n2;
-    cf2R = gam * (P / rho);
-  }
-  double Sl = vnL - sqrt(cf2L);
-  double Sr = vnL + sqrt(cf2L);
-  if (Sl > vnR - sqrt(cf2R)) Sl = vnR - sqrt(cf2R);
-  if (Sr < vnR + sqrt(cf2R)) Sr = vnR + sqrt(cf2R);
-  double Ss = (pR[D_RHO] * vnR * (Sr - vnR) - pL[D_RHO] * vnL * (Sl - vnL) + pL[D_PPP] - pR[D_PPP]) /
-              (pR[D_RHO] * (Sr - vnR) - pL[D_RHO] * (Sl - vnL));
-  int state;
-  if (w < Sl) state = DS_LEFT;
-  else if (w > Sr) state = DS_RIGHT;
-  else if (w < Ss) state = DS_LEFTSTAR;
-  else state = DS_RIGHTSTAR;
-
-  double Fk[5], Uk[5];
-  if (state == DS_LEFT || state == DS_RIGHT) {
-    const double *p = state == DS_LEFT ? pL : pR;
-    phys_flux(p, r, n0, n1, n2, gam, Fk);
-    prim2cons(p, Uk, r, 1.0, gam);
-#pragma unroll
-    for (int q = 0; q < 5; ++q) F[q] = Fk[q] - w * Uk[q];
-    return;
-  }
-  double Ustar[5], Fstar[5];
-  if (solver == DR_HLL) {
-    double FL[5], FR[5], UL[5], UR[5];
-    phys_flux(pL, r, n0, n1, n2, gam, FL);
-    phys_flux(pR, r, n0, n1, n2, gam, FR);
-    prim2cons(pL, UL, r, 1.0, gam);
-    prim2cons(pR, UR, r, 1.0, gam);
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      Ustar[q] = (Sr * UR[q] - Sl * UL[q] + FL[q] - FR[q]) / (Sr - Sl);
-      Fstar[q] = (Sr * FL[q] - Sl * FR[q] - Sr * Sl * (UL[q] - UR[q])) / (Sr - Sl);
-    }
-  } else {
-    const double *prim = state == DS_LEFTSTAR ? pL : pR;
-    double Sk = state == DS_LEFTSTAR ? Sl : Sr;
-    phys_flux(prim, r, n0, n1, n2, gam, Fk);
-    prim2cons(prim, Uk, r, 1.0, gam);
-    double rho = prim[D_RHO];
-    double vr = prim[D_URR];
-    double vp = prim[D_UPP] * r;
-    double vz = prim[D_UZZ];
-    double Pp = prim[D_PPP];
-    double v2 = vr * vr + vp * vp + vz * vz;
-    double vn = vr * n0 + vp * n1 + vz * n2;
-    double rhoe = Pp / (gam - 1.);
-    double D = rho;
-    double mr = rho * vr;
-    double mp = rho * vp;
-    double mz = rho * vz;
-    double E_hydro = .5 * rho * v2 + rhoe;
-    double Ps = rho * (Sk - vn) * (Ss - vn) + Pp;
-    double Dstar = (Sk - vn) * D / (Sk - Ss);
-    double Msn = Dstar * Ss;
-    double Msr = (Sk - vn) * mr / (Sk - Ss);
-    double Msp = (Sk - vn) * mp / (Sk - Ss);
-    double Msz = (Sk - vn) * mz / (Sk - Ss);
-    double Estar = ((Sk - vn) * E_hydro + Ps * Ss - Pp * vn) / (Sk - Ss);
-    double mn = Msr * n0 + Msp * n1 + Msz * n2;
-    Msr += n0 * (Msn - mn);
-    Msp += n1 * (Msn - mn);
-    Msz += n2 * (Msn - mn);
-    Ustar[D_DDD] = Dstar;
-    Ustar[D_SRR] = Msr;
-    Ustar[D_LLL] = r * Msp;
-    Ustar[D_SZZ] = Msz;
-    Ustar[D_TAU] = Estar;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) Fstar[q] = Fk[q] + Sk * (Ustar[q] - Uk[q]);
-  }
-#pragma unroll
-  for (int q = 0; q < 5; ++q) F[q] = Fstar[q] - w * Ustar[q];
-}
-
-// Inputs of riemann_visc_flux (src/Riemann/Riemann_routines.c:193-311).
-struct ViscIn {
-  const double *pL, *pR;        // reconstructed face states (primL, primR)
-  double cL[5], cR[5];          // cell prims
-  double gpL[5], gpR[5];        // cell gradp
-  double grL[5], grR[5];        // cell grad
-  double tL, tR;                // cell tiph (wrapped)
-  double dpL, dpR;              // r faces: wrapped offsets of the face centre (k_rslope)
-  double r, cm, r_cell_L, r_cell_R;
-  double rdr_om;                // sim_rdrOm_a at r
-};
-
-__device__ __forceinline__ void visc_flux(const ViscIn &v, int dir, const DiskParams &P, const InstState &S,
-                          const double *gx, const double *gy, double *Fv, int *err) {
-  const double r = v.r;
-  double Avg[5], Gr[5], Gp[5];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    Avg[q] = .5 * (v.pL[q] + v.pR[q]);
-    Gp[q] = .5 * (v.gpL[q] + v.gpR[q]) / r;
-    Gr[q] = .5 * (v.grL[q] + v.grR[q]);
-  }
-  if (dir == 0) {
-    const double dpL = v.dpL, dpR = v.dpR;
-    double deltaL = v.r - v.r_cell_L;
-    double deltaR = v.r_cell_R - v.r;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      double WL = v.cL[q] + dpL * v.gpL[q];
-      double WR = v.cR[q] - dpR * v.gpR[q];
-      Avg[q] = 0.5 * (WL + WR);
-      Gr[q] = (WR - WL) / (deltaR + deltaL);
-    }
-  } else {
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      Avg[q] = 0.5 * (v.cR[q] + v.cL[q]);
-      Gp[q] = (v.cR[q] - v.cL[q]) / (v.tR - v.tL) / r;
-    }
-  }
-  double nu;
-  double alpha = P.visc;
-  if (P.visc_const == 1) {
-    nu = alpha;
-  } else if (P.init_type == DI_SHEAR) {
-    nu = alpha * P.gamma * Avg[D_PPP] / Avg[D_RHO] * dpow(fabs(r * cos(v.cm)), 2.0);
-    if (r * cos(v.cm) > 20.) nu = 0.0;
-  } else {
-    double sc, cc;
-    sincos(v.cm, &sc, &cc);
-    const double x = r * cc, y = r * sc;
-    double d0 = gm_dist_xy(x, y, gx[0], gy[0]);
-    double d1 = gm_dist_xy(x, y, gx[1], gy[1]);
-    double eps = P.g_eps;
-    nu = alpha * Avg[D_PPP] / Avg[D_RHO] /
-         sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.gM[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.gM[1]);
-  }
-  double rho = Avg[D_RHO];
-  double vr = Avg[D_URR];
-  double om = Avg[D_UPP];
-  double vz = Avg[D_UZZ];
-  if (fabs(vz) > 1.e-12) set_err(err, DGPU_EF_VISC_VZ);
-  double Gr_vr = Gr[D_URR], Gr_om = Gr[D_UPP];
-  double Gp_vr = Gp[D_URR], Gp_om = Gp[D_UPP];
-  double rdr = v.rdr_om;
-  if (dir == 0) {
-    Fv[0] = -nu * rho * (r * Gr_vr - vr - r * r * Gp_om);
-    Fv[1] = -nu * rho * (r * (r * Gr_om + rdr) + r * Gp_vr);
-    Fv[2] = -nu * rho * (vr * (Gr_vr - vr / r - r * Gp_om) + r * om * (Gp_vr + (rdr + r * Gr_om)));
-  } else {
-    Fv[0] = -nu * rho * (r * (r * Gr_om + rdr) + r * Gp_vr);
-    Fv[1] = -nu * rho * (-r * Gr_vr + vr + r * r * Gp_om);
-    Fv[2] = -nu * rho * (-r * om * (Gr_vr - vr / r - r * Gp_om) + vr * (Gp_vr + (rdr + r * Gr_om)));
-  }
-}
-
-__device__ __forceinline__ double ld(const double *p, int q, int n, int g) { return p[(size_t)q * n + g]; }
 
 // ---------------------------------------------------------------------------
 // r-face list of one annulus pair (build_jloop, face_create_destroy.c:22-128)
@@ -446,7 +150,8 @@ __device__ T block_excl_scan(T v, T *sh, T &total) {
 // cell_plm_p (src/Cell/cell_plm.c:116-161) and, for the first cell of each disk,
 // gravMass_copy at the start of a step (GravMass_misc.c:20-28) and
 // gravMass_clean_pi (GravMass_misc.c:9-17).  Runs concurrently with k_merge.
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, int substep) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   if (g >= N) return;
@@ -464,15 +169,9 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, int
     const double dpR = .5 * (dc + d.dphi[gr]);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      double pc = ld(d.prim, q, N, g), pl = ld(d.prim, q, N, gl), pr = ld(d.prim, q, N, gr);
-      double sL = (pc - pl) / dpL;
-      double sR = (pr - pc) / dpR;
-      double sM = (pr - pl) / (dpL + dpR);
-      double sv = P.plm * sL;
-      if (fabs(sv) > P.plm * fabs(sR)) sv = P.plm * sR;
-      if (fabs(sv) > fabs(sM)) sv = sM;
-      if (sL * sR < 0.0) sv = 0.0;
-      d.gradp[(size_t)q * N + g] = sv;
+      T pc = ldq<T>(d.prim, tp.prim, q, N, g), pl = ldq<T>(d.prim, tp.prim, q, N, gl),
+        pr = ldq<T>(d.prim, tp.prim, q, N, gr);
+      stq<T>(d.gradp, tp.gradp, q, N, g, plm_p_slope(pl, pc, pr, dpL, dpR, P.plm));
     }
   }
   if (g == P.cell_base) {
@@ -694,73 +393,12 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
 // ---------------------------------------------------------------------------
 // cell_plm_rz (src/Cell/cell_plm.c:13-114) per cell + CFL (cell_mindt.c:32-100)
 // ---------------------------------------------------------------------------
-struct RFace {
-  int cL, cR;
-  double dphi, cm;
-  double r, dl, dr, dperp;
-};
-
-// Calls f(face) for every r face of cell g in the reference's face order:
-// first the faces of pair (i-1, i) where g is the outer cell, then the faces
-// of pair (i, i+1) where g is the inner cell.
-template <typename Fn>
-__device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus &A, int a, int g, int NR,
-                                                Fn f) {
-  const int j = g - A.cell_off;
-  if (A.i > 0) {
-    const Annulus &Q = d.ann[a - 1];
-    const int4 rr = reinterpret_cast<const int4 *>(d.rr)[g];
-    auto one = [&](int n) {
-      RFace F;
-      F.cL = d.fL[Q.face_base + n];
-      F.cR = g;
-      F.dphi = d.fdphi[Q.face_base + n];
-      F.cm = d.fcm[Q.face_base + n];
-      F.r = Q.f_r;
-      F.dl = Q.f_dl;
-      F.dr = Q.f_dr;
-      F.dperp = Q.f_dperp;
-      f(F, Q.face_base + n, 1);
-    };
-    if (rr.z != INT_MIN) {
-      for (int n = rr.x; n < rr.y; ++n) one(n);
-      for (int n = rr.z; n < rr.w; ++n) one(n);
-    } else {
-      // three or more runs (the outer pointer went round more than twice)
-      const int T = d.pair_T[a - 1];
-      const int jpmin = d.pair_jpmin[a - 1];
-      int dd = j - jpmin;
-      if (dd < 0) dd += A.np;
-      const int *runs = d.runs + Q.run_base;
-      for (int s = dd; s <= T; s += A.np)
-        for (int n = runs[s]; n < runs[s + 1]; ++n) one(n);
-    }
-  }
-  if (A.i < NR - 1) {
-    const int nf = d.pair_nf[a];
-    int n0 = d.fstart[g];
-    int n1 = (j + 1 < A.np) ? d.fstart[g + 1] : nf;
-    if (nf <= 0) n1 = n0;
-    for (int n = n0; n < n1; ++n) {
-      RFace F;
-      F.cL = g;
-      F.cR = d.fR[A.face_base + n];
-      F.dphi = d.fdphi[A.face_base + n];
-      F.cm = d.fcm[A.face_base + n];
-      F.r = A.f_r;
-      F.dl = A.f_dl;
-      F.dr = A.f_dr;
-      F.dperp = A.f_dperp;
-      f(F, A.face_base + n, 0);
-    }
-  }
-}
-
 // r-face slope and reconstruction offsets, once per face: the S of
 // cell_plm_rz (src/Cell/cell_plm.c:31-53) and the wrapped dpL, dpR that
 // cell_plm_rz, riemann_setup_rz (Riemann_setup.c:18-25) and riemann_visc_flux
 // (Riemann_routines.c:220-228) all form the same way.
-__global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d) {
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= d.n_slots) return;
   const int cL = d.fL[slot];
@@ -781,13 +419,14 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d) {
   const double den = A.f_dr + A.f_dl;
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    double WL = ld(d.prim, q, N, cL) + dpL * ld(d.gradp, q, N, cL);
-    double WR = ld(d.prim, q, N, cR) - dpR * ld(d.gradp, q, N, cR);
-    d.fS[(size_t)q * NS + slot] = (WR - WL) / den;
+    T WL = ldq<T>(d.prim, tp.prim, q, N, cL) + dpL * ldq<T>(d.gradp, tp.gradp, q, N, cL);
+    T WR = ldq<T>(d.prim, tp.prim, q, N, cR) - dpR * ldq<T>(d.gradp, tp.gradp, q, N, cR);
+    stq<T>(d.fS, tp.fS, q, NS, slot, (WR - WL) / den);
   }
 }
 
-__global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int substep) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells, NS = d.n_slots;
   unsigned long long key = ~0ull;
@@ -807,11 +446,11 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int sub
     const Annulus A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
     inst = A.inst;
-    double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    T gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
       double dA = F.r * F.dphi * F.dperp;
 #pragma unroll
-      for (int q = 0; q < 5; ++q) gq[q] += d.fS[(size_t)q * NS + slot] * dA;
+      for (int q = 0; q < 5; ++q) gq[q] += ldq<T>(d.fS, tp.fS, q, NS, slot) * dA;
     });
     {
       double dz = P.dz, dp = d.dphi[g], dAtot;
@@ -824,13 +463,13 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int sub
     for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        double Sq = d.fS[(size_t)q * NS + slot];
+        T Sq = ldq<T>(d.fS, tp.fS, q, NS, slot);
         if (Sq * gq[q] < 0.0) gq[q] = 0.0;
         else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
       }
     });
 #pragma unroll
-    for (int q = 0; q < 5; ++q) d.grad[(size_t)q * N + g] = gq[q];
+    for (int q = 0; q < 5; ++q) stq<T>(d.grad, tp.grad, q, N, g, gq[q]);
 
     // CFL candidate (cell_mindt), substep 1 only, non-ghost annuli
     if (substep == 1 && (A.kind & DGPU_AK_CFL)) {
@@ -915,13 +554,39 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, int sub
 // ---------------------------------------------------------------------------
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
+// GravMass positions and masses of the substep and alpha as T: the tangent
+// seeds of TanPtrs give d/de of M_p and of the orbit radius r_p (the positions
+// are r_p (cos, sin) of the orbit phase, which has no tangent).
+template <typename T>
+__device__ __forceinline__ void grav_t(GravT<T> &G, const InstState &S, const DiskParams &P, const TanPtrs &tp,
+                                       int inst) {
+  if constexpr (std::is_same<T, Dual>::value) {
+    const double *sd = tp.seed + (size_t)DGPU_TP_N * inst;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      G.gM[p] = Dual(S.gM[p], sd[DGPU_TP_DM0 + p]);
+      G.gx[p] = Dual(S.gx[p], sd[DGPU_TP_DR0 + p] * S.gc[p]);
+      G.gy[p] = Dual(S.gy[p], sd[DGPU_TP_DR0 + p] * S.gs[p]);
+    }
+    G.alpha = Dual(P.visc, sd[DGPU_TP_DALPHA]);
+  } else {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      G.gM[p] = S.gM[p];
+      G.gx[p] = S.gx[p];
+      G.gy[p] = S.gy[p];
+    }
+    G.alpha = P.visc;
+  }
+}
+
 // phi faces: thread per cell j, face (j, j+1) (riemann_setup_p, Riemann_setup.c:46-80)
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, int substep) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
   if (t >= N) return;
-    // phi face (j, j+1): riemann_setup_p (Riemann_setup.c:46-80)
   const int g = t;
   const int a = d.cell_ann[g];
   const Annulus A = d.ann[a];
@@ -934,32 +599,27 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, int
   const double dr = A.rp - A.rm;
   const double r = .5 * (A.rp + A.rm);
   const double dA = dr * dz;
-  double pL[5], pR[5];
+  T pL[5], pR[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    pL[q] = ld(d.prim, q, N, cL) + 0.5 * ld(d.gradp, q, N, cL) * dpL;
-    pR[q] = ld(d.prim, q, N, cR) - 0.5 * ld(d.gradp, q, N, cR) * dpR;
+    pL[q] = ldq<T>(d.prim, tp.prim, q, N, cL) + 0.5 * ldq<T>(d.gradp, tp.gradp, q, N, cL) * dpL;
+    pR[q] = ldq<T>(d.prim, tp.prim, q, N, cR) - 0.5 * ldq<T>(d.gradp, tp.gradp, q, N, cR) * dpR;
   }
   const double w = d.w_ann[a];
-  double F[5];
+  T F[5];
   riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F);
   const double dt = fac * S.dt;
   const double k = dt * dA;
-  double *out = d.fphi;
 #pragma unroll
-  for (int q = 0; q < 5; ++q) out[(size_t)q * N + g] = k * F[q];
+  for (int q = 0; q < 5; ++q) stq<T>(d.fphi, tp.fphi, q, N, g, k * F[q]);
   if (P.has_visc) {
-    ViscIn v;
-    v.pL = pL;
-    v.pR = pR;
+    ViscIn<T> v;
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      v.cL[q] = ld(d.prim, q, N, cL);
-      v.cR[q] = ld(d.prim, q, N, cR);
-      v.gpL[q] = ld(d.gradp, q, N, cL);
-      v.gpR[q] = ld(d.gradp, q, N, cR);
-      v.grL[q] = ld(d.grad, q, N, cL);
-      v.grR[q] = ld(d.grad, q, N, cR);
+      v.cL[q] = ldq<T>(d.prim, tp.prim, q, N, cL);
+      v.cR[q] = ldq<T>(d.prim, tp.prim, q, N, cR);
+      v.grL[q] = ldq<T>(d.grad, tp.grad, q, N, cL);
+      v.grR[q] = ldq<T>(d.grad, tp.grad, q, N, cR);
     }
     v.tL = d.tiphw[cL];
     v.tR = d.tiphw[cR];
@@ -970,15 +630,18 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, int
     v.r_cell_R = r;
     double a_sep = S.gr[0] + S.gr[1];
     v.rdr_om = frame_rdrom(P, A.rdrom, r, a_sep);
-    double Fv[3];
-    visc_flux(v, 1, P, S, S.gx, S.gy, Fv, d.err);
+    GravT<T> G;
+    grav_t(G, S, P, tp, A.inst);
+    T Fv[3];
+    visc_flux(v, 1, P, G, Fv, d.err);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * N + g] = k * Fv[q];
+    for (int q = 0; q < 3; ++q) stq<T>(d.fphi, tp.fphi, 5 + q, N, g, k * Fv[q]);
   }
 }
 
 // r faces: thread per face slot (riemann_setup_rz, Riemann_setup.c:11-44)
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, int substep) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
@@ -999,32 +662,29 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, int s
   const double dA = r * fdphi * A.f_dperp;
   const double r_cell_L = r - deltaL;
   const double r_cell_R = r + deltaR;
-  double pL[5], pR[5];
+  T pL[5], pR[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    pL[q] = ld(d.prim, q, N, cL) + ld(d.grad, q, N, cL) * deltaL + ld(d.gradp, q, N, cL) * dpL;
-    pR[q] = ld(d.prim, q, N, cR) - ld(d.grad, q, N, cR) * deltaR - ld(d.gradp, q, N, cR) * dpR;
+    pL[q] = ldq<T>(d.prim, tp.prim, q, N, cL) + ldq<T>(d.grad, tp.grad, q, N, cL) * deltaL +
+            ldq<T>(d.gradp, tp.gradp, q, N, cL) * dpL;
+    pR[q] = ldq<T>(d.prim, tp.prim, q, N, cR) - ldq<T>(d.grad, tp.grad, q, N, cR) * deltaR -
+            ldq<T>(d.gradp, tp.gradp, q, N, cR) * dpR;
   }
-  double F[5];
+  T F[5];
   riemann_flux(pL, pR, r, 0, 0.0, P.gamma, P.riemann, F);
   const double dt = fac * S.dt;
   const double k = dt * dA;
   const int NS = d.n_slots;
-  double *out = d.frf;
 #pragma unroll
-  for (int q = 0; q < 5; ++q) out[(size_t)q * NS + slot] = k * F[q];
+  for (int q = 0; q < 5; ++q) stq<T>(d.frf, tp.frf, q, NS, slot, k * F[q]);
   if (P.has_visc) {
-    ViscIn v;
-    v.pL = pL;
-    v.pR = pR;
+    ViscIn<T> v;
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      v.cL[q] = ld(d.prim, q, N, cL);
-      v.cR[q] = ld(d.prim, q, N, cR);
-      v.gpL[q] = ld(d.gradp, q, N, cL);
-      v.gpR[q] = ld(d.gradp, q, N, cR);
-      v.grL[q] = ld(d.grad, q, N, cL);
-      v.grR[q] = ld(d.grad, q, N, cR);
+      v.cL[q] = ldq<T>(d.prim, tp.prim, q, N, cL);
+      v.cR[q] = ldq<T>(d.prim, tp.prim, q, N, cR);
+      v.gpL[q] = ldq<T>(d.gradp, tp.gradp, q, N, cL);
+      v.gpR[q] = ldq<T>(d.gradp, tp.gradp, q, N, cR);
     }
     v.tL = d.tiphw[cL];
     v.tR = d.tiphw[cR];
@@ -1036,20 +696,18 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, int s
     v.r_cell_R = r_cell_R;
     double a_sep = S.gr[0] + S.gr[1];
     v.rdr_om = frame_rdrom(P, A.f_rdrom, r, a_sep);
-    double Fv[3];
-    visc_flux(v, 0, P, S, S.gx, S.gy, Fv, d.err);
+    GravT<T> G;
+    grav_t(G, S, P, tp, A.inst);
+    T Fv[3];
+    visc_flux(v, 0, P, G, Fv, d.err);
 #pragma unroll
-    for (int q = 0; q < 3; ++q) out[(size_t)(5 + q) * NS + slot] = k * Fv[q];
+    for (int q = 0; q < 3; ++q) stq<T>(d.frf, tp.frf, 5 + q, NS, slot, k * Fv[q]);
   }
 }
 
 // ---------------------------------------------------------------------------
 // Per-cell update: flux gather + sources + mesh motion + prim/cons + BC + damping
 // ---------------------------------------------------------------------------
-// fgrav (src/Cell/cell_source.c:11-13)
-__device__ __forceinline__ double fgrav(double M, double r, double eps, int n) {
-  return (M * dpow(r, n - 1.) / dpow(dpow(r, n) + dpow(eps, n), 1. + 1. / n));
-}
 
 // Advanced phi edge of a cell (cell_update_phi, src/Cell/cell_misc.c:59-79).
 __device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, double w_total, double dt, double r,
@@ -1068,7 +726,8 @@ __device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, dou
 // so this kernel runs concurrently with k_flux.  Its first n_ann threads also
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, int substep) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, TanPtrs tp, int substep) {
   __shared__ double sh_md[2][BLK / 32];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -1112,64 +771,58 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, int
     const double dphi = d.dphi[g];
     const double rm = A.rm, rp = A.rp;
     double phi = d.tiphw[g] - .5 * dphi;
-    double rho = ld(d.prim, D_RHO, N, g);
-    double Pp = ld(d.prim, D_PPP, N, g);
     double r = .5 * (rp + rm);
-    double vr = ld(d.prim, D_URR, N, g);
-    double vz = ld(d.prim, D_UZZ, N, g);
-    double vp = ld(d.prim, D_UPP, N, g) * r;
-    double dz = P.dz;
-    double dV = dphi * .5 * A.dv_diff * dz;
-    double sinp, cosp;
-    sincos(phi, &sinp, &cosp);
-    double xpos = r * cosp;
-    double ypos = r * sinp;
-    double z = P.z;
-    double R = sqrt(r * r + z * z);
-    double sint, cost, gravdist;
-    if (P.grav2d == 1) {
-      sint = 1.0;
-      cost = 0.0;
-      gravdist = r;
-    } else {
-      sint = r / R;
-      cost = z / R;
-      gravdist = R;
-    }
-    double Fr = 0.0, Fp = 0.0;
-    for (int p = 0; p < 2; ++p) {
-      // gravMassForce (src/Cell/cell_source.c:49-71)
-      double dx = gravdist * cosp - S.gx[p];
-      double dy = gravdist * sinp - S.gy[p];
-      double script_r = sqrt(dx * dx + dy * dy);
-      double cosa = dx / script_r;
-      double sina = dy / script_r;
-      double cosap = cosa * cosp + sina * sinp;
-      double sinap = sina * cosp - cosa * sinp;
-      double f1 = -fgrav(S.gM[p], script_r, P.g_eps, P.phi_order);
-      Fr += cosap * f1;
-      Fp += sinap * f1;
+    T pm[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) pm[q] = ldq<T>(d.prim, tp.prim, q, N, g);
+    SrcGeom sg;
+    sg.r = r;
+    sg.dt = dt;
+    sg.dV = dphi * .5 * A.dv_diff * P.dz;
+    sincos(phi, &sg.sinp, &sg.cosp);
+    sg.xpos = r * sg.cosp;
+    sg.ypos = r * sg.sinp;
+    {
+      double z = P.z;
+      double R = sqrt(r * r + z * z);
+      if (P.grav2d == 1) {
+        sg.sint = 1.0;
+        sg.cost = 0.0;
+        sg.gravdist = r;
+      } else {
+        sg.sint = r / R;
+        sg.cost = z / R;
+        sg.gravdist = R;
+      }
     }
     double w_a = frame_rom(P, A.rom, r, a_sep);
-    double rdrOm_a = frame_rdrom(P, A.rdrom, r, a_sep);
-    double F_centrifugal_r = w_a * w_a / r;
-    double dtOm_a = frame_dtom(P, A.dtom, r, a_sep);
-    double F_euler_phi = -(r * dtOm_a + vr * rdrOm_a);
-    double *src = d.src;
-    src[g] = dt * dV * (rho * vp * vp + Pp) / r;
-    src[(size_t)N + g] = dt * dV * rho * (Fr * sint + F_centrifugal_r);
-    src[2 * (size_t)N + g] = dt * dV * rho * (Fp - r * dtOm_a) * r;
-    src[3 * (size_t)N + g] = dt * dV * rho * Fr * cost;
-    src[4 * (size_t)N + g] =
-        dt * dV * rho * ((Fr * sint + F_centrifugal_r) * vr + Fr * vz * cost + (Fp + F_euler_phi) * vp);
+    sg.rdrOm = frame_rdrom(P, A.rdrom, r, a_sep);
+    sg.Fc = w_a * w_a / r;
+    sg.dtOm = frame_dtom(P, A.dtom, r, a_sep);
+    GravT<T> G;
+    grav_t(G, S, P, tp, A.inst);
+    T gu = 0.0, gpu = 0.0;
+    if (P.has_visc) {
+      gu = ldq<T>(d.grad, tp.grad, D_UPP, N, g);
+      gpu = ldq<T>(d.gradp, tp.gradp, D_URR, N, g);
+    }
+    T sv[6];
+    source_cell(sg, P, pm, gu, gpu, G, sv);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) stq<T>(d.src, tp.src, q, N, g, sv[q]);
+    if (P.has_visc) stq<T>(d.src, tp.src, 5, N, g, sv[5]);
+    const double xpos = sg.xpos, ypos = sg.ypos, dV = sg.dV;
+    const T rho = pm[D_RHO], Pp = pm[D_PPP];
     if (P.rho_sink_on == 1) {
-      // get_rho_sink (src/Cell/cell_source.c:15-47)
+      // get_rho_sink (src/Cell/cell_source.c:15-47); no tangent (refused by the
+      // differentiated runs)
+      const double rhov = val(rho), Pv = val(Pp);
       double r0 = sqrt((xpos - S.gx[0]) * (xpos - S.gx[0]) + (ypos - S.gy[0]) * (ypos - S.gy[0]));
       double r1 = sqrt((xpos - S.gx[1]) * (xpos - S.gx[1]) + (ypos - S.gy[1]) * (ypos - S.gy[1]));
       double M0 = S.gM[0], M1 = S.gM[1];
       double Mtotal = M0 + M1;
       double alpha = P.visc;
-      double one_o_nu = 1.0 / (alpha * Pp / rho) * sqrt(pow(r0, -3) * M0 / Mtotal + pow(r1, -3) * M1 / Mtotal);
+      double one_o_nu = 1.0 / (alpha * Pv / rhov) * sqrt(pow(r0, -3) * M0 / Mtotal + pow(r1, -3) * M1 / Mtotal);
       double t_visc0 = 1.0 * 2. / 3. * r0 * r0 * one_o_nu;
       double t_visc1 = 1.0 * 2. / 3. * r1 * r1 * one_o_nu;
       if (t_visc0 < 10. * dt) t_visc0 = 10. * dt;
@@ -1177,30 +830,14 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, int
       double sink_size = 0.5;
       for (int p = 0; p < P.num_sinks && p < 2; ++p) {
         double drho = 0.0;
-        if (p == 0) { if (r0 < sink_size) drho = rho / t_visc0; }
-        else { if (r1 < sink_size) drho = rho / t_visc1; }
-        src[(6 + (size_t)p) * N + g] = drho * dt * dV;
+        if (p == 0) { if (r0 < sink_size) drho = rhov / t_visc0; }
+        else { if (r1 < sink_size) drho = rhov / t_visc1; }
+        stq<T>(d.src, tp.src, 6 + p, N, g, T(drho * dt * dV));
         if (A.kind & DGPU_AK_SINK_SUM) {
           if (p == 0) md0 += drho * dV;
           else md1 += drho * dV;
         }
       }
-    }
-    if (P.has_visc) {
-      double dist_bh0 = sqrt((xpos - S.gx[0]) * (xpos - S.gx[0]) + (ypos - S.gy[0]) * (ypos - S.gy[0]));
-      double dist_bh1 = sqrt((xpos - S.gx[1]) * (xpos - S.gx[1]) + (ypos - S.gy[1]) * (ypos - S.gy[1]));
-      double alpha = P.visc;
-      double eps = P.g_eps;
-      double Sigma_nu;
-      if (P.visc_const == 1) {
-        Sigma_nu = rho * alpha;
-      } else {
-        Sigma_nu = alpha * Pp /
-                   sqrt(dpow(dist_bh0 * dist_bh0 + eps * eps, -1.5) * S.gM[0] +
-                        dpow(dist_bh1 * dist_bh1 + eps * eps, -1.5) * S.gM[1]);
-      }
-      src[5 * (size_t)N + g] =
-          dt * dV * Sigma_nu * rdrOm_a * (rdrOm_a + r * ld(d.grad, D_UPP, N, g) + ld(d.gradp, D_URR, N, g));
     }
   }
   // deterministic per-block Mdot partial sums (reduced in block order by k_update)
@@ -1226,7 +863,9 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, int
   }
 }
 
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int substep, int stop, int tail) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
+                                                                  int tail) {
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -1240,17 +879,17 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
     const int j = g - A.cell_off;
     const int np = A.np;
     const double dt = fac * S.dt;
-    double c[5];
+    T c[5];
     // cell_copy (substep 1) + cell_adjust_RK_cons (cell_misc.c:28-57)
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      double cq = ld(d.cons, q, N, g);
-      double rk;
+      T cq = ldq<T>(d.cons, tp.cons, q, N, g);
+      T rk;
       if (substep == 1) {
         rk = cq;
-        d.rkcons[(size_t)q * N + g] = cq;
+        stq<T>(d.rkcons, tp.rkcons, q, N, g, cq);
       } else {
-        rk = ld(d.rkcons, q, N, g);
+        rk = ldq<T>(d.rkcons, tp.rkcons, q, N, g);
       }
       c[q] = (1.0 - RK) * cq + RK * rk;
     }
@@ -1261,20 +900,20 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
       const double r = .5 * (A.rp + A.rm);
       auto addL = [&](int f) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] -= ld(d.fphi, q, N, f);
+        for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.fphi, tp.fphi, q, N, f);
         if (P.has_visc) {
-          c[D_SRR] -= ld(d.fphi, 5, N, f) / r;
-          c[D_LLL] -= ld(d.fphi, 6, N, f);
-          c[D_TAU] -= ld(d.fphi, 7, N, f);
+          c[D_SRR] -= ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
+          c[D_LLL] -= ldq<T>(d.fphi, tp.fphi, 6, N, f);
+          c[D_TAU] -= ldq<T>(d.fphi, tp.fphi, 7, N, f);
         }
       };
       auto addR = [&](int f) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] += ld(d.fphi, q, N, f);
+        for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.fphi, tp.fphi, q, N, f);
         if (P.has_visc) {
-          c[D_SRR] += ld(d.fphi, 5, N, f) / r;
-          c[D_LLL] += ld(d.fphi, 6, N, f);
-          c[D_TAU] += ld(d.fphi, 7, N, f);
+          c[D_SRR] += ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
+          c[D_LLL] += ldq<T>(d.fphi, tp.fphi, 6, N, f);
+          c[D_TAU] += ldq<T>(d.fphi, tp.fphi, 7, N, f);
         }
       };
       if (j == 0) {
@@ -1292,21 +931,21 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
       for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int asR) {
         if (asR) {
 #pragma unroll
-          for (int q = 0; q < 5; ++q) c[q] += ld(d.frf, q, NS, slot);
+          for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.frf, tp.frf, q, NS, slot);
           if (P.has_visc) {
             double rR = F.r + F.dr;
-            c[D_SRR] += ld(d.frf, 5, NS, slot) / rR;
-            c[D_LLL] += ld(d.frf, 6, NS, slot);
-            c[D_TAU] += ld(d.frf, 7, NS, slot);
+            c[D_SRR] += ldq<T>(d.frf, tp.frf, 5, NS, slot) / rR;
+            c[D_LLL] += ldq<T>(d.frf, tp.frf, 6, NS, slot);
+            c[D_TAU] += ldq<T>(d.frf, tp.frf, 7, NS, slot);
           }
         } else {
 #pragma unroll
-          for (int q = 0; q < 5; ++q) c[q] -= ld(d.frf, q, NS, slot);
+          for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.frf, tp.frf, q, NS, slot);
           if (P.has_visc) {
             double rL = F.r - F.dl;
-            c[D_SRR] -= ld(d.frf, 5, NS, slot) / rL;
-            c[D_LLL] -= ld(d.frf, 6, NS, slot);
-            c[D_TAU] -= ld(d.frf, 7, NS, slot);
+            c[D_SRR] -= ldq<T>(d.frf, tp.frf, 5, NS, slot) / rL;
+            c[D_LLL] -= ldq<T>(d.frf, tp.frf, 6, NS, slot);
+            c[D_TAU] -= ldq<T>(d.frf, tp.frf, 7, NS, slot);
           }
         }
       });
@@ -1319,34 +958,33 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
     if (!done) {
       // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
       // increments come from k_source; added here in the reference's order
-      const double *src = d.src;
-      c[D_SRR] += src[g];
-      c[D_SRR] += src[(size_t)N + g];
-      c[D_LLL] += src[2 * (size_t)N + g];
-      c[D_SZZ] += src[3 * (size_t)N + g];
-      c[D_TAU] += src[4 * (size_t)N + g];
+      c[D_SRR] += ldq<T>(d.src, tp.src, 0, N, g);
+      c[D_SRR] += ldq<T>(d.src, tp.src, 1, N, g);
+      c[D_LLL] += ldq<T>(d.src, tp.src, 2, N, g);
+      c[D_SZZ] += ldq<T>(d.src, tp.src, 3, N, g);
+      c[D_TAU] += ldq<T>(d.src, tp.src, 4, N, g);
       if (P.rho_sink_on == 1) {
-        for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= src[(6 + (size_t)p) * N + g];
+        for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldq<T>(d.src, tp.src, 6 + p, N, g);
       }
       const double r = .5 * (rp + rm);
       if (P.cooling == 1) {
         // cooling reads the running tau (cell_source.c:187-203)
-        const double rho = ld(d.prim, D_RHO, N, g), Pp = ld(d.prim, D_PPP, N, g);
+        const T rho = ldq<T>(d.prim, tp.prim, D_RHO, N, g), Pp = ldq<T>(d.prim, tp.prim, D_PPP, N, g);
         const double dV = dphi * .5 * A.dv_diff * P.dz;
         if (P.init_type == DI_SHEAR) {
-          double cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
+          T cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
           if (cooling_term < 0.0) cooling_term = 0.0;
           c[D_TAU] -= cooling_term * dt;
         } else {
           double numfac = 1.0;
           double alpha = P.visc;
-          double cooling_cap = c[D_TAU] * numfac;
-          double cooling_term = 9. / 4. * alpha * pow(P.poro_r1, -3) / rho * pow(Pp / rho, 4.) * dt * dV;
+          T cooling_cap = c[D_TAU] * numfac;
+          T cooling_term = 9. / 4. * alpha * pow(P.poro_r1, -3) / rho * pow(Pp / rho, 4.) * dt * dV;
           if (cooling_term > cooling_cap) cooling_term = cooling_cap;
           c[D_TAU] -= cooling_term;
         }
       }
-      if (P.has_visc) c[D_TAU] += src[5 * (size_t)N + g];
+      if (P.has_visc) c[D_TAU] += ldq<T>(d.src, tp.src, 5, N, g);
       // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
       {
         const double rom = frame_rom(P, A.rom, r, a_sep);
@@ -1354,21 +992,13 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
         const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
         const int NA = d.n_ann;
         const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
-        if (kappa > 0.) {
-          double l0 = c[D_LLL];
-          double rhov0 = c[D_SRR];
-          double ck = d.ann_c[NA + a], sk = d.ann_c[2 * NA + a];
-          double l = l0 * ck - c[D_SRR] * dr_r2Om / kappa * sk;
-          double rhov = rhov0 * ck + 2.0 * Omega * c[D_LLL] / r / kappa * sk;
-          c[D_LLL] = l;
-          c[D_SRR] = rhov;
-        }
+        if (kappa > 0.) split_rotate(c, d.ann_c[NA + a], d.ann_c[2 * NA + a], dr_r2Om, kappa, Omega, r);
       }
       done = stop == 4;
     }
     if (done) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+      for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
     } else {
       // cell_update_phi + cell_update_dphi (src/Cell/cell_misc.c:59-96)
       const double r = .5 * (rm + rp);
@@ -1388,34 +1018,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
       // cell_calc_prim -> cell_cons2prim (src/Cell/cell_conversion.c:57-122)
       const double dz = P.dz;
       const double dV = A.dv_half * dphi_n * dz;
-      double pr[5];
-      {
-        double rho = c[D_DDD] / dV;
-        if (rho < P.rho_floor) rho = P.rho_floor;
-        double Sr = c[D_SRR] / dV;
-        double Sp = c[D_LLL] / dV / r;
-        double Sz = c[D_SZZ] / dV;
-        double E = c[D_TAU] / dV;
-        double vr = Sr / rho;
-        double vp = Sp / rho;
-        double vz = Sz / rho;
-        double KE = .5 * (Sr * vr + Sp * vp + Sz * vz);
-        double v_magnitude = sqrt(2. * KE / rho);
-        double rhoe = E - KE;
-        double Pp = (P.gamma - 1.) * rhoe;
-        if (Pp < P.cs_floor * P.cs_floor * rho / P.gamma) Pp = P.cs_floor * P.cs_floor * rho / P.gamma;
-        if (Pp > P.cs_cap * P.cs_cap * rho / P.gamma) Pp = P.cs_cap * P.cs_cap * rho / P.gamma;
-        if (v_magnitude > P.vel_cap) {
-          vr = vr * P.vel_cap / v_magnitude;
-          vp = vp * P.vel_cap / v_magnitude;
-          vz = vz * P.vel_cap / v_magnitude;
-        }
-        pr[D_RHO] = rho;
-        pr[D_PPP] = Pp;
-        pr[D_URR] = vr;
-        pr[D_UPP] = vp / r;
-        pr[D_UZZ] = vz;
-      }
+      T pr[5];
+      cons2prim(c, dV, r, P, pr);
       if (stop >= 6) {
         // cell_boundary_fixed_r (src/Cell/cell_boundary.c:208-231)
         if ((A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC)) {
@@ -1424,10 +1028,10 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
         }
         // cell_bc_damp (src/Cell/cell_misc.c:98-132)
         if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
-          double f = d.ann_c[3 * d.n_ann + a];  // 1.-exp(-rate*dt), k_flux
+          double f = d.ann_c[3 * d.n_ann + a];  // 1.-exp(-rate*dt), k_source
 #pragma unroll
           for (int q = 0; q < 5; ++q) {
-            double dprim = A.ic[q] - pr[q];
+            T dprim = A.ic[q] - pr[q];
             pr[q] += f * dprim;
           }
         }
@@ -1438,8 +1042,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
       }
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        d.prim[(size_t)q * N + g] = pr[q];
-        d.cons[(size_t)q * N + g] = c[q];
+        stq<T>(d.prim, tp.prim, q, N, g, pr[q]);
+        stq<T>(d.cons, tp.cons, q, N, g, c[q]);
       }
     }
   }
@@ -1514,7 +1118,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, int
 }
 
 // cell_calc_cons over all cells (set-up and state upload)
-__global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d) {
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   if (g >= N) return;
@@ -1522,12 +1127,12 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d) {
   const DiskParams &P = d.par[A.inst];
   double r = .5 * (A.rp + A.rm);
   double dV = A.dv_half * d.dphi[g] * P.dz;
-  double p[5], c[5];
+  T p[5], c[5];
 #pragma unroll
-  for (int q = 0; q < 5; ++q) p[q] = ld(d.prim, q, N, g);
+  for (int q = 0; q < 5; ++q) p[q] = ldq<T>(d.prim, tp.prim, q, N, g);
   prim2cons(p, c, r, dV, P.gamma);
 #pragma unroll
-  for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+  for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
 }
 
 // Torque on the binary: -sum over non-ghost cells of r*rho*dV*F_phi, with the
@@ -1612,49 +1217,62 @@ int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa,
 
 int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
 
-int dgk_cellprep(const DevPtrs *d, int substep, void *stream) {
-  k_cellprep<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+// t == NULL: the forward kernels; otherwise their tangent instances.
+#define DGK_LAUNCH(kern, grid, smem, stream, ...)                                                  \
+  do {                                                                                            \
+    static const TanPtrs none_ = {};                                                              \
+    if (t) kern<Dual><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, *t, __VA_ARGS__);       \
+    else kern<double><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, none_, __VA_ARGS__);    \
+  } while (0)
+
+int dgk_cellprep(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
+  DGK_LAUNCH(k_cellprep, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_merge(const DevPtrs *d, int substep, void *stream) {
   k_merge<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
-int dgk_rslope(const DevPtrs *d, void *stream) {
+int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream) {
   if (d->n_slots <= 0) return 0;
-  k_rslope<<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
+  static const TanPtrs none = {};
+  if (t) k_rslope<Dual><<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, *t);
+  else k_rslope<double><<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   return (int)cudaGetLastError();
 }
-int dgk_plm_r(const DevPtrs *d, int substep, void *stream) {
-  k_plm_r<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+int dgk_plm_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
+  DGK_LAUNCH(k_plm_r, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
   return (int)cudaGetLastError();
 }
-int dgk_flux_phi(const DevPtrs *d, int substep, void *stream) {
-  k_flux_phi<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
+  DGK_LAUNCH(k_flux_phi, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
   return (int)cudaGetLastError();
 }
-int dgk_flux_r(const DevPtrs *d, int substep, void *stream) {
+int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   if (d->n_slots <= 0) return 0;
-  k_flux_r<<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  DGK_LAUNCH(k_flux_r, (d->n_slots + BLK - 1) / BLK, 0, stream, substep);
   return (int)cudaGetLastError();
 }
-int dgk_source(const DevPtrs *d, int substep, void *stream) {
+int dgk_source(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   int n = d->n_cells > d->n_ann ? d->n_cells : d->n_ann;
-  k_source<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  DGK_LAUNCH(k_source, (n + BLK - 1) / BLK, 0, stream, substep);
   return (int)cudaGetLastError();
 }
-int dgk_update(const DevPtrs *d, int substep, int stop, void *stream) {
+int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream) {
   int tail = stop >= 7 ? 2 : (stop >= 5 ? 1 : 0);
-  k_update<<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, substep, stop, tail);
+  DGK_LAUNCH(k_update, dgk_update_blocks(d->n_cells), 0, stream, substep, stop, tail);
   return (int)cudaGetLastError();
 }
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
   int tail = stop >= 5 ? 1 : 0;
-  k_update<<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, substep, stop, tail);
+  static const TanPtrs none = {};
+  k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop, tail);
   return (int)cudaGetLastError();
 }
-int dgk_calc_cons(const DevPtrs *d, void *stream) {
-  k_calc_cons<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
+int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream) {
+  static const TanPtrs none = {};
+  if (t) k_calc_cons<Dual><<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, *t);
+  else k_calc_cons<double><<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   return (int)cudaGetLastError();
 }
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream) {

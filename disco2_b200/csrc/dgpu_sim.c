@@ -489,6 +489,8 @@ void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a) {
   }
   a->kind = 0;
   if (i >= s->ng_min[0] && i < NR - s->ng_max[0]) a->kind |= DGPU_AK_CFL;
+  /* the accretion-rate objective is measured on the innermost non-ghost annulus */
+  if (i == s->ng_min[0]) a->kind |= DGPU_AK_MDOT;
   {
     int imin = (s->ng_min[0] == 1) ? 0 : s->ng_min[0];
     if (i >= imin && i < NR - s->ng_max[0]) a->kind |= DGPU_AK_SINK_SUM;
