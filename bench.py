@@ -270,6 +270,46 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
                    "back to back, same steps, L2 flushed before each step"}
 
 
+def run_adjoint(args):
+    """Cost of the gradient against the forward it differentiates: the
+    circumbinary disk at 192 annuli, 500 RK2 steps, both objectives averaged
+    over steps 251-500; forward = dgpu_objective (graph-replayed steps plus the
+    objective after each step), adjoint = dgpu_adjoint (forward sweep with a
+    checkpoint every 25 steps, then each segment replayed and reversed),
+    tangent = dgpu_tangent along q.  Wall time of the synchronous calls."""
+    from disco2_b200 import configs, lib
+    n, w0, K = args.adj_steps, args.adj_steps // 2, 25
+    s = lib.Sim(configs.circumbinary(num_r=192))
+    ctx = lib.Context(s, device=int(os.environ.get("LOCAL_RANK", "0")))
+    ctx.init_state(0)
+    ctx.objective(4, 2)          # graph capture, buffers
+    ctx.init_state(0)
+    ctx.adjoint(4, 2, ckpt_every=2)
+    ctx.init_state(0)
+    ctx.tangent(4, 2, dq=1.0)
+    res = {}
+    for name, fn in (("forward", lambda: ctx.objective(n, w0)),
+                     ("adjoint", lambda: ctx.adjoint(n, w0, ckpt_every=K)),
+                     ("tangent", lambda: ctx.tangent(n, w0, dq=1.0))):
+        best = None
+        for _ in range(2):
+            ctx.init_state(0)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            ctx.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        res[name] = best
+    ctx.close()
+    return {"workload": f"circumbinary disk, 192 annuli ({s.num_cells} cells), {n} steps, objectives "
+                        f"averaged over steps {w0 + 1}-{n}, checkpoints every {K} steps",
+            "forward_s": res["forward"], "adjoint_s": res["adjoint"], "tangent_s": res["tangent"],
+            "adjoint_over_forward": res["adjoint"] / res["forward"],
+            "tangent_over_forward": res["tangent"] / res["forward"],
+            "how": "wall time of the synchronous library calls, best of 2, same initial state"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -282,6 +322,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=500)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -411,6 +453,10 @@ def main():
     if not args.no_batched:
         batched = run_batched(args, rank, world, flush, barrier, max_over_ranks)
 
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = run_adjoint(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         res = cpu_baseline_run(configs.parfile_text(p), args.cpu_steps, 1)
@@ -446,6 +492,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
     if world > 1:

@@ -15,36 +15,11 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include "../../include/disco_gpu.h"
-#include "dgpu_internal.h"
-#include "dgpu_sim.h"
-
-struct dgpu_ctx {
-  int device;
-  cudaStream_t stream;
-  int own_stream;
-  cudaStream_t side;        /* second stream: concurrent branches inside the step graph */
-  cudaEvent_t fork[4];
-  int n_inst;
-  struct dgpu_sim **sims;
-  DiskParams *h_par;
-  Annulus *h_ann;
-  int n_ann, n_cells, n_slots, n_runs, n_upd_blocks;
-  DevPtrs d;          /* device pointers */
-  DiskParams *d_par;
-  InstState *d_ist;
-  Annulus *d_ann;
-  int *d_cell_ann, *d_slot_ann;
-  double *d_stage;    /* AoS staging buffer: max cells of a disk x NQ */
-  double *d_torque;   /* partial sums + result */
-  cudaGraphExec_t graph;
-  int have_graph;
-  char err[512];
-};
+#include "dgpu_ctx.h"
 
 static __thread char g_err[512];
 
-static int fail(struct dgpu_ctx *c, int code, const char *fmt, ...) {
+int dctx_fail(struct dgpu_ctx *c, int code, const char *fmt, ...) {
   va_list ap;
   char *dst = c ? c->err : g_err;
   va_start(ap, fmt);
@@ -52,21 +27,7 @@ static int fail(struct dgpu_ctx *c, int code, const char *fmt, ...) {
   va_end(ap);
   return code;
 }
-
-#define CK(call)                                                                          \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      return fail(c, DGPU_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),      \
-                  __FILE__, __LINE__);                                                    \
-  } while (0)
-#define CKK(call)                                                                         \
-  do {                                                                                    \
-    int e_ = (call);                                                                      \
-    if (e_ != 0)                                                                          \
-      return fail(c, DGPU_ERR_CUDA, "%s: %s (%s:%d)", #call,                              \
-                  cudaGetErrorString((cudaError_t)e_), __FILE__, __LINE__);               \
-  } while (0)
+#define fail dctx_fail
 
 /* ---------------- Sim ---------------- */
 
@@ -226,6 +187,7 @@ void dgpu_destroy(dgpu_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->have_graph) cudaGraphExecDestroy(c->graph);
+  dctx_diff_free(c);
   {
     void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
@@ -442,7 +404,7 @@ static int check_inst(struct dgpu_ctx *c, int inst) {
   return DGPU_OK;
 }
 
-static int read_err(struct dgpu_ctx *c) {
+int dctx_read_err(struct dgpu_ctx *c) {
   int e = 0;
   CK(cudaMemcpyAsync(&e, c->d.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -462,7 +424,7 @@ int dgpu_synchronize(dgpu_ctx *c) {
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
-  return read_err(c);
+  return dctx_read_err(c);
 }
 
 /* state upload of one disk: prim AoS [N][5], tiph, dphi (host) */
@@ -647,6 +609,18 @@ int dgpu_init_state(dgpu_ctx *c, int inst) {
   return rc;
 }
 
+int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int full) {
+  CKK(dgk_cellprep(&c->d, t, sub, c->stream));
+  CKK(dgk_merge(&c->d, sub, c->stream));
+  CKK(dgk_rslope(&c->d, t, c->stream));
+  CKK(dgk_plm_r(&c->d, t, sub, c->stream));
+  CKK(dgk_source(&c->d, t, sub, c->stream));
+  CKK(dgk_flux_phi(&c->d, t, sub, c->stream));
+  CKK(dgk_flux_r(&c->d, t, sub, c->stream));
+  if (full) CKK(dgk_update(&c->d, t, sub, 7, c->stream));
+  return DGPU_OK;
+}
+
 static int launch_step(struct dgpu_ctx *c) {
   int sub;
   for (sub = 1; sub <= 2; ++sub) {
@@ -732,7 +706,7 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
     }
   }
   for (k = 0; k <= DGPU_STEP_KERNELS; ++k) cudaEventDestroy(ev[k]);
-  return read_err(c);
+  return dctx_read_err(c);
 }
 
 int dgpu_stage(dgpu_ctx *c, int phase) {

@@ -159,6 +159,30 @@ typedef struct {
   const double *seed;                          /* [n_inst][DGPU_TP_N] */
 } TanPtrs;
 
+/* Reverse mode (one disk per context): adjoints of the state and of the
+ * substep intermediates, and per-block partial adjoints of the binary and of
+ * alpha.  Columns of part: DGPU_AP_* below. */
+#define DGPU_AP_M0 0
+#define DGPU_AP_M1 1
+#define DGPU_AP_R0 2
+#define DGPU_AP_R1 3
+#define DGPU_AP_ALPHA 4
+#define DGPU_AP_N 8
+typedef struct {
+  double *lW;          /* [5][n_cells] adjoint of prim */
+  double *lC;          /* [5][n_cells] adjoint of cons */
+  double *lCrk;        /* [5][n_cells] adjoint of rkcons (substep 2 -> substep 1) */
+  double *lU;          /* [5][n_cells] adjoint of the conserved sum before cons2prim */
+  double *lWt;         /* [5][n_cells] partial adjoint of prim within a substep */
+  double *lG, *lGp;    /* [5][n_cells] adjoints of grad and gradp */
+  double *aphiL, *aphiR; /* [15][n_cells] phi face (j, j+1): adjoints of (prim, gradp, grad) of cell j / j+1 */
+  double *arL, *arR;   /* [15][n_slots] r face: the same for its inner / outer cell */
+  double *fsL, *fsR;   /* [5][n_slots] adjoint of the face slope from the inner / outer cell's limiter */
+  double *part;        /* [rows][DGPU_AP_N] per-block partial adjoints */
+  double *acc;         /* [8]: dJ/dq, dJ/dalpha accumulated */
+  const double *dq;    /* [4]: dM_0/dq, dM_1/dq, dr_0/dq, dr_1/dq */
+} AdjPtrs;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -174,6 +198,12 @@ int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream);
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream);
+/* differentiation (dgpu_adjoint.cu) */
+int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, void *stream);
+int dgk_adj_rows(const DevPtrs *d);
+int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double wT, double wM, void *stream);
+int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream);
+int dgk_adj_calc_cons(const DevPtrs *d, const AdjPtrs *J, void *stream);
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
 int dgk_update_blocks(int n_cells);
 int dgk_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n, void *stream);

@@ -1,0 +1,217 @@
+// Device functions of the substep shared by the forward/tangent kernels
+// (dgpu_kernels.cu) and the adjoint kernels (dgpu_adjoint.cu).
+#ifndef DGPU_STEP_CUH
+#define DGPU_STEP_CUH
+
+#include <type_traits>
+
+#include "dgpu_device.cuh"
+
+namespace {
+
+// GravMass positions and masses of the substep and alpha as T: the tangent
+// seeds of TanPtrs give d/de of M_p and of the orbit radius r_p (the positions
+// are r_p (cos, sin) of the orbit phase, which has no tangent).
+template <typename T>
+__device__ __forceinline__ void grav_t(GravT<T> &G, const InstState &S, const DiskParams &P, const TanPtrs &tp,
+                                       int inst) {
+  if constexpr (std::is_same<T, Dual>::value) {
+    const double *sd = tp.seed + (size_t)DGPU_TP_N * inst;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      G.gM[p] = Dual(S.gM[p], sd[DGPU_TP_DM0 + p]);
+      G.gx[p] = Dual(S.gx[p], sd[DGPU_TP_DR0 + p] * S.gc[p]);
+      G.gy[p] = Dual(S.gy[p], sd[DGPU_TP_DR0 + p] * S.gs[p]);
+    }
+    G.alpha = Dual(P.visc, sd[DGPU_TP_DALPHA]);
+  } else {
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      G.gM[p] = S.gM[p];
+      G.gx[p] = S.gx[p];
+      G.gy[p] = S.gy[p];
+    }
+    G.alpha = P.visc;
+  }
+}
+
+// Advanced phi edge of a cell (cell_update_phi, src/Cell/cell_misc.c:59-79).
+__device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, double w_total, double dt, double r,
+                                           int *err) {
+  rk = adjust_toward(tw, rk, PHIMAX / 2., PHIMAX, err);
+  double t = (1.0 - RK) * tw + RK * rk;
+  t += w_total * dt / r;
+  return t;
+}
+
+// The conserved sum of a cell before cons2prim: cell_adjust_RK_cons, the phi
+// and r face increments in the reference's order, cell_add_src, cooling,
+// cell_add_visc_src and cell_add_split_fictitious (the forward stops after
+// `stop` like the stage-parity path; returns false when it stopped early).
+// Writes rkcons in substep 1 when `write_rk`.
+template <typename T>
+__device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, const Annulus &A, int a, int g,
+                                           int substep, int stop, double dt, bool write_rk, T *c) {
+  const int N = d.n_cells;
+  const DiskParams &P = d.par[A.inst];
+  const InstState &S = d.ist[A.inst];
+  const int j = g - A.cell_off;
+  const int np = A.np;
+  const double RK = substep == 1 ? 0.0 : 0.5;
+  // cell_copy (substep 1) + cell_adjust_RK_cons (cell_misc.c:28-57)
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    T cq = ldq<T>(d.cons, tp.cons, q, N, g);
+    T rk;
+    if (substep == 1) {
+      rk = cq;
+      if (write_rk) stq<T>(d.rkcons, tp.rkcons, q, N, g, cq);
+    } else {
+      rk = ldq<T>(d.rkcons, tp.rkcons, q, N, g);
+    }
+    c[q] = (1.0 - RK) * cq + RK * rk;
+  }
+  if (stop <= 1) return false;
+  // phi faces: for j = 0 the face (0,1) comes before (N-1,0)
+  {
+    const int gl = j == 0 ? A.cell_off + np - 1 : g - 1;
+    const double r = .5 * (A.rp + A.rm);
+    auto addL = [&](int f) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.fphi, tp.fphi, q, N, f);
+      if (P.has_visc) {
+        c[D_SRR] -= ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] -= ldq<T>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] -= ldq<T>(d.fphi, tp.fphi, 7, N, f);
+      }
+    };
+    auto addR = [&](int f) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.fphi, tp.fphi, q, N, f);
+      if (P.has_visc) {
+        c[D_SRR] += ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] += ldq<T>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] += ldq<T>(d.fphi, tp.fphi, 7, N, f);
+      }
+    };
+    if (j == 0) {
+      addL(g);
+      addR(gl);
+    } else {
+      addR(gl);
+      addL(g);
+    }
+  }
+  if (stop == 2) return false;
+  // r faces in face-list order
+  {
+    const int NS = d.n_slots;
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int asR) {
+      if (asR) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.frf, tp.frf, q, NS, slot);
+        if (P.has_visc) {
+          double rR = F.r + F.dr;
+          c[D_SRR] += ldq<T>(d.frf, tp.frf, 5, NS, slot) / rR;
+          c[D_LLL] += ldq<T>(d.frf, tp.frf, 6, NS, slot);
+          c[D_TAU] += ldq<T>(d.frf, tp.frf, 7, NS, slot);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.frf, tp.frf, q, NS, slot);
+        if (P.has_visc) {
+          double rL = F.r - F.dl;
+          c[D_SRR] -= ldq<T>(d.frf, tp.frf, 5, NS, slot) / rL;
+          c[D_LLL] -= ldq<T>(d.frf, tp.frf, 6, NS, slot);
+          c[D_TAU] -= ldq<T>(d.frf, tp.frf, 7, NS, slot);
+        }
+      }
+    });
+  }
+  if (stop == 3) return false;
+  // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
+  // increments come from k_source; added here in the reference's order
+  c[D_SRR] += ldq<T>(d.src, tp.src, 0, N, g);
+  c[D_SRR] += ldq<T>(d.src, tp.src, 1, N, g);
+  c[D_LLL] += ldq<T>(d.src, tp.src, 2, N, g);
+  c[D_SZZ] += ldq<T>(d.src, tp.src, 3, N, g);
+  c[D_TAU] += ldq<T>(d.src, tp.src, 4, N, g);
+  if (P.rho_sink_on == 1) {
+    for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldq<T>(d.src, tp.src, 6 + p, N, g);
+  }
+  const double rm = A.rm, rp = A.rp;
+  const double r = .5 * (rp + rm);
+  if (P.cooling == 1) {
+    // cooling reads the running tau (cell_source.c:187-203)
+    const T rho = ldq<T>(d.prim, tp.prim, D_RHO, N, g), Pp = ldq<T>(d.prim, tp.prim, D_PPP, N, g);
+    const double dV = d.dphi[g] * .5 * A.dv_diff * P.dz;
+    if (P.init_type == DI_SHEAR) {
+      T cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
+      if (cooling_term < 0.0) cooling_term = 0.0;
+      c[D_TAU] -= cooling_term * dt;
+    } else {
+      double numfac = 1.0;
+      double alpha = P.visc;
+      T cooling_cap = c[D_TAU] * numfac;
+      T cooling_term = 9. / 4. * alpha * pow(P.poro_r1, -3) / rho * pow(Pp / rho, 4.) * dt * dV;
+      if (cooling_term > cooling_cap) cooling_term = cooling_cap;
+      c[D_TAU] -= cooling_term;
+    }
+  }
+  if (P.has_visc) c[D_TAU] += ldq<T>(d.src, tp.src, 5, N, g);
+  // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
+  {
+    const double a_sep = S.gr[0] + S.gr[1];
+    const double rom = frame_rom(P, A.rom, r, a_sep);
+    const double Omega = rom / r;
+    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
+    const int NA = d.n_ann;
+    const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
+    if (kappa > 0.) split_rotate(c, d.ann_c[NA + a], d.ann_c[2 * NA + a], dr_r2Om, kappa, Omega, r);
+  }
+  return stop > 4;
+}
+
+// cell_update_phi + cell_update_dphi (src/Cell/cell_misc.c:59-96): the new
+// phi edge tn of cell g, its RK copy rk and the new width.
+__device__ __forceinline__ double mesh_advance(const DevPtrs &d, const Annulus &A, int a, int g, int substep,
+                                               double dt, double &tn, double &rk) {
+  const DiskParams &P = d.par[A.inst];
+  const InstState &S = d.ist[A.inst];
+  const double RK = substep == 1 ? 0.0 : 0.5;
+  const int j = g - A.cell_off;
+  const double r = .5 * (A.rm + A.rp);
+  const double a_sep = S.gr[0] + S.gr[1];
+  const double w_total = d.w_ann[a] + frame_rom(P, A.rom, r, a_sep);
+  const double *tin = substep == 1 ? d.tiph0 : d.tiph1;
+  const int gm1 = j == 0 ? A.cell_off + A.np - 1 : g - 1;
+  rk = substep == 1 ? tin[g] : d.rktiph[g];
+  double rkm = substep == 1 ? tin[gm1] : d.rktiph[gm1];
+  tn = new_tiph(d.tiphw[g], rk, RK, w_total, dt, r, d.err);
+  double tnm = new_tiph(d.tiphw[gm1], rkm, RK, w_total, dt, r, d.err);
+  double dphi_n = tn - tnm;
+  return wrap_pos(dphi_n, d.err);
+}
+
+// cell_boundary_fixed_r (src/Cell/cell_boundary.c:208-231) and cell_bc_damp
+// (src/Cell/cell_misc.c:98-132) on the new prims of a cell.
+template <typename T>
+__device__ __forceinline__ void bc_damp(const DevPtrs &d, const Annulus &A, int a, T *pr) {
+  const DiskParams &P = d.par[A.inst];
+  if ((A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC)) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) pr[q] = A.ic[q];
+  }
+  if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
+    double f = d.ann_c[3 * d.n_ann + a];  // 1.-exp(-rate*dt), k_source
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      T dprim = A.ic[q] - pr[q];
+      pr[q] += f * dprim;
+    }
+  }
+}
+
+}  // namespace
+
+#endif

@@ -51,6 +51,9 @@ SIGNATURES = {
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
     "dgpu_torque": (_I, [_P, _I, _dp]),
     "dgpu_face_list_noalloc": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _ip, _P]),
+    "dgpu_objective": (_I, [_P, _I, _I, _dp, _dp, _dp]),
+    "dgpu_tangent": (_I, [_P, _I, _I, _D, _D, _dp, _dp, _dp]),
+    "dgpu_adjoint": (_I, [_P, _I, _I, _I, _dp, _dp, _dp, _dp, _dp]),
 }
 
 _lib = None
@@ -254,3 +257,41 @@ class Context:
         v = C.c_double()
         self._ck(load().dgpu_torque(self._h, inst, C.byref(v)))
         return v.value
+
+    # ---- differentiation (one disk per context) ----
+    def objective(self, nsteps: int, window_start: int, dt=None, return_dt: bool = False):
+        """J = (mean torque, mean accretion rate) over steps window_start+1..nsteps;
+        dt (nsteps values) freezes the dt schedule instead of the CFL dt."""
+        J = np.zeros(2)
+        dt_out = np.zeros(nsteps)
+        dt_in = None
+        if dt is not None:
+            dt = np.ascontiguousarray(dt, dtype=np.float64)
+            assert dt.shape == (nsteps,)
+            dt_in = _dptr(dt)
+        self._ck(load().dgpu_objective(self._h, nsteps, window_start, dt_in, _dptr(dt_out), _dptr(J)))
+        return (J, dt_out) if return_dt else J
+
+    def tangent(self, nsteps: int, window_start: int, dq: float = 0.0, dalpha: float = 0.0,
+                dprim: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """(J, dJ/de) along dq/de, dalpha/de and d prim_0/de ([N][5] or None)."""
+        J, dJ = np.zeros(2), np.zeros(2)
+        dp = None
+        if dprim is not None:
+            dprim = np.ascontiguousarray(dprim, dtype=np.float64)
+            dp = _dptr(dprim)
+        self._ck(load().dgpu_tangent(self._h, nsteps, window_start, float(dq), float(dalpha), dp,
+                                     _dptr(J), _dptr(dJ)))
+        return J, dJ
+
+    def adjoint(self, nsteps: int, window_start: int, ckpt_every: int = 25,
+                weights=(1.0, 0.0)) -> dict:
+        """Gradient of weights . J with respect to q, alpha and the initial prims."""
+        w = np.asarray(weights, dtype=np.float64)
+        J = np.zeros(2)
+        dq, da = C.c_double(), C.c_double()
+        n = self.sims[0].num_cells
+        dprim = np.zeros((n, 5))
+        self._ck(load().dgpu_adjoint(self._h, nsteps, window_start, ckpt_every, _dptr(w), _dptr(J),
+                                     C.byref(dq), C.byref(da), _dptr(dprim)))
+        return {"J": J, "dq": dq.value, "dalpha": da.value, "dprim": dprim}

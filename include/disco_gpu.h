@@ -168,6 +168,35 @@ int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double
  * diagnostic). */
 int dgpu_torque(dgpu_ctx *ctx, int inst, double *torque);
 
+/* ---- Differentiation (a context holding one disk) ------------------------------
+ * No counterpart in the reference.  A run advances the context's disk by
+ * nsteps RK2 steps from its current state (leaving it at the final state,
+ * like dgpu_step_rk2) and evaluates, after each step n, the binary torque T_n
+ * (as dgpu_torque) and the accretion rate through the innermost non-ghost
+ * annulus Mdot_n = -sum rho v_r r dphi dz; J[0] and J[1] are their
+ * dt-weighted means over steps window_start+1 .. nsteps.
+ * Derivatives are taken with the dt schedule of the run frozen and are with
+ * respect to the mass ratio q (MassRatio, through the binary's masses and
+ * orbit radii), alpha (Explicit_Viscosity) and the initial prims.  Refused
+ * (DGPU_ERR_UNSUPPORTED) for contexts with several disks, C_RIGID meshes
+ * (state-dependent mesh motion), Cooling and RhoSinkOn. */
+/* dt_in (nsteps values, or NULL for the CFL dt) replaces the CFL dt of each
+ * step: the frozen schedule under which finite differences match the
+ * derivatives below; dt_out (nsteps, may be NULL) receives the dt used. */
+int dgpu_objective(dgpu_ctx *ctx, int nsteps, int window_start, const double *dt_in, double *dt_out, double *J);
+/* Forward-mode tangent: dJ[k] = dJ_k/de along dq/de = dq, dalpha/de = dalpha,
+ * d prim_0/de = dprim ([N][NUM_Q] in the cell order of dgpu_set_state, or
+ * NULL for zero). */
+int dgpu_tangent(dgpu_ctx *ctx, int nsteps, int window_start, double dq, double dalpha, const double *dprim,
+                 double *J, double *dJ);
+/* Reverse mode: the gradient of weights[0] J[0] + weights[1] J[1] (weights
+ * NULL: J[0]) with respect to q, alpha and the initial prims (dJ_dprim
+ * [N][NUM_Q], may be NULL).  Stores the state every ckpt_every steps and
+ * recomputes the steps in between (device memory grows with
+ * nsteps / ckpt_every + 2 ckpt_every stored states of 19 doubles per cell). */
+int dgpu_adjoint(dgpu_ctx *ctx, int nsteps, int window_start, int ckpt_every, const double *weights, double *J,
+                 double *dJ_dq, double *dJ_dalpha, double *dJ_dprim);
+
 #ifdef __cplusplus
 }
 #endif

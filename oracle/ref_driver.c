@@ -18,6 +18,15 @@
  *       loop alone goes to stderr as "steps_wall_s <seconds>"; --warmup runs W
  *       untimed steps first (not dumped).
  *
+ *   disco_ref objective <par> <nsteps> <out.txt> [--load in.bin] [--dtfile dt.txt]
+ *       runs nsteps steps and writes "n t dt torque mdot" after each: the
+ *       binary torque -sum r rho dV F_phi over non-ghost cells (F_phi from the
+ *       reference's gravMassForce, src/Cell/cell_source.c:49-71) and the
+ *       accretion rate -sum rho v_r r dphi dz over the innermost non-ghost
+ *       annulus.  --dtfile freezes the dt schedule: each step runs the calls of
+ *       timestep_rk2 (src/TimeStep/timestep_algorithm.c:13-39) in its order
+ *       with timestep_set_dt replaced by the next dt of the file.
+ *
  *   disco_ref stage <par> <phase> <out.bin> [--load in.bin]
  *       runs the prologue of timestep_rk2 and then the body of
  *       timestep_substep (src/TimeStep/timestep_routines.c:16-113), calling
@@ -224,8 +233,60 @@ out:
   face_destroy(Fr);
 }
 
+void gravMassForce(struct GravMass *theGravMasses, struct Sim *theSim, int p, double r, double phi, double *fr,
+                   double *fp);
+
+/* timestep_rk2 (src/TimeStep/timestep_algorithm.c:13-39) with a given dt in
+ * place of timestep_set_dt: the same reference calls in the same order. */
+static void rk2_frozen_dt(struct TimeStep *ts, struct Sim *s, struct Cell ***cells, struct GravMass *gm,
+                          struct MPIsetup *mpi, double dt) {
+  int p;
+  cell_clear_w(cells, s);
+  cell_set_w(cells, s);
+  ts->dt = dt;
+  cell_copy(cells, s);
+  gravMass_copy(gm, s);
+  timestep_set_RK(ts, 0.0);
+  timestep_substep(ts, cells, s, gm, mpi, 1.0);
+  gravMass_move(s, gm, timestep_get_t(ts), 1.0 * timestep_dt(ts));
+  timestep_set_RK(ts, 0.5);
+  timestep_substep(ts, cells, s, gm, mpi, 0.5);
+  gravMass_move(s, gm, timestep_get_t(ts), 0.5 * timestep_dt(ts));
+  timestep_update_t(ts);
+  for (p = 0; p < sim_NumGravMass(s); ++p)
+    gravMass_set_Macc(gm, gravMass_Macc(gm, p) + gravMass_Mdot(gm, p) * timestep_dt(ts), p);
+}
+
+/* The two objectives of the differentiated runs on the current state. */
+static void objectives(struct Sim *s, struct Cell ***cells, struct GravMass *gm, double *torque, double *mdot) {
+  int i, j, p, NR = sim_N(s, R_DIR), n = 0;
+  int i0 = sim_Nghost_min(s, R_DIR), i1 = NR - sim_Nghost_max(s, R_DIR);
+  double dz = sim_FacePos(s, 0, Z_DIR) - sim_FacePos(s, -1, Z_DIR);
+  struct Cell *c = cell_base(cells);
+  double T = 0.0, M = 0.0;
+  for (i = 0; i < NR; ++i) {
+    double rm = sim_FacePos(s, i - 1, R_DIR), rp = sim_FacePos(s, i, R_DIR);
+    double r = .5 * (rm + rp);
+    for (j = 0; j < sim_N_p(s, i); ++j, ++n) {
+      double dphi = c[n].dphi, phi = c[n].tiph - .5 * dphi, rho = c[n].prim[RHO];
+      if (i >= i0 && i < i1) {
+        double dV = dphi * .5 * (rp * rp - rm * rm) * dz, Fp = 0.0;
+        for (p = 0; p < 2; ++p) {
+          double fr, fp;
+          gravMassForce(gm, s, p, r, phi, &fr, &fp);
+          Fp += fp;
+        }
+        T += -(r * rho * dV * Fp);
+      }
+      if (i == i0) M += -(rho * c[n].prim[URR] * r * dphi * dz);
+    }
+  }
+  *torque = T;
+  *mdot = M;
+}
+
 int main(int argc, char **argv) {
-  const char *mode, *par, *out, *load = NULL, *faces = NULL, *dtlog = NULL;
+  const char *mode, *par, *out, *load = NULL, *faces = NULL, *dtlog = NULL, *dtfile = NULL;
   int nsteps, a, step, warmup = 0;
   char parbuf[1024];
   struct MPIsetup *mpi;
@@ -247,6 +308,7 @@ int main(int argc, char **argv) {
     else if (!strcmp(argv[a], "--faces") && a + 1 < argc) faces = argv[++a];
     else if (!strcmp(argv[a], "--dtlog") && a + 1 < argc) dtlog = argv[++a];
     else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = atoi(argv[++a]);
+    else if (!strcmp(argv[a], "--dtfile") && a + 1 < argc) dtfile = argv[++a];
     else {
       fprintf(stderr, "unknown option %s\n", argv[a]);
       return 2;
@@ -303,6 +365,29 @@ int main(int argc, char **argv) {
     fprintf(stderr, "steps_wall_s %.9f\n", (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec));
     if (flog) fclose(flog);
     dump_state(out, s, cells, gm, ts, 0);
+  } else if (!strcmp(mode, "objective")) {
+    FILE *fo = fopen(out, "w"), *fd = dtfile ? fopen(dtfile, "r") : NULL;
+    if (!fo || (dtfile && !fd)) {
+      fprintf(stderr, "cannot open %s\n", fo ? dtfile : out);
+      return 2;
+    }
+    for (step = 0; step < nsteps; ++step) {
+      double T, M;
+      if (fd) {
+        double dt;
+        if (fscanf(fd, "%lf", &dt) != 1) {
+          fprintf(stderr, "dt file has fewer than %d values\n", nsteps);
+          return 2;
+        }
+        rk2_frozen_dt(ts, s, cells, gm, mpi, dt);
+      } else {
+        timestep_rk2(ts, s, cells, gm, mpi);
+      }
+      objectives(s, cells, gm, &T, &M);
+      fprintf(fo, "%d %.17g %.17g %.17g %.17g\n", step + 1, ts->t, ts->dt, T, M);
+    }
+    fclose(fo);
+    if (fd) fclose(fd);
   } else if (!strcmp(mode, "stage")) {
     /* prologue of timestep_rk2 (timestep_algorithm.c:13-24), then one substep */
     cell_clear_w(cells, s);

@@ -1,0 +1,195 @@
+"""Differentiation of the step on the GPU: objective, tangent and adjoint.
+
+The tangent (Dual instances of the forward kernels) must reproduce the
+forward trajectory bit for bit and agree with central finite differences of
+the GPU forward; the adjoint must be the transpose of the tangent (the
+dot-product test <grad J, v> = dJ/de along v, to round-off) for q, alpha and
+random directions in the initial prims, whatever the checkpoint spacing.
+The derivatives hold the dt schedule fixed, so the finite differences replay
+the unperturbed run's dt schedule (dgpu_objective with dt_in)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from disco2_b200 import configs, lib
+
+pytestmark = pytest.mark.gpu
+
+NSTEPS, W0 = 40, 20
+Q0, ALPHA0 = 0.5, 0.1  # q = 1 is the symmetric point, where dJ/dq is round-off small
+
+
+def _cbd(q=Q0, alpha=ALPHA0):
+    return configs.circumbinary(num_r=64, q=q, alpha=alpha)
+
+
+@pytest.fixture(scope="module")
+def base():
+    s = lib.Sim(_cbd())
+    ctx = lib.Context(s)
+    ctx.init_state(0)
+    st = ctx.get_state(0)
+    J, dt = ctx.objective(NSTEPS, W0, return_dt=True)
+    ctx.close()
+    return {"prim": st["prim"], "tiph": st["tiph"], "dphi": st["dphi"], "N": s.num_cells, "dt": dt, "J": J}
+
+
+def _ctx(base, q=Q0, alpha=ALPHA0, prim=None):
+    ctx = lib.Context(lib.Sim(_cbd(q, alpha)))
+    ctx.init_state(0)  # binary of this q
+    ctx.set_state(0, base["prim"] if prim is None else prim, base["tiph"], base["dphi"])
+    return ctx
+
+
+def _J(base, **kw):
+    """J with the unperturbed run's dt schedule."""
+    ctx = _ctx(base, **kw)
+    J = ctx.objective(NSTEPS, W0, dt=base["dt"])
+    ctx.close()
+    return J
+
+
+def _direction(base, seed):
+    """A relative perturbation of the surface density with the pressure
+    following it (P/rho fixed): d rho = rho u, d P = P u, u ~ N(0, 1)."""
+    u = np.random.default_rng(seed).standard_normal(base["N"])
+    d = np.zeros((base["N"], 5))
+    d[:, 0] = base["prim"][:, 0] * u
+    d[:, 1] = base["prim"][:, 1] * u
+    return d
+
+
+def test_tangent_reproduces_forward(base):
+    ctx = _ctx(base)
+    J, dJ = ctx.tangent(NSTEPS, W0, dq=1.0)
+    st_t = ctx.get_state(0)
+    ctx.close()
+    ctx = _ctx(base)
+    J0 = ctx.objective(NSTEPS, W0)
+    st_f = ctx.get_state(0)
+    ctx.close()
+    assert np.array_equal(J, J0)
+    assert np.array_equal(st_t["prim"], st_f["prim"])
+    # the frozen-dt forward with the run's own schedule is the same run
+    assert np.array_equal(_J(base), J0)
+    assert np.all(np.isfinite(dJ)) and np.any(dJ != 0.0)
+
+
+@pytest.mark.parametrize("which", ["q", "alpha", "sigma"])
+def test_tangent_matches_finite_differences(base, which):
+    """Central differences of the frozen-dt GPU forward with a relative step of
+    1e-8: small enough that no limiter or Riemann-state branch flips between
+    the two runs (at 1e-6 some do, and the differences of the accretion rate
+    then move by up to ~1e-2), large enough that round-off stays below ~1e-7
+    of the derivative.  The torque is a sum with strong cancellation, so its
+    differences carry ~1e-5 of round-off noise."""
+    h = 1e-8
+    ctx = _ctx(base)
+    if which == "q":
+        _, dJ = ctx.tangent(NSTEPS, W0, dq=1.0)
+        fd = (_J(base, q=Q0 * (1 + h)) - _J(base, q=Q0 * (1 - h))) / (2 * Q0 * h)
+    elif which == "alpha":
+        _, dJ = ctx.tangent(NSTEPS, W0, dalpha=1.0)
+        fd = (_J(base, alpha=ALPHA0 * (1 + h)) - _J(base, alpha=ALPHA0 * (1 - h))) / (2 * ALPHA0 * h)
+    else:
+        v = _direction(base, 3)
+        _, dJ = ctx.tangent(NSTEPS, W0, dprim=v)
+        fd = (_J(base, prim=base["prim"] + h * v) - _J(base, prim=base["prim"] - h * v)) / (2 * h)
+    ctx.close()
+    rel = np.abs(dJ - fd) / np.maximum(np.abs(fd), 1e-300)
+    print(which, dJ, fd, rel)
+    assert rel[1] < 1e-6, (which, dJ, fd, rel)   # accretion rate
+    assert rel[0] < 1e-4, (which, dJ, fd, rel)   # torque
+
+
+@pytest.mark.parametrize("weights", [(1.0, 0.0), (0.0, 1.0)])
+def test_adjoint_is_transpose_of_tangent(base, weights):
+    w = np.array(weights)
+    ctx = _ctx(base)
+    g = ctx.adjoint(NSTEPS, W0, ckpt_every=7, weights=weights)
+    ctx.close()
+    checks = []
+    ctx = _ctx(base)
+    _, dJ = ctx.tangent(NSTEPS, W0, dq=1.0)
+    ctx.close()
+    checks.append((g["dq"], w @ dJ))
+    ctx = _ctx(base)
+    _, dJ = ctx.tangent(NSTEPS, W0, dalpha=1.0)
+    ctx.close()
+    checks.append((g["dalpha"], w @ dJ))
+    for seed in (1, 2):
+        v = _direction(base, seed)
+        ctx = _ctx(base)
+        _, dJ = ctx.tangent(NSTEPS, W0, dprim=v)
+        ctx.close()
+        checks.append((float(np.sum(g["dprim"] * v)), w @ dJ))
+    # a direction in every prim, ghost annuli included
+    v = np.random.default_rng(5).standard_normal((base["N"], 5)) * 1e-2
+    ctx = _ctx(base)
+    _, dJ = ctx.tangent(NSTEPS, W0, dprim=v)
+    ctx.close()
+    checks.append((float(np.sum(g["dprim"] * v)), w @ dJ))
+    for a, t in checks:
+        assert abs(a - t) <= 1e-9 * max(abs(t), 1e-300), checks
+
+
+def test_adjoint_independent_of_checkpoint_spacing(base):
+    out = []
+    for K in (1, 6, NSTEPS):
+        ctx = _ctx(base)
+        g = ctx.adjoint(NSTEPS, W0, ckpt_every=K)
+        st = ctx.get_state(0)
+        ctx.close()
+        out.append((g, st))
+    for g, st in out[1:]:
+        assert g["dq"] == out[0][0]["dq"] and g["dalpha"] == out[0][0]["dalpha"]
+        assert np.array_equal(g["dprim"], out[0][0]["dprim"])
+        assert np.array_equal(st["prim"], out[0][1]["prim"])
+
+
+def test_differentiation_refuses_unsupported():
+    s = lib.Sim(configs.gresho(num_r=16))  # C_RIGID mesh
+    ctx = lib.Context(s)
+    ctx.init_state(0)
+    with pytest.raises(lib.DiscoError):
+        ctx.objective(4, 2)
+    ctx.close()
+
+
+def test_gradient_matches_reference_finite_differences():
+    """The adjoint gradient of the circumbinary disk at 192 annuli over 500
+    steps (objectives averaged over steps 251-500, checkpoints every 25 steps)
+    against central finite differences of the reference C code with the same
+    frozen dt schedule (tests/golden/cbd192_fd.json, made by
+    tests/golden/make_fd_reference.py): q, alpha and 16 seeded directions of
+    the initial surface density."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "cbd192_fd.json")
+    ref = json.load(open(path))
+    s = lib.Sim(configs.circumbinary(num_r=ref["num_r"]))
+    assert s.num_cells == ref["cells"]
+    grads = []
+    for w in ((1.0, 0.0), (0.0, 1.0)):
+        ctx = lib.Context(s)
+        ctx.init_state(0)
+        prim0 = ctx.get_state(0)["prim"]
+        grads.append(ctx.adjoint(ref["nsteps"], ref["window_start"], ckpt_every=25, weights=w))
+        ctx.close()
+    assert np.allclose([grads[0]["J"][0], grads[1]["J"][1]], ref["J"], rtol=1e-8, atol=0)
+    fd = ref["fd"]["1e-08"]
+    rows = []
+    for k in range(2):
+        g = grads[k]
+        rows.append(("q", k, g["dq"], fd["q"][k]))
+        rows.append(("alpha", k, g["dalpha"], fd["alpha"][k]))
+        for d in range(len(fd["sigma"])):
+            u = np.random.default_rng(1000 + d).standard_normal(prim0.shape[0])
+            dirv = np.zeros_like(prim0)
+            dirv[:, 0] = prim0[:, 0] * u
+            dirv[:, 1] = prim0[:, 1] * u
+            rows.append((f"sigma{d}", k, float(np.sum(g["dprim"] * dirv)), fd["sigma"][d][k]))
+    for name, k, a, f in rows:
+        print(f"{name:8s} {'torque' if k == 0 else 'mdot':6s} adjoint={a:+.9e} reference_fd={f:+.9e} "
+              f"rel={abs(a - f) / max(abs(f), 1e-300):.2e}")
