@@ -27,6 +27,12 @@
 #include "dgpu_adjoint.cuh"
 #include "dgpu_step.cuh"
 
+// minimum resident blocks per SM for the three heavy adjoint kernels (their
+// reverse sweeps hold ~170 registers per thread without a bound)
+#ifndef DGPU_MINB_ADJ
+#define DGPU_MINB_ADJ 2
+#endif
+
 namespace {
 
 // Deterministic block sum of K values per thread into out[0..K-1] (every
@@ -51,6 +57,33 @@ __device__ __forceinline__ void block_partial(const double (&v)[K], double *out)
       out[k] = s;
     }
   }
+}
+
+// Deterministic sum of rows [0, nrows) of a [rows][stride] array, columns
+// [0, K), by one whole block: thread t sums rows t, t + blockDim.x, ... in
+// order, then a fixed-shape tree over the threads.  Result in out[0..K-1]
+// (written by thread 0).  blockDim.x must be a power of two <= BLK.
+template <int K>
+__device__ __forceinline__ void block_rows_sum(const double *rows, int nrows, int stride, double *out) {
+  __shared__ double sh[K][BLK];
+  double s[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) s[k] = 0.0;
+  for (int b = threadIdx.x; b < nrows; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] += ((volatile const double *)rows)[(size_t)stride * b + k];
+#pragma unroll
+  for (int k = 0; k < K; ++k) sh[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+#pragma unroll
+      for (int k = 0; k < K; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = sh[k][0];
 }
 
 // per-thread adjoints of (M0, M1, r0, r1, alpha) from position adjoints
@@ -113,9 +146,11 @@ __device__ __forceinline__ void objective_cell(const DevPtrs &d, const TanPtrs &
 
 // Sums over the disk (one context = one disk) into out[0..1] (torque,
 // accretion rate) and, for the tangent, their derivatives into out_d[0..1];
-// per-block partials reduced in block order by the last block.
+// per-block partials reduced in block order by the last block.  With idx,
+// out and out_d advance by 2 * (*idx) (the step's slot of a log).
 template <typename T>
-__global__ void __launch_bounds__(BLK) k_objective(DevPtrs d, TanPtrs tp, double *part, double *out, double *out_d) {
+__global__ void __launch_bounds__(BLK) k_objective(DevPtrs d, TanPtrs tp, double *part, double *out, double *out_d,
+                                                   const int *idx) {
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -134,35 +169,99 @@ __global__ void __launch_bounds__(BLK) k_objective(DevPtrs d, TanPtrs tp, double
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(&d.counters[3], 1u) == gridDim.x - 1;
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last) return;
   __threadfence();
-  double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int b = 0; b < (int)gridDim.x; ++b)
-    for (int k = 0; k < 4; ++k) s[k] += ((volatile double *)part)[4 * b + k];
-  out[0] = s[0];
-  out[1] = s[1];
+  __shared__ double s[4];
+  block_rows_sum<4>(part, gridDim.x, 4, s);
+  if (threadIdx.x != 0) return;
+  const size_t o = idx ? 2 * (size_t)(*idx) : 0;
+  out[o] = s[0];
+  out[o + 1] = s[1];
   if (out_d) {
-    out_d[0] = s[2];
-    out_d[1] = s[3];
+    out_d[o] = s[2];
+    out_d[o + 1] = s[3];
   }
   d.counters[3] = 0;
 }
 
-// Adjoint of wT * torque + wM * accretion on the current state, added to lW;
-// binary adjoints to part rows [row0, row0 + gridDim.x).
-__global__ void __launch_bounds__(BLK) a_objective(DevPtrs d, AdjPtrs J, double wT, double wM, int row0) {
+// End of a logged step: dtlog[*idx] = dt of the step, then ++*idx.
+__global__ void k_step_end(DevPtrs d, double *dtlog, int *idx) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    dtlog[*idx] = d.ist[0].dt;
+    *idx += 1;
+  }
+}
+// A frozen dt schedule: the dt of step *idx in place of the CFL value.
+__global__ void k_set_dt(DevPtrs d, const double *dtin, const int *idx) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) d.ist[0].dt = dtin[*idx];
+}
+__global__ void k_set_int(int *p, int v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *p = v;
+}
+__global__ void k_add_int(int *p, int dv) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *p += dv;
+}
+
+// Stored states: 19 doubles per cell (prim, cons, rkcons, tiph0, tiph1,
+// rktiph, dphi) and the disk states.  save: context -> store; else back.
+__device__ __forceinline__ void snap_copy_dev(const DevPtrs &d, double *sb, InstState *si, int save) {
+  const size_t N = (size_t)d.n_cells;
+  const size_t n = 19 * N;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double *c;
+    if (i < 5 * N) c = d.prim + i;
+    else if (i < 10 * N) c = d.cons + (i - 5 * N);
+    else if (i < 15 * N) c = d.rkcons + (i - 10 * N);
+    else if (i < 16 * N) c = d.tiph0 + (i - 15 * N);
+    else if (i < 17 * N) c = d.tiph1 + (i - 16 * N);
+    else if (i < 18 * N) c = d.rktiph + (i - 17 * N);
+    else c = d.dphi + (i - 18 * N);
+    if (save) sb[i] = *c;
+    else *c = sb[i];
+  }
+  if (blockIdx.x == 0) {
+    const int nw = (int)(sizeof(InstState) / sizeof(unsigned long long)) * d.n_inst;
+    unsigned long long *a = reinterpret_cast<unsigned long long *>(d.ist);
+    unsigned long long *b = reinterpret_cast<unsigned long long *>(si);
+    for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+      if (save) b[w] = a[w];
+      else a[w] = b[w];
+    }
+  }
+}
+__global__ void __launch_bounds__(BLK) k_snap_ptr(DevPtrs d, double *sb, InstState *si, int save) {
+  snap_copy_dev(d, sb, si, save);
+}
+// the store of slot *idx + off of a table of stores
+__global__ void __launch_bounds__(BLK) k_snap_tab(DevPtrs d, double *const *bufs, InstState *const *ists,
+                                                  const int *idx, int off, int save) {
+  const int k = *idx + off;
+  snap_copy_dev(d, bufs[k], ists[k], save);
+}
+
+// Adjoint of wT * torque + wM * accretion on the stored state of slot
+// *idx + off (prims, phi edges, widths, disk state), added to lW; binary
+// adjoints to part rows [row0, row0 + gridDim.x).  The weights of the step
+// are wts[2 n], wts[2 n + 1] with n = *base + *idx.
+__global__ void __launch_bounds__(BLK) a_objective(DevPtrs d, AdjPtrs J, double *const *bufs,
+                                                   InstState *const *ists, const int *idx, int off,
+                                                   const double *wts, const int *base, int row0) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double *sb = bufs[*idx + off];
+  const double *prim = sb, *tiph0 = sb + 15 * (size_t)N, *dphiv = sb + 18 * (size_t)N;
+  const int n = *base + *idx;
+  const double wT = wts[2 * n], wM = wts[2 * n + 1];
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  if (g < d.n_cells) {
-    const int N = d.n_cells;
+  if (g < N) {
     const Annulus A = d.ann[d.cell_ann[g]];
     const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const double dphi = d.dphi[g];
+    const InstState &S = ists[*idx + off][A.inst];
+    const double dphi = dphiv[g];
     const double r = .5 * (A.rp + A.rm);
     if ((A.kind & DGPU_AK_CFL) && wT != 0.0) {
-      const double phi = d.tiph0[g] - .5 * dphi;
-      const double rho = ld(d.prim, D_RHO, N, g);
+      const double phi = tiph0[g] - .5 * dphi;
+      const double rho = ld(prim, D_RHO, N, g);
       const double dV = dphi * .5 * A.dv_diff * P.dz;
       const double cosp = cos(phi), sinp = sin(phi);
       double Fp = 0.0, f1[2], sinap[2], dx[2], dy[2], sr[2], cosa[2], sina[2], cg[2], sg[2];
@@ -184,11 +283,11 @@ __global__ void __launch_bounds__(BLK) a_objective(DevPtrs d, AdjPtrs J, double 
       for (int p = 0; p < 2; ++p) {
         const double asinap = aFp * f1[p], af1 = aFp * sinap[p];
         const double asina = asinap * cosp, acosa = -asinap * sinp;
-        const int n = P.phi_order;
-        const double qv = fgrav(1.0, sr[p], P.g_eps, n);
+        const int no = P.phi_order;
+        const double qv = fgrav(1.0, sr[p], P.g_eps, no);
         v[DGPU_AP_M0 + p] += -af1 * qv;
-        const double srn = dpow(sr[p], (double)n), epn = dpow(P.g_eps, (double)n);
-        const double dln = (n - 1.) / sr[p] - (n + 1.) * dpow(sr[p], n - 1.) / (srn + epn);
+        const double srn = dpow(sr[p], (double)no), epn = dpow(P.g_eps, (double)no);
+        const double dln = (no - 1.) / sr[p] - (no + 1.) * dpow(sr[p], no - 1.) / (srn + epn);
         double asr = af1 * f1[p] * dln - (acosa * dx[p] + asina * dy[p]) / (sr[p] * sr[p]);
         const double adx = acosa / sr[p] + asr * dx[p] / sr[p];
         const double ady = asina / sr[p] + asr * dy[p] / sr[p];
@@ -197,7 +296,7 @@ __global__ void __launch_bounds__(BLK) a_objective(DevPtrs d, AdjPtrs J, double 
       }
     }
     if ((A.kind & DGPU_AK_MDOT) && wM != 0.0) {
-      const double rho = ld(d.prim, D_RHO, N, g), vr = ld(d.prim, D_URR, N, g);
+      const double rho = ld(prim, D_RHO, N, g), vr = ld(prim, D_URR, N, g);
       const double k = r * dphi * P.dz;
       J.lW[(size_t)D_RHO * N + g] += -wM * vr * k;
       J.lW[(size_t)D_URR * N + g] += -wM * rho * k;
@@ -206,13 +305,12 @@ __global__ void __launch_bounds__(BLK) a_objective(DevPtrs d, AdjPtrs J, double 
   block_partial<5>(v, J.part + DGPU_AP_N * (size_t)(row0 + blockIdx.x));
 }
 
-// Sums part rows [row0, row0 + nrows) in order and adds dJ/dq and dJ/dalpha to
-// acc (one thread).
-__global__ void a_par_reduce(AdjPtrs J, int row0, int nrows) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int b = row0; b < row0 + nrows; ++b)
-    for (int k = 0; k < 5; ++k) s[k] += J.part[DGPU_AP_N * (size_t)b + k];
+// Sums part rows [row0, row0 + nrows) (one block, deterministic order) and
+// adds dJ/dq and dJ/dalpha to acc.
+__global__ void __launch_bounds__(BLK) a_par_reduce(AdjPtrs J, int row0, int nrows) {
+  __shared__ double s[5];
+  block_rows_sum<5>(J.part + DGPU_AP_N * (size_t)row0, nrows, DGPU_AP_N, s);
+  if (threadIdx.x != 0) return;
   J.acc[0] += s[DGPU_AP_M0] * J.dq[0] + s[DGPU_AP_M1] * J.dq[1] + s[DGPU_AP_R0] * J.dq[2] + s[DGPU_AP_R1] * J.dq[3];
   J.acc[1] += s[DGPU_AP_ALPHA];
 }
@@ -220,79 +318,72 @@ __global__ void a_par_reduce(AdjPtrs J, int row0, int nrows) {
 // ---------------------------------------------------------------------------
 // Substep adjoint
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(BLK) a_update(DevPtrs d, AdjPtrs J, int substep) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int N = d.n_cells;
-  if (g >= N) return;
-  const int a = d.cell_ann[g];
-  const Annulus A = d.ann[a];
-  const DiskParams &P = d.par[A.inst];
-  const InstState &S = d.ist[A.inst];
-  const double fac = substep == 1 ? 1.0 : 0.5, RK = substep == 1 ? 0.0 : 0.5;
-  const double dt = fac * S.dt;
-  const TanPtrs none = {};
-  double c[5];
-  update_sum<double>(d, none, A, a, g, substep, 7, dt, false, c);
-  double tn, rk;
-  const double dphi_n = mesh_advance(d, A, a, g, substep, dt, tn, rk);
-  const double r = .5 * (A.rm + A.rp);
-  const double dV = A.dv_half * dphi_n * P.dz;
-  double pr[5];
-  cons2prim(c, dV, r, P, pr);
-  bc_damp<double>(d, A, a, pr);
-  double apr[5], alc[5];
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    apr[q] = J.lW[(size_t)q * N + g];
-    alc[q] = J.lC[(size_t)q * N + g];
-  }
-  prim2cons_rev(pr, r, dV, P.gamma, alc, apr);
-  if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
-    const double f = d.ann_c[3 * d.n_ann + a];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) apr[q] *= (1.0 - f);
-  }
-  if ((A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC)) {
-#pragma unroll
-    for (int q = 0; q < 5; ++q) apr[q] = 0.0;
-  }
-  double ac[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  cons2prim_rev(c, dV, r, P, apr, ac);
-  {
-    const double a_sep = S.gr[0] + S.gr[1];
-    const double rom = frame_rom(P, A.rom, r, a_sep);
-    const double Omega = rom / r;
-    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
-    const int NA = d.n_ann;
-    const double kappa = d.ann_c[a];
-    if (kappa > 0.) split_rotate_rev(ac, d.ann_c[NA + a], d.ann_c[2 * NA + a], dr_r2Om, kappa, Omega, r);
-  }
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    J.lU[(size_t)q * N + g] = ac[q];
-    double lc = (1.0 - RK) * ac[q];
-    if (substep == 1) lc += J.lCrk[(size_t)q * N + g];
-    else J.lCrk[(size_t)q * N + g] = RK * ac[q];
-    J.lC[(size_t)q * N + g] = lc;
-  }
-}
-
-__global__ void __launch_bounds__(BLK) a_source(DevPtrs d, AdjPtrs J, int substep, int row0) {
+// k_update reversed, then k_source reversed on the same cell (it reads only
+// the cell's own lU): lU, the substep's input lC / lCrk, and the source part
+// of lWt, lG[UPP], lGp[URR]; binary adjoints to part rows [row0, ...).
+__global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_update_source(DevPtrs d, AdjPtrs J, int substep, int row0) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (g < N) {
     const int a = d.cell_ann[g];
-    const Annulus &A = d.ann[a];
+    const Annulus A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
     const InstState &S = d.ist[A.inst];
-    const double fac = substep == 1 ? 1.0 : 0.5;
+    const double fac = substep == 1 ? 1.0 : 0.5, RK = substep == 1 ? 0.0 : 0.5;
+    const double dt = fac * S.dt;
+    const TanPtrs none = {};
+    const double r = .5 * (A.rm + A.rp);
+    double ac[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    {
+      double c[5];
+      update_sum<double>(d, none, A, a, g, substep, 7, dt, false, c);
+      double tn, rk;
+      const double dphi_n = mesh_advance(d, A, a, g, substep, dt, tn, rk);
+      const double dV = A.dv_half * dphi_n * P.dz;
+      double pr[5];
+      cons2prim(c, dV, r, P, pr);
+      bc_damp<double>(d, A, a, pr);
+      double apr[5], alc[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        apr[q] = J.lW[(size_t)q * N + g];
+        alc[q] = J.lC[(size_t)q * N + g];
+      }
+      prim2cons_rev(pr, r, dV, P.gamma, alc, apr);
+      if (P.has_damp && (A.kind & DGPU_AK_DAMP) && (A.kind & DGPU_AK_IC)) {
+        const double f = d.ann_c[3 * d.n_ann + a];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) apr[q] *= (1.0 - f);
+      }
+      if ((A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC)) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) apr[q] = 0.0;
+      }
+      cons2prim_rev(c, dV, r, P, apr, ac);
+    }
     const double a_sep = S.gr[0] + S.gr[1];
+    {
+      const double rom = frame_rom(P, A.rom, r, a_sep);
+      const double Omega = rom / r;
+      const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
+      const int NA = d.n_ann;
+      const double kappa = d.ann_c[a];
+      if (kappa > 0.) split_rotate_rev(ac, d.ann_c[NA + a], d.ann_c[2 * NA + a], dr_r2Om, kappa, Omega, r);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      J.lU[(size_t)q * N + g] = ac[q];
+      double lc = (1.0 - RK) * ac[q];
+      if (substep == 1) lc += J.lCrk[(size_t)q * N + g];
+      else J.lCrk[(size_t)q * N + g] = RK * ac[q];
+      J.lC[(size_t)q * N + g] = lc;
+    }
+    // k_source reversed
     const double dphi = d.dphi[g];
-    const double r = .5 * (A.rp + A.rm);
     SrcGeom sg;
     sg.r = r;
-    sg.dt = fac * S.dt;
+    sg.dt = dt;
     sg.dV = dphi * .5 * A.dv_diff * P.dz;
     sincos(d.tiphw[g] - .5 * dphi, &sg.sinp, &sg.cosp);
     sg.xpos = r * sg.cosp;
@@ -314,7 +405,6 @@ __global__ void __launch_bounds__(BLK) a_source(DevPtrs d, AdjPtrs J, int subste
     sg.rdrOm = frame_rdrom(P, A.rdrom, r, a_sep);
     sg.Fc = w_a * w_a / r;
     sg.dtOm = frame_dtom(P, A.dtom, r, a_sep);
-    const TanPtrs none = {};
     GravT<double> G;
     grav_t(G, S, P, none, A.inst);
     double pm[5];
@@ -326,11 +416,11 @@ __global__ void __launch_bounds__(BLK) a_source(DevPtrs d, AdjPtrs J, int subste
       gpu = ld(d.gradp, D_URR, N, g);
     }
     double as[6];
-    as[0] = as[1] = ld(J.lU, D_SRR, N, g);
-    as[2] = ld(J.lU, D_LLL, N, g);
-    as[3] = ld(J.lU, D_SZZ, N, g);
-    as[4] = ld(J.lU, D_TAU, N, g);
-    as[5] = P.has_visc ? as[4] : 0.0;
+    as[0] = as[1] = ac[D_SRR];
+    as[2] = ac[D_LLL];
+    as[3] = ac[D_SZZ];
+    as[4] = ac[D_TAU];
+    as[5] = P.has_visc ? ac[D_TAU] : 0.0;
     double apm[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, agu = 0.0, agpu = 0.0;
     GravAdj ag;
     grav_adj_zero(ag);
@@ -355,7 +445,7 @@ __device__ __forceinline__ void store15(double *arr, int n, int i, const double 
   }
 }
 
-__global__ void __launch_bounds__(BLK) a_flux_phi(DevPtrs d, AdjPtrs J, int substep, int row0) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_flux_phi(DevPtrs d, AdjPtrs J, int substep, int row0) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -431,7 +521,7 @@ __global__ void __launch_bounds__(BLK) a_flux_phi(DevPtrs d, AdjPtrs J, int subs
   block_partial<5>(v, J.part + DGPU_AP_N * (size_t)(row0 + blockIdx.x));
 }
 
-__global__ void __launch_bounds__(BLK) a_flux_r(DevPtrs d, AdjPtrs J, int substep, int row0) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_flux_r(DevPtrs d, AdjPtrs J, int substep, int row0) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells, NS = d.n_slots;
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -682,11 +772,44 @@ __global__ void __launch_bounds__(BLK) a_calc_cons(DevPtrs d, AdjPtrs J) {
 
 extern "C" {
 
-int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, void *stream) {
+int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, const int *idx,
+                  void *stream) {
   const int nb = (d->n_cells + BLK - 1) / BLK;
   static const TanPtrs none = {};
-  if (t) k_objective<Dual><<<nb, BLK, 0, (cudaStream_t)stream>>>(*d, *t, part, out, out_d);
-  else k_objective<double><<<nb, BLK, 0, (cudaStream_t)stream>>>(*d, none, part, out, out_d);
+  if (t) k_objective<Dual><<<nb, BLK, 0, (cudaStream_t)stream>>>(*d, *t, part, out, out_d, idx);
+  else k_objective<double><<<nb, BLK, 0, (cudaStream_t)stream>>>(*d, none, part, out, out_d, idx);
+  return (int)cudaGetLastError();
+}
+
+int dgk_step_end(const DevPtrs *d, double *dtlog, int *idx, void *stream) {
+  k_step_end<<<1, 32, 0, (cudaStream_t)stream>>>(*d, dtlog, idx);
+  return (int)cudaGetLastError();
+}
+int dgk_set_dt(const DevPtrs *d, const double *dtin, const int *idx, void *stream) {
+  k_set_dt<<<1, 32, 0, (cudaStream_t)stream>>>(*d, dtin, idx);
+  return (int)cudaGetLastError();
+}
+int dgk_set_int(int *p, int v, void *stream) {
+  k_set_int<<<1, 32, 0, (cudaStream_t)stream>>>(p, v);
+  return (int)cudaGetLastError();
+}
+int dgk_add_int(int *p, int dv, void *stream) {
+  k_add_int<<<1, 32, 0, (cudaStream_t)stream>>>(p, dv);
+  return (int)cudaGetLastError();
+}
+
+static int snap_grid(const DevPtrs *d) {
+  long long n = 19LL * d->n_cells;
+  long long b = (n + BLK - 1) / BLK;
+  return (int)(b < 148 * 8 ? b : 148 * 8);
+}
+int dgk_snap(const DevPtrs *d, double *buf, InstState *ist, int save, void *stream) {
+  k_snap_ptr<<<snap_grid(d), BLK, 0, (cudaStream_t)stream>>>(*d, buf, ist, save);
+  return (int)cudaGetLastError();
+}
+int dgk_snap_tab(const DevPtrs *d, double *const *bufs, InstState *const *ists, const int *idx, int off, int save,
+                 void *stream) {
+  k_snap_tab<<<snap_grid(d), BLK, 0, (cudaStream_t)stream>>>(*d, bufs, ists, idx, off, save);
   return (int)cudaGetLastError();
 }
 
@@ -695,22 +818,29 @@ int dgk_adj_rows(const DevPtrs *d) {
   return 3 * nbC + nbS;
 }
 
-int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double wT, double wM, void *stream) {
+int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double *const *bufs, InstState *const *ists,
+                      const int *idx, int off, const double *wts, const int *base, void *stream) {
   const int nbC = (d->n_cells + BLK - 1) / BLK, nbS = (d->n_slots + BLK - 1) / BLK;
   const int row0 = 2 * nbC + nbS;
-  a_objective<<<nbC, BLK, 0, (cudaStream_t)stream>>>(*d, *J, wT, wM, row0);
-  a_par_reduce<<<1, 32, 0, (cudaStream_t)stream>>>(*J, row0, nbC);
+  a_objective<<<nbC, BLK, 0, (cudaStream_t)stream>>>(*d, *J, bufs, ists, idx, off, wts, base, row0);
+  a_par_reduce<<<1, BLK, 0, (cudaStream_t)stream>>>(*J, row0, nbC);
   return (int)cudaGetLastError();
 }
 
-int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream) {
-  cudaStream_t s = (cudaStream_t)stream;
+int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream, void *side, void *ev_fork,
+                    void *ev_join) {
+  cudaStream_t s = (cudaStream_t)stream, s2 = (cudaStream_t)side;
   const int nbC = (d->n_cells + BLK - 1) / BLK, nbS = (d->n_slots + BLK - 1) / BLK;
-  a_update<<<nbC, BLK, 0, s>>>(*d, *J, substep);
-  a_source<<<nbC, BLK, 0, s>>>(*d, *J, substep, 0);
-  a_flux_phi<<<nbC, BLK, 0, s>>>(*d, *J, substep, nbC);
+  cudaError_t e;
+  a_update_source<<<nbC, BLK, 0, s>>>(*d, *J, substep, 0);
+  /* the phi faces beside the r faces */
+  if ((e = cudaEventRecord((cudaEvent_t)ev_fork, s)) != cudaSuccess) return (int)e;
+  if ((e = cudaStreamWaitEvent(s2, (cudaEvent_t)ev_fork, 0)) != cudaSuccess) return (int)e;
+  a_flux_phi<<<nbC, BLK, 0, s2>>>(*d, *J, substep, nbC);
   if (nbS > 0) a_flux_r<<<nbS, BLK, 0, s>>>(*d, *J, substep, 2 * nbC);
-  a_par_reduce<<<1, 32, 0, s>>>(*J, 0, 2 * nbC + nbS);
+  if ((e = cudaEventRecord((cudaEvent_t)ev_join, s2)) != cudaSuccess) return (int)e;
+  if ((e = cudaStreamWaitEvent(s, (cudaEvent_t)ev_join, 0)) != cudaSuccess) return (int)e;
+  a_par_reduce<<<1, BLK, 0, s>>>(*J, 0, 2 * nbC + nbS);
   a_gather_plm<<<nbC, BLK, 0, s>>>(*d, *J);
   a_rslope<<<nbC, BLK, 0, s>>>(*d, *J);
   a_cellprep<<<nbC, BLK, 0, s>>>(*d, *J);

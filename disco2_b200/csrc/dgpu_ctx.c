@@ -610,18 +610,28 @@ int dgpu_init_state(dgpu_ctx *c, int inst) {
 }
 
 int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int full) {
+  /* the layout of the step graph: merge beside cellprep, source and the phi
+   * faces beside the r faces */
+  CK(cudaEventRecord(c->fork[0], c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
+  CKK(dgk_merge(&c->d, sub, c->side));
   CKK(dgk_cellprep(&c->d, t, sub, c->stream));
-  CKK(dgk_merge(&c->d, sub, c->stream));
+  CK(cudaEventRecord(c->fork[1], c->side));
+  CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
   CKK(dgk_rslope(&c->d, t, c->stream));
   CKK(dgk_plm_r(&c->d, t, sub, c->stream));
-  CKK(dgk_source(&c->d, t, sub, c->stream));
-  CKK(dgk_flux_phi(&c->d, t, sub, c->stream));
+  CK(cudaEventRecord(c->fork[2], c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
+  CKK(dgk_source(&c->d, t, sub, c->side));
+  CKK(dgk_flux_phi(&c->d, t, sub, c->side));
   CKK(dgk_flux_r(&c->d, t, sub, c->stream));
+  CK(cudaEventRecord(c->fork[3], c->side));
+  CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
   if (full) CKK(dgk_update(&c->d, t, sub, 7, c->stream));
   return DGPU_OK;
 }
 
-static int launch_step(struct dgpu_ctx *c) {
+int dctx_launch_step(struct dgpu_ctx *c) {
   int sub;
   for (sub = 1; sub <= 2; ++sub) {
     /* k_merge (per annulus pair) alongside k_cellprep (per cell) */
@@ -654,7 +664,7 @@ int dgpu_step_rk2(dgpu_ctx *c, int nsteps) {
     cudaGraph_t g;
     int rc;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    rc = launch_step(c);
+    rc = dctx_launch_step(c);
     {
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       if (rc) return rc;

@@ -45,6 +45,9 @@ int dctx_read_err(struct dgpu_ctx *c);
 /* Launches the eight kernels of one substep (all but k_update when !full) on
  * the context's stream, forward (t == NULL) or tangent. */
 int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int substep, int full);
+/* Launches one RK2 step (the sequence the step graph captures) on the
+ * context's stream. */
+int dctx_launch_step(struct dgpu_ctx *c);
 /* Frees the differentiation buffers (dgpu_diff.c). */
 void dctx_diff_free(struct dgpu_ctx *c);
 

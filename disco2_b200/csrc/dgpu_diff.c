@@ -37,6 +37,8 @@ typedef struct {
   InstState *ist;
 } Snap;
 
+enum { G_OBJ, G_OBJ_DT, G_TAN, G_SEG, G_REV, G_N };
+
 struct dgpu_diff {
   /* tangent */
   TanPtrs t;
@@ -44,18 +46,36 @@ struct dgpu_diff {
   /* adjoint */
   AdjPtrs J;
   double *j_buf, *j_dq;
-  /* objective */
-  double *o_part, *o_val, *o_dot, *dtlog, *dtin;
+  /* objective and dt logs, indexed on the device by *d_idx */
+  double *o_part, *o_val, *o_dot, *dtlog, *dtin, *wts;
   int o_cap;
-  /* stored states */
+  int *d_idx, *d_base;
+  /* stored states: checkpoints, then the segment's K+1 step starts and K
+   * mid-steps (their device pointer tables tab_buf / tab_ist), then the end */
   Snap *snaps;
   int n_snaps;
+  double **tab_buf;
+  InstState **tab_ist;
+  int tab_K, tab_base;
+  /* step graphs (G_*), valid for tab_K */
+  cudaGraphExec_t g[G_N];
+  int have[G_N];
 };
+
+static void drop_graphs(struct dgpu_diff *D) {
+  int k;
+  for (k = 0; k < G_N; ++k)
+    if (D->have[k]) {
+      cudaGraphExecDestroy(D->g[k]);
+      D->have[k] = 0;
+    }
+}
 
 void dctx_diff_free(struct dgpu_ctx *c) {
   struct dgpu_diff *D = c->diff;
   int k;
   if (!D) return;
+  drop_graphs(D);
   cudaFree(D->t_buf);
   cudaFree(D->t_seed);
   cudaFree(D->j_buf);
@@ -65,6 +85,11 @@ void dctx_diff_free(struct dgpu_ctx *c) {
   cudaFree(D->o_dot);
   cudaFree(D->dtlog);
   cudaFree(D->dtin);
+  cudaFree(D->wts);
+  cudaFree(D->d_idx);
+  cudaFree(D->d_base);
+  cudaFree(D->tab_buf);
+  cudaFree(D->tab_ist);
   for (k = 0; k < D->n_snaps; ++k) {
     cudaFree(D->snaps[k].buf);
     cudaFree(D->snaps[k].ist);
@@ -96,17 +121,25 @@ static int diff_check(struct dgpu_ctx *c) {
 }
 
 static int ensure_obj(struct dgpu_ctx *c, struct dgpu_diff *D, int nsteps) {
+  if (!D->d_idx) {
+    CK(cudaMalloc((void **)&D->d_idx, sizeof(int)));
+    CK(cudaMalloc((void **)&D->d_base, sizeof(int)));
+  }
   if (D->o_cap < nsteps) {
+    /* the log buffers move: graphs that write them are rebuilt */
+    drop_graphs(D);
     cudaFree(D->o_val);
     cudaFree(D->o_dot);
     cudaFree(D->dtlog);
     cudaFree(D->dtin);
-    D->o_val = D->o_dot = D->dtlog = D->dtin = NULL;
+    cudaFree(D->wts);
+    D->o_val = D->o_dot = D->dtlog = D->dtin = D->wts = NULL;
     D->o_cap = 0;
     CK(cudaMalloc((void **)&D->dtin, sizeof(double) * (size_t)nsteps));
     CK(cudaMalloc((void **)&D->o_val, sizeof(double) * 2 * (size_t)nsteps));
     CK(cudaMalloc((void **)&D->o_dot, sizeof(double) * 2 * (size_t)nsteps));
     CK(cudaMalloc((void **)&D->dtlog, sizeof(double) * (size_t)nsteps));
+    CK(cudaMalloc((void **)&D->wts, sizeof(double) * 2 * (size_t)nsteps));
     D->o_cap = nsteps;
   }
   if (!D->o_part) CK(cudaMalloc((void **)&D->o_part, sizeof(double) * 4 * ((size_t)c->n_cells / 256 + 2)));
@@ -162,42 +195,62 @@ static int ensure_adj(struct dgpu_ctx *c, struct dgpu_diff *D) {
   return DGPU_OK;
 }
 
-static int ensure_snaps(struct dgpu_ctx *c, struct dgpu_diff *D, int count) {
+/* nck checkpoints, then the segment's K+1 step starts and K mid-steps (with
+ * their device pointer tables), then the run's end: nck + 2K + 2 stored states */
+static int ensure_snaps(struct dgpu_ctx *c, struct dgpu_diff *D, int nck, int K) {
+  const int count = nck + 2 * K + 2;
   int k;
-  if (D->n_snaps >= count) return DGPU_OK;
-  {
+  if (D->n_snaps < count) {
     Snap *s = (Snap *)realloc(D->snaps, sizeof(Snap) * (size_t)count);
     if (!s) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
     D->snaps = s;
-  }
-  for (k = D->n_snaps; k < count; ++k) {
-    D->snaps[k].buf = NULL;
-    D->snaps[k].ist = NULL;
-    if (cudaMalloc((void **)&D->snaps[k].buf, sizeof(double) * 19 * (size_t)c->n_cells) != cudaSuccess ||
-        cudaMalloc((void **)&D->snaps[k].ist, sizeof(InstState) * (size_t)c->n_inst) != cudaSuccess) {
-      cudaFree(D->snaps[k].buf);
-      D->n_snaps = k;
-      cudaGetLastError();
-      return fail(c, DGPU_ERR_NOMEM, "device allocation of %d stored states failed", count);
+    for (k = D->n_snaps; k < count; ++k) {
+      D->snaps[k].buf = NULL;
+      D->snaps[k].ist = NULL;
+      if (cudaMalloc((void **)&D->snaps[k].buf, sizeof(double) * 19 * (size_t)c->n_cells) != cudaSuccess ||
+          cudaMalloc((void **)&D->snaps[k].ist, sizeof(InstState) * (size_t)c->n_inst) != cudaSuccess) {
+        cudaFree(D->snaps[k].buf);
+        D->n_snaps = k;
+        cudaGetLastError();
+        return fail(c, DGPU_ERR_NOMEM, "device allocation of %d stored states failed", count);
+      }
     }
+    D->n_snaps = count;
+    D->tab_K = 0;
   }
-  D->n_snaps = count;
-  return DGPU_OK;
-}
-
-static int snap_copy(struct dgpu_ctx *c, const Snap *s, int save) {
-  size_t N = (size_t)c->n_cells, b = sizeof(double) * N;
-  double *arr[7] = {c->d.prim, c->d.cons, c->d.rkcons, c->d.tiph0, c->d.tiph1, c->d.rktiph, c->d.dphi};
-  size_t off[7] = {0, 5 * N, 10 * N, 15 * N, 16 * N, 17 * N, 18 * N};
-  size_t len[7] = {5 * b, 5 * b, 5 * b, b, b, b, b};
-  int k;
-  enum cudaMemcpyKind kind = cudaMemcpyDeviceToDevice;
-  for (k = 0; k < 7; ++k) {
-    if (save) CK(cudaMemcpyAsync(s->buf + off[k], arr[k], len[k], kind, c->stream));
-    else CK(cudaMemcpyAsync(arr[k], s->buf + off[k], len[k], kind, c->stream));
+  if (D->tab_K != K || D->tab_base != nck) {
+    /* tables of the segment's states: S[0..K] then M[0..K-1] */
+    double **hb = (double **)malloc(sizeof(double *) * (size_t)(2 * K + 1));
+    InstState **hi = (InstState **)malloc(sizeof(InstState *) * (size_t)(2 * K + 1));
+    const int base = nck;
+    if (!hb || !hi) {
+      free(hb);
+      free(hi);
+      return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+    }
+    for (k = 0; k < 2 * K + 1; ++k) {
+      hb[k] = D->snaps[base + k].buf;
+      hi[k] = D->snaps[base + k].ist;
+    }
+    drop_graphs(D);
+    cudaFree(D->tab_buf);
+    cudaFree(D->tab_ist);
+    D->tab_buf = NULL;
+    D->tab_ist = NULL;
+    if (cudaMalloc((void **)&D->tab_buf, sizeof(double *) * (size_t)(2 * K + 1)) != cudaSuccess ||
+        cudaMalloc((void **)&D->tab_ist, sizeof(InstState *) * (size_t)(2 * K + 1)) != cudaSuccess ||
+        cudaMemcpy(D->tab_buf, hb, sizeof(double *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(D->tab_ist, hi, sizeof(InstState *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+      free(hb);
+      free(hi);
+      return fail(c, DGPU_ERR_CUDA, "stored-state tables failed");
+    }
+    free(hb);
+    free(hi);
+    D->tab_K = K;
+    D->tab_base = nck;
   }
-  if (save) CK(cudaMemcpyAsync(s->ist, c->d_ist, sizeof(InstState) * (size_t)c->n_inst, kind, c->stream));
-  else CK(cudaMemcpyAsync(c->d_ist, s->ist, sizeof(InstState) * (size_t)c->n_inst, kind, c->stream));
   return DGPU_OK;
 }
 
@@ -222,8 +275,69 @@ static int dq_consts(struct dgpu_ctx *c, double *dq) {
   return DGPU_OK;
 }
 
-static int step_log(struct dgpu_ctx *c, struct dgpu_diff *D, int n) {
-  CK(cudaMemcpyAsync(D->dtlog + n, &c->d_ist[0].dt, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+/* ---- step graphs -------------------------------------------------------- */
+static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
+  struct dgpu_diff *Dd = D;
+  const int nbK = D->tab_K;
+  double *const *tabS = (double *const *)D->tab_buf;
+  InstState *const *istS = (InstState *const *)D->tab_ist;
+  double *const *tabM = (double *const *)(D->tab_buf + nbK + 1);
+  InstState *const *istM = (InstState *const *)(D->tab_ist + nbK + 1);
+  switch (which) {
+    case G_OBJ: /* one step, its objective and dt into slot *idx, ++*idx */
+      if (dctx_launch_step(c)) return -1;
+      if (dgk_objective(&c->d, NULL, Dd->o_part, Dd->o_val, NULL, Dd->d_idx, c->stream)) return -1;
+      return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
+    case G_OBJ_DT: /* the same with dt = dtin[*idx] */
+      if (dgk_cellprep(&c->d, NULL, 1, c->stream) || dgk_merge(&c->d, 1, c->stream) ||
+          dgk_rslope(&c->d, NULL, c->stream) || dgk_plm_r(&c->d, NULL, 1, c->stream) ||
+          dgk_set_dt(&c->d, Dd->dtin, Dd->d_idx, c->stream) || dgk_source(&c->d, NULL, 1, c->stream) ||
+          dgk_flux_phi(&c->d, NULL, 1, c->stream) || dgk_flux_r(&c->d, NULL, 1, c->stream) ||
+          dgk_update(&c->d, NULL, 1, 7, c->stream) || dctx_substep(c, NULL, 2, 1))
+        return -1;
+      if (dgk_objective(&c->d, NULL, Dd->o_part, Dd->o_val, NULL, Dd->d_idx, c->stream)) return -1;
+      return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
+    case G_TAN: /* one tangent step */
+      if (dctx_substep(c, &Dd->t, 1, 1) || dctx_substep(c, &Dd->t, 2, 1)) return -1;
+      if (dgk_objective(&c->d, &Dd->t, Dd->o_part, Dd->o_val, Dd->o_dot, Dd->d_idx, c->stream)) return -1;
+      return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
+    case G_SEG: /* replay one step of a segment, storing its substep inputs in slot *idx */
+      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 1, c->stream) || dctx_substep(c, NULL, 1, 1) ||
+          dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 1, c->stream) || dctx_substep(c, NULL, 2, 1))
+        return -1;
+      return dgk_add_int(Dd->d_idx, 1, c->stream);
+    case G_REV: /* reverse step *idx of the segment (step n = *base + *idx) */
+      if (dgk_adj_objective(&c->d, &Dd->J, tabS, istS, Dd->d_idx, 1, Dd->wts, Dd->d_base, c->stream)) return -1;
+      if (dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 0, c->stream) || dctx_substep(c, NULL, 2, 0) ||
+          dgk_adj_substep(&c->d, &Dd->J, 2, c->stream, c->side, c->fork[0], c->fork[1]))
+        return -1;
+      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 0, c->stream) || dctx_substep(c, NULL, 1, 0) ||
+          dgk_adj_substep(&c->d, &Dd->J, 1, c->stream, c->side, c->fork[0], c->fork[1]))
+        return -1;
+      return dgk_add_int(Dd->d_idx, -1, c->stream);
+  }
+  return -1;
+}
+
+static int launch_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
+  if (!D->have[which]) {
+    cudaGraph_t g;
+    int rc;
+    cudaError_t e;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = record_graph(c, D, which);
+    e = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return fail(c, DGPU_ERR_CUDA, "differentiation step capture failed (%d)", which);
+    }
+    if (e != cudaSuccess) return fail(c, DGPU_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&D->g[which], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(c, DGPU_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    D->have[which] = 1;
+  }
+  CK(cudaGraphLaunch(D->g[which], c->stream));
   return DGPU_OK;
 }
 
@@ -265,22 +379,6 @@ static int run_args(struct dgpu_ctx *c, int nsteps, int w0) {
   return diff_check(c);
 }
 
-/* One step with dt = dt_dev[0] in place of the CFL value (timestep_set_dt,
- * src/TimeStep/timestep_set.c:16-21): the kernels of substep 1 up to the CFL
- * minimum, then the given dt, then the rest. */
-static int step_frozen_dt(struct dgpu_ctx *c, const double *dt_dev) {
-  CKK(dgk_cellprep(&c->d, NULL, 1, c->stream));
-  CKK(dgk_merge(&c->d, 1, c->stream));
-  CKK(dgk_rslope(&c->d, NULL, c->stream));
-  CKK(dgk_plm_r(&c->d, NULL, 1, c->stream));
-  CK(cudaMemcpyAsync(&c->d_ist[0].dt, dt_dev, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  CKK(dgk_source(&c->d, NULL, 1, c->stream));
-  CKK(dgk_flux_phi(&c->d, NULL, 1, c->stream));
-  CKK(dgk_flux_r(&c->d, NULL, 1, c->stream));
-  CKK(dgk_update(&c->d, NULL, 1, 7, c->stream));
-  return dctx_substep(c, NULL, 2, 1);
-}
-
 int dgpu_objective(dgpu_ctx *c, int nsteps, int window_start, const double *dt_in, double *dt_out, double *J) {
   struct dgpu_diff *D = NULL;
   int n, rc = run_args(c, nsteps, window_start);
@@ -288,11 +386,9 @@ int dgpu_objective(dgpu_ctx *c, int nsteps, int window_start, const double *dt_i
   if (!J) return fail(c, DGPU_ERR_ARG, "null J");
   if ((rc = diff_get(c, &D)) || (rc = ensure_obj(c, D, nsteps))) return rc;
   if (dt_in) CK(cudaMemcpyAsync(D->dtin, dt_in, sizeof(double) * (size_t)nsteps, cudaMemcpyHostToDevice, c->stream));
-  for (n = 0; n < nsteps; ++n) {
-    rc = dt_in ? step_frozen_dt(c, D->dtin + n) : dgpu_step_rk2(c, 1);
-    if (rc || (rc = step_log(c, D, n))) return rc;
-    if (n >= window_start) CKK(dgk_objective(&c->d, NULL, D->o_part, D->o_val + 2 * n, NULL, c->stream));
-  }
+  CKK(dgk_set_int(D->d_idx, 0, c->stream));
+  for (n = 0; n < nsteps; ++n)
+    if ((rc = launch_graph(c, D, dt_in ? G_OBJ_DT : G_OBJ))) return rc;
   if ((rc = dgpu_synchronize(c))) return rc;
   if (dt_out) CK(cudaMemcpy(dt_out, D->dtlog, sizeof(double) * (size_t)nsteps, cudaMemcpyDeviceToHost));
   return window_mean(c, D, nsteps, window_start, D->o_val, J, NULL);
@@ -324,12 +420,9 @@ int dgpu_tangent(dgpu_ctx *c, int nsteps, int window_start, double dq_dir, doubl
     CKK(dgk_aos_to_soa(D->t.prim, 5, c->n_cells, 0, c->d_stage, c->n_cells, c->stream));
   }
   CKK(dgk_calc_cons(&c->d, &D->t, c->stream));
-  for (n = 0; n < nsteps; ++n) {
-    if ((rc = dctx_substep(c, &D->t, 1, 1)) || (rc = dctx_substep(c, &D->t, 2, 1))) return rc;
-    if ((rc = step_log(c, D, n))) return rc;
-    if (n >= window_start)
-      CKK(dgk_objective(&c->d, &D->t, D->o_part, D->o_val + 2 * n, D->o_dot + 2 * n, c->stream));
-  }
+  CKK(dgk_set_int(D->d_idx, 0, c->stream));
+  for (n = 0; n < nsteps; ++n)
+    if ((rc = launch_graph(c, D, G_TAN))) return rc;
   if ((rc = dgpu_synchronize(c))) return rc;
   if ((rc = window_mean(c, D, nsteps, window_start, D->o_val, J, NULL))) return rc;
   return window_mean(c, D, nsteps, window_start, D->o_dot, dJ, NULL);
@@ -340,9 +433,9 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   struct dgpu_diff *D = NULL;
   int n, seg, nck, K = ckpt_every, rc = run_args(c, nsteps, window_start);
   double dq[4], W, wts[2], acc[2];
-  double *dt = NULL;
+  double *w = NULL;
   size_t N;
-  Snap *ck, *sS, *sM, *fin;
+  Snap *ck, *fin;
   if (rc) return rc;
   if (K < 1) return fail(c, DGPU_ERR_ARG, "ckpt_every must be >= 1");
   if (!J) return fail(c, DGPU_ERR_ARG, "null J");
@@ -352,70 +445,59 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   wts[0] = weights ? weights[0] : 1.0;
   wts[1] = weights ? weights[1] : 0.0;
   if ((rc = diff_get(c, &D)) || (rc = ensure_obj(c, D, nsteps)) || (rc = ensure_adj(c, D)) ||
-      (rc = ensure_snaps(c, D, nck + 2 * K + 2)))
+      (rc = ensure_snaps(c, D, nck, K)))
     return rc;
   ck = D->snaps;
-  sS = ck + nck;     /* K + 1: state before substep 1 of each step of a segment, and the segment's end */
-  sM = sS + K + 1;   /* K: state before substep 2 */
-  fin = sM + K;
+  fin = D->snaps + nck + 2 * K + 1;
   if ((rc = dq_consts(c, dq))) return rc;
   CK(cudaMemcpyAsync(D->j_dq, dq, sizeof(dq), cudaMemcpyHostToDevice, c->stream));
 
   /* forward sweep: checkpoints, dt schedule, objective */
+  CKK(dgk_set_int(D->d_idx, 0, c->stream));
   for (n = 0; n < nsteps; ++n) {
-    if (n % K == 0 && (rc = snap_copy(c, &ck[n / K], 1))) return rc;
-    if ((rc = dgpu_step_rk2(c, 1)) || (rc = step_log(c, D, n))) return rc;
-    if (n >= window_start) CKK(dgk_objective(&c->d, NULL, D->o_part, D->o_val + 2 * n, NULL, c->stream));
+    if (n % K == 0) CKK(dgk_snap(&c->d, ck[n / K].buf, ck[n / K].ist, 1, c->stream));
+    if ((rc = launch_graph(c, D, G_OBJ))) return rc;
   }
-  if ((rc = snap_copy(c, fin, 1))) return rc;
+  CKK(dgk_snap(&c->d, fin->buf, fin->ist, 1, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
   if ((rc = window_mean(c, D, nsteps, window_start, D->o_val, J, &W))) return rc;
-  dt = (double *)malloc(sizeof(double) * (size_t)nsteps);
-  if (!dt) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
-  if (cudaMemcpy(dt, D->dtlog, sizeof(double) * (size_t)nsteps, cudaMemcpyDeviceToHost) != cudaSuccess) {
-    free(dt);
+
+  /* objective weights of each step: w_k dt_n / sum dt over the window */
+  w = (double *)malloc(sizeof(double) * 3 * (size_t)nsteps);
+  if (!w) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+  if (cudaMemcpy(w + 2 * nsteps, D->dtlog, sizeof(double) * (size_t)nsteps, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    free(w);
     return fail(c, DGPU_ERR_CUDA, "dt download failed");
   }
-
-  /* reverse sweep */
-  rc = DGPU_OK;
-  if (cudaMemsetAsync(D->J.lW, 0, sizeof(double) * 15 * N, c->stream) != cudaSuccess ||
-      cudaMemsetAsync(D->J.acc, 0, sizeof(double) * 8, c->stream) != cudaSuccess)
-    rc = fail(c, DGPU_ERR_CUDA, "adjoint reset failed");
-  for (seg = nck - 1; seg >= 0 && rc == DGPU_OK; --seg) {
-    int n0 = seg * K, n1 = n0 + K < nsteps ? n0 + K : nsteps;
-    if ((rc = snap_copy(c, &ck[seg], 0))) break;
-    for (n = n0; n < n1 && rc == DGPU_OK; ++n) {
-      if (!(rc = snap_copy(c, &sS[n - n0], 1)) && !(rc = dctx_substep(c, NULL, 1, 1)) &&
-          !(rc = snap_copy(c, &sM[n - n0], 1)))
-        rc = dctx_substep(c, NULL, 2, 1);
-    }
-    if (rc || (rc = snap_copy(c, &sS[n1 - n0], 1))) break;
-    for (n = n1 - 1; n >= n0 && rc == DGPU_OK; --n) {
-      if (n >= window_start) {
-        double w = dt[n] / W;
-        if ((rc = snap_copy(c, &sS[n - n0 + 1], 0))) break;
-        if (dgk_adj_objective(&c->d, &D->J, wts[0] * w, wts[1] * w, c->stream)) {
-          rc = fail(c, DGPU_ERR_CUDA, "objective adjoint launch failed");
-          break;
-        }
-      }
-      if ((rc = snap_copy(c, &sM[n - n0], 0)) || (rc = dctx_substep(c, NULL, 2, 0))) break;
-      if (dgk_adj_substep(&c->d, &D->J, 2, c->stream)) {
-        rc = fail(c, DGPU_ERR_CUDA, "adjoint launch failed");
-        break;
-      }
-      if ((rc = snap_copy(c, &sS[n - n0], 0)) || (rc = dctx_substep(c, NULL, 1, 0))) break;
-      if (dgk_adj_substep(&c->d, &D->J, 1, c->stream)) {
-        rc = fail(c, DGPU_ERR_CUDA, "adjoint launch failed");
-        break;
-      }
-    }
+  for (n = 0; n < nsteps; ++n) {
+    double f = n >= window_start ? w[2 * nsteps + n] / W : 0.0;
+    w[2 * n] = wts[0] * f;
+    w[2 * n + 1] = wts[1] * f;
   }
-  free(dt);
+  rc = cudaMemcpy(D->wts, w, sizeof(double) * 2 * (size_t)nsteps, cudaMemcpyHostToDevice) != cudaSuccess
+           ? fail(c, DGPU_ERR_CUDA, "weight upload failed")
+           : DGPU_OK;
+  free(w);
   if (rc) return rc;
+
+  /* reverse sweep, segment by segment */
+  CK(cudaMemsetAsync(D->J.lW, 0, sizeof(double) * 15 * N, c->stream));
+  CK(cudaMemsetAsync(D->J.acc, 0, sizeof(double) * 8, c->stream));
+  for (seg = nck - 1; seg >= 0; --seg) {
+    int n0 = seg * K, n1 = n0 + K < nsteps ? n0 + K : nsteps;
+    CKK(dgk_snap(&c->d, ck[seg].buf, ck[seg].ist, 0, c->stream));
+    CKK(dgk_set_int(D->d_idx, 0, c->stream));
+    for (n = n0; n < n1; ++n)
+      if ((rc = launch_graph(c, D, G_SEG))) return rc;
+    /* the segment's end state in slot n1 - n0 */
+    CKK(dgk_snap_tab(&c->d, (double *const *)D->tab_buf, (InstState *const *)D->tab_ist, D->d_idx, 0, 1, c->stream));
+    CKK(dgk_add_int(D->d_idx, -1, c->stream));
+    CKK(dgk_set_int(D->d_base, n0, c->stream));
+    for (n = n1 - 1; n >= n0; --n)
+      if ((rc = launch_graph(c, D, G_REV))) return rc;
+  }
   /* the initial cons are cell_calc_cons of the initial prims */
-  if ((rc = snap_copy(c, &ck[0], 0))) return rc;
+  CKK(dgk_snap(&c->d, ck[0].buf, ck[0].ist, 0, c->stream));
   CKK(dgk_adj_calc_cons(&c->d, &D->J, c->stream));
   if (dJ_dprim) {
     CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, 0, D->J.lW, c->n_cells, c->stream));
@@ -423,7 +505,7 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   }
   CK(cudaMemcpyAsync(acc, D->J.acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
   /* leave the context at the end of the run, like the forward */
-  if ((rc = snap_copy(c, fin, 0))) return rc;
+  CKK(dgk_snap(&c->d, fin->buf, fin->ist, 0, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
   if (dJ_dq) *dJ_dq = acc[0];
   if (dJ_dalpha) *dJ_dalpha = acc[1];

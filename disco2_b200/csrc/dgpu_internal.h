@@ -199,10 +199,20 @@ int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream);
 /* differentiation (dgpu_adjoint.cu) */
-int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, void *stream);
+int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, const int *idx,
+                  void *stream);
+int dgk_step_end(const DevPtrs *d, double *dtlog, int *idx, void *stream);
+int dgk_set_dt(const DevPtrs *d, const double *dtin, const int *idx, void *stream);
+int dgk_set_int(int *p, int v, void *stream);
+int dgk_add_int(int *p, int dv, void *stream);
+int dgk_snap(const DevPtrs *d, double *buf, InstState *ist, int save, void *stream);
+int dgk_snap_tab(const DevPtrs *d, double *const *bufs, InstState *const *ists, const int *idx, int off, int save,
+                 void *stream);
 int dgk_adj_rows(const DevPtrs *d);
-int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double wT, double wM, void *stream);
-int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream);
+int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double *const *bufs, InstState *const *ists,
+                      const int *idx, int off, const double *wts, const int *base, void *stream);
+int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream, void *side, void *ev_fork,
+                    void *ev_join);
 int dgk_adj_calc_cons(const DevPtrs *d, const AdjPtrs *J, void *stream);
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
 int dgk_update_blocks(int n_cells);
