@@ -321,7 +321,8 @@ __global__ void __launch_bounds__(BLK) a_par_reduce(AdjPtrs J, int row0, int nro
 // k_update reversed, then k_source reversed on the same cell (it reads only
 // the cell's own lU): lU, the substep's input lC / lCrk, and the source part
 // of lWt, lG[UPP], lGp[URR]; binary adjoints to part rows [row0, ...).
-__global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_update_source(DevPtrs d, AdjPtrs J, int substep, int row0) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_update_source(DevPtrs d, AdjPtrs J, int substep, int row0,
+                                                                     const double *rec, const int *idx) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -336,10 +337,13 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_ADJ) a_update_source(DevPtrs d,
     const double r = .5 * (A.rm + A.rp);
     double ac[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     {
+      // the conserved sum before cons2prim and the new width, recorded by the
+      // segment replay's k_update
+      const double *rs = rec + (size_t)(2 * (*idx) + substep - 1) * 6 * N;
       double c[5];
-      update_sum<double>(d, none, A, a, g, substep, 7, dt, false, c);
-      double tn, rk;
-      const double dphi_n = mesh_advance(d, A, a, g, substep, dt, tn, rk);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) c[q] = rs[(size_t)q * N + g];
+      const double dphi_n = rs[(size_t)5 * N + g];
       const double dV = A.dv_half * dphi_n * P.dz;
       double pr[5];
       cons2prim(c, dV, r, P, pr);
@@ -827,12 +831,12 @@ int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double *const *bufs, I
   return (int)cudaGetLastError();
 }
 
-int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream, void *side, void *ev_fork,
-                    void *ev_join) {
+int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, const double *rec, const int *idx,
+                    void *stream, void *side, void *ev_fork, void *ev_join) {
   cudaStream_t s = (cudaStream_t)stream, s2 = (cudaStream_t)side;
   const int nbC = (d->n_cells + BLK - 1) / BLK, nbS = (d->n_slots + BLK - 1) / BLK;
   cudaError_t e;
-  a_update_source<<<nbC, BLK, 0, s>>>(*d, *J, substep, 0);
+  a_update_source<<<nbC, BLK, 0, s>>>(*d, *J, substep, 0, rec, idx);
   /* the phi faces beside the r faces */
   if ((e = cudaEventRecord((cudaEvent_t)ev_fork, s)) != cudaSuccess) return (int)e;
   if ((e = cudaStreamWaitEvent(s2, (cudaEvent_t)ev_fork, 0)) != cudaSuccess) return (int)e;

@@ -350,7 +350,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
     c->d.err = (int *)dmalloc(sizeof(int), &ok);
     c->d_stage = (double *)dmalloc(sizeof(double) * 5 * (size_t)maxcells, &ok);
-    c->d_torque = (double *)dmalloc(sizeof(double) * ((size_t)maxcells / 256 + 8), &ok);
+    c->d_torque = (double *)dmalloc(sizeof(double) * ((size_t)maxcells / dgk_block_size() + 8), &ok);
   }
   if (!ok) {
     free(h_cell_ann);
@@ -609,7 +609,7 @@ int dgpu_init_state(dgpu_ctx *c, int inst) {
   return rc;
 }
 
-int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int full) {
+int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double *rec, const int *rec_idx) {
   /* the layout of the step graph: merge beside cellprep, source and the phi
    * faces beside the r faces */
   CK(cudaEventRecord(c->fork[0], c->stream));
@@ -620,6 +620,10 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int full) {
   CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
   CKK(dgk_rslope(&c->d, t, c->stream));
   CKK(dgk_plm_r(&c->d, t, sub, c->stream));
+  if (mode == DCTX_ADJPREP) {
+    CKK(dgk_ann_consts(&c->d, sub, c->stream));
+    return DGPU_OK;
+  }
   CK(cudaEventRecord(c->fork[2], c->stream));
   CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
   CKK(dgk_source(&c->d, t, sub, c->side));
@@ -627,7 +631,8 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int full) {
   CKK(dgk_flux_r(&c->d, t, sub, c->stream));
   CK(cudaEventRecord(c->fork[3], c->side));
   CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
-  if (full) CKK(dgk_update(&c->d, t, sub, 7, c->stream));
+  if (mode == DCTX_REC) CKK(dgk_update_rec(&c->d, sub, rec, rec_idx, c->stream));
+  else CKK(dgk_update(&c->d, t, sub, 7, c->stream));
   return DGPU_OK;
 }
 
@@ -806,7 +811,7 @@ int dgpu_torque(dgpu_ctx *c, int inst, double *torque) {
   if (rc) return rc;
   if (!torque) return fail(c, DGPU_ERR_ARG, "null torque");
   p = &c->h_par[inst];
-  nb = (p->n_cells + 255) / 256;
+  nb = (p->n_cells + dgk_block_size() - 1) / dgk_block_size();
   CKK(dgk_torque(&c->d, inst, c->d_torque, c->d_torque + nb, p->n_cells, c->stream));
   CK(cudaMemcpyAsync(torque, c->d_torque + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   return dgpu_synchronize(c);

@@ -42,9 +42,13 @@ struct dgpu_ctx {
 int dctx_fail(struct dgpu_ctx *c, int code, const char *fmt, ...);
 /* Reads and clears the device error flags; DGPU_OK or the matching error. */
 int dctx_read_err(struct dgpu_ctx *c);
-/* Launches the eight kernels of one substep (all but k_update when !full) on
- * the context's stream, forward (t == NULL) or tangent. */
-int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int substep, int full);
+/* Launches one substep on the context's stream, forward (t == NULL) or
+ * tangent: DCTX_FULL the eight kernels; DCTX_REC the same with k_update
+ * recording into rec slot 2 * (*rec_idx) + substep - 1 (forward only);
+ * DCTX_ADJPREP only what the substep's adjoint reads (phi slopes, face list,
+ * face slopes, r slopes, annulus constants). */
+enum { DCTX_FULL, DCTX_REC, DCTX_ADJPREP };
+int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int substep, int mode, double *rec, const int *rec_idx);
 /* Launches one RK2 step (the sequence the step graph captures) on the
  * context's stream. */
 int dctx_launch_step(struct dgpu_ctx *c);

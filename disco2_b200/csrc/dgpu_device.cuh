@@ -25,7 +25,11 @@
 #include "dgpu_internal.h"
 
 #define PHIMAX (2.0 * M_PI)
-#define BLK 256
+// threads per block of every kernel
+#ifndef DGPU_BLK
+#define DGPU_BLK 256
+#endif
+#define BLK DGPU_BLK
 
 #define HD __host__ __device__ __forceinline__
 

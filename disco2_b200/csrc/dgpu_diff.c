@@ -37,7 +37,10 @@ typedef struct {
   InstState *ist;
 } Snap;
 
-enum { G_OBJ, G_OBJ_DT, G_TAN, G_SEG, G_REV, G_N };
+/* step graphs: logged forward step, the same with a frozen dt, tangent step,
+ * segment replay step into stored-state set 0 / 1 (shadow buffers, second
+ * stream), reverse step from set 0 / 1 */
+enum { G_OBJ, G_OBJ_DT, G_TAN, G_SEG0, G_SEG1, G_REV0, G_REV1, G_N };
 
 struct dgpu_diff {
   /* tangent */
@@ -49,14 +52,22 @@ struct dgpu_diff {
   /* objective and dt logs, indexed on the device by *d_idx */
   double *o_part, *o_val, *o_dot, *dtlog, *dtin, *wts;
   int o_cap;
-  int *d_idx, *d_base;
-  /* stored states: checkpoints, then the segment's K+1 step starts and K
-   * mid-steps (their device pointer tables tab_buf / tab_ist), then the end */
+  int *d_idx, *d_base, *d_idx2;
+  /* stored states: checkpoints, then two sets of a segment's K+1 step starts
+   * and K mid-steps (device pointer tables tab_buf / tab_ist per set), then
+   * the run's end.  A set is filled by the replay of one segment while the
+   * reverse sweep reads the other. */
   Snap *snaps;
   int n_snaps;
-  double **tab_buf;
-  InstState **tab_ist;
+  double **tab_buf[2];
+  InstState **tab_ist[2];
+  double *rec[2]; /* per set [2K][6][n_cells]: conserved sums and new widths of the substeps */
   int tab_K, tab_base;
+  /* the replay's own copy of the per-cell and per-face buffers (tables shared) */
+  DevPtrs sh;
+  void *sh_mem;
+  cudaStream_t s2;
+  cudaEvent_t e_rep, e_rev;
   /* step graphs (G_*), valid for tab_K */
   cudaGraphExec_t g[G_N];
   int have[G_N];
@@ -88,8 +99,16 @@ void dctx_diff_free(struct dgpu_ctx *c) {
   cudaFree(D->wts);
   cudaFree(D->d_idx);
   cudaFree(D->d_base);
-  cudaFree(D->tab_buf);
-  cudaFree(D->tab_ist);
+  for (k = 0; k < 2; ++k) {
+    cudaFree(D->tab_buf[k]);
+    cudaFree(D->tab_ist[k]);
+    cudaFree(D->rec[k]);
+  }
+  cudaFree(D->d_idx2);
+  cudaFree(D->sh_mem);
+  if (D->s2) cudaStreamDestroy(D->s2);
+  if (D->e_rep) cudaEventDestroy(D->e_rep);
+  if (D->e_rev) cudaEventDestroy(D->e_rev);
   for (k = 0; k < D->n_snaps; ++k) {
     cudaFree(D->snaps[k].buf);
     cudaFree(D->snaps[k].ist);
@@ -142,7 +161,8 @@ static int ensure_obj(struct dgpu_ctx *c, struct dgpu_diff *D, int nsteps) {
     CK(cudaMalloc((void **)&D->wts, sizeof(double) * 2 * (size_t)nsteps));
     D->o_cap = nsteps;
   }
-  if (!D->o_part) CK(cudaMalloc((void **)&D->o_part, sizeof(double) * 4 * ((size_t)c->n_cells / 256 + 2)));
+  if (!D->o_part)
+    CK(cudaMalloc((void **)&D->o_part, sizeof(double) * 4 * ((size_t)c->n_cells / dgk_block_size() + 2)));
   return DGPU_OK;
 }
 
@@ -195,15 +215,15 @@ static int ensure_adj(struct dgpu_ctx *c, struct dgpu_diff *D) {
   return DGPU_OK;
 }
 
-/* nck checkpoints, then the segment's K+1 step starts and K mid-steps (with
- * their device pointer tables), then the run's end: nck + 2K + 2 stored states */
+/* nck checkpoints, two sets of 2K+1 segment states (with their device
+ * pointer tables S[0..K], M[0..K-1]), the run's end: nck + 4K + 3 states */
 static int ensure_snaps(struct dgpu_ctx *c, struct dgpu_diff *D, int nck, int K) {
-  const int count = nck + 2 * K + 2;
-  int k;
+  const int count = nck + 4 * K + 3;
+  int k, set;
   if (D->n_snaps < count) {
-    Snap *s = (Snap *)realloc(D->snaps, sizeof(Snap) * (size_t)count);
-    if (!s) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
-    D->snaps = s;
+    Snap *sn = (Snap *)realloc(D->snaps, sizeof(Snap) * (size_t)count);
+    if (!sn) return fail(c, DGPU_ERR_NOMEM, "out of host memory");
+    D->snaps = sn;
     for (k = D->n_snaps; k < count; ++k) {
       D->snaps[k].buf = NULL;
       D->snaps[k].ist = NULL;
@@ -219,38 +239,118 @@ static int ensure_snaps(struct dgpu_ctx *c, struct dgpu_diff *D, int nck, int K)
     D->tab_K = 0;
   }
   if (D->tab_K != K || D->tab_base != nck) {
-    /* tables of the segment's states: S[0..K] then M[0..K-1] */
     double **hb = (double **)malloc(sizeof(double *) * (size_t)(2 * K + 1));
     InstState **hi = (InstState **)malloc(sizeof(InstState *) * (size_t)(2 * K + 1));
-    const int base = nck;
     if (!hb || !hi) {
       free(hb);
       free(hi);
       return fail(c, DGPU_ERR_NOMEM, "out of host memory");
     }
-    for (k = 0; k < 2 * K + 1; ++k) {
-      hb[k] = D->snaps[base + k].buf;
-      hi[k] = D->snaps[base + k].ist;
-    }
     drop_graphs(D);
-    cudaFree(D->tab_buf);
-    cudaFree(D->tab_ist);
-    D->tab_buf = NULL;
-    D->tab_ist = NULL;
-    if (cudaMalloc((void **)&D->tab_buf, sizeof(double *) * (size_t)(2 * K + 1)) != cudaSuccess ||
-        cudaMalloc((void **)&D->tab_ist, sizeof(InstState *) * (size_t)(2 * K + 1)) != cudaSuccess ||
-        cudaMemcpy(D->tab_buf, hb, sizeof(double *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(D->tab_ist, hi, sizeof(InstState *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) !=
-            cudaSuccess) {
-      free(hb);
-      free(hi);
-      return fail(c, DGPU_ERR_CUDA, "stored-state tables failed");
+    for (set = 0; set < 2; ++set) {
+      const int base = nck + set * (2 * K + 1);
+      for (k = 0; k < 2 * K + 1; ++k) {
+        hb[k] = D->snaps[base + k].buf;
+        hi[k] = D->snaps[base + k].ist;
+      }
+      cudaFree(D->tab_buf[set]);
+      cudaFree(D->tab_ist[set]);
+      cudaFree(D->rec[set]);
+      D->tab_buf[set] = NULL;
+      D->tab_ist[set] = NULL;
+      D->rec[set] = NULL;
+      if (cudaMalloc((void **)&D->rec[set], sizeof(double) * 12 * (size_t)K * (size_t)c->n_cells) != cudaSuccess ||
+          cudaMalloc((void **)&D->tab_buf[set], sizeof(double *) * (size_t)(2 * K + 1)) != cudaSuccess ||
+          cudaMalloc((void **)&D->tab_ist[set], sizeof(InstState *) * (size_t)(2 * K + 1)) != cudaSuccess ||
+          cudaMemcpy(D->tab_buf[set], hb, sizeof(double *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) !=
+              cudaSuccess ||
+          cudaMemcpy(D->tab_ist[set], hi, sizeof(InstState *) * (size_t)(2 * K + 1), cudaMemcpyHostToDevice) !=
+              cudaSuccess) {
+        free(hb);
+        free(hi);
+        cudaGetLastError();
+        D->tab_K = 0;
+        return fail(c, DGPU_ERR_NOMEM, "device allocation of the segment states failed");
+      }
     }
     free(hb);
     free(hi);
     D->tab_K = K;
     D->tab_base = nck;
   }
+  return DGPU_OK;
+}
+
+/* The replay's buffers: every per-cell, per-face and per-annulus array the
+ * step writes, and its own disk state and counters; the read-only tables and
+ * the error flags are shared with the context. */
+static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
+  const size_t N = (size_t)c->n_cells, S = (size_t)(c->n_slots ? c->n_slots : 1), A = (size_t)c->n_ann;
+  const size_t R = (size_t)(c->n_runs ? c->n_runs : 1), B = (size_t)c->n_upd_blocks;
+  size_t sz[32], off[33], k = 0, n;
+  char *m;
+  DevPtrs *h = &D->sh;
+  if (D->sh_mem) return DGPU_OK;
+#define SZ(bytes) sz[k++] = ((bytes) + 255) / 256 * 256
+  SZ(8 * 25 * N);              /* 0: prim cons rkcons grad gradp */
+  SZ(8 * 5 * N);               /* 1: tiph0 tiph1 tiphw rktiph dphi */
+  SZ(8 * A);                   /* 2: w_ann */
+  SZ(8 * 16 * N);              /* 3: fphi src */
+  SZ(8 * 8 * S);               /* 4: frf */
+  SZ(8 * 5 * S);               /* 5: fS */
+  SZ(8 * 2 * S);               /* 6: fdp */
+  SZ(8 * 4 * A);               /* 7: ann_c */
+  SZ(4 * N);                   /* 8: fstart */
+  SZ(4 * 4 * N);               /* 9: rr */
+  SZ(4 * 2 * S);               /* 10: fL fR */
+  SZ(8 * 2 * S);               /* 11: fdphi fcm */
+  SZ(4 * 4 * A);               /* 12: pair_nf pair_jpmin pair_T pair_seq */
+  SZ(4 * R);                   /* 13: runs */
+  SZ(8 * 2 * B);               /* 14: mdot_part */
+  SZ(4 * 8);                   /* 15: counters */
+  SZ(sizeof(InstState) * (size_t)c->n_inst); /* 16: ist */
+#undef SZ
+  off[0] = 0;
+  for (n = 0; n < k; ++n) off[n + 1] = off[n] + sz[n];
+  CK(cudaMalloc(&D->sh_mem, off[k]));
+  CK(cudaMemset(D->sh_mem, 0, off[k]));
+  m = (char *)D->sh_mem;
+  *h = c->d;
+  h->prim = (double *)(m + off[0]);
+  h->cons = h->prim + 5 * N;
+  h->rkcons = h->cons + 5 * N;
+  h->grad = h->rkcons + 5 * N;
+  h->gradp = h->grad + 5 * N;
+  h->tiph0 = (double *)(m + off[1]);
+  h->tiph1 = h->tiph0 + N;
+  h->tiphw = h->tiph1 + N;
+  h->rktiph = h->tiphw + N;
+  h->dphi = h->rktiph + N;
+  h->w_ann = (double *)(m + off[2]);
+  h->fphi = (double *)(m + off[3]);
+  h->src = h->fphi + 8 * N;
+  h->frf = (double *)(m + off[4]);
+  h->fS = (double *)(m + off[5]);
+  h->fdp = (double *)(m + off[6]);
+  h->ann_c = (double *)(m + off[7]);
+  h->fstart = (int *)(m + off[8]);
+  h->rr = (int *)(m + off[9]);
+  h->fL = (int *)(m + off[10]);
+  h->fR = h->fL + S;
+  h->fdphi = (double *)(m + off[11]);
+  h->fcm = h->fdphi + S;
+  h->pair_nf = (int *)(m + off[12]);
+  h->pair_jpmin = h->pair_nf + A;
+  h->pair_T = h->pair_jpmin + A;
+  h->pair_seq = h->pair_T + A;
+  h->runs = (int *)(m + off[13]);
+  h->mdot_part = (double *)(m + off[14]);
+  h->counters = (unsigned int *)(m + off[15]);
+  h->ist = (InstState *)(m + off[16]);
+  CK(cudaMalloc((void **)&D->d_idx2, sizeof(int)));
+  CK(cudaStreamCreateWithFlags(&D->s2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&D->e_rep, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&D->e_rev, cudaEventDisableTiming));
   return DGPU_OK;
 }
 
@@ -276,13 +376,28 @@ static int dq_consts(struct dgpu_ctx *c, double *dq) {
 }
 
 /* ---- step graphs -------------------------------------------------------- */
+/* One substep of the replay on the shadow buffers (stream s): the eight
+ * kernels in order, k_update recording into rec slot 2 * (*idx) + sub - 1. */
+static int shadow_substep(struct dgpu_ctx *c, DevPtrs *h, cudaStream_t s, int sub, double *rec, const int *idx) {
+  CKK(dgk_cellprep(h, NULL, sub, s));
+  CKK(dgk_merge(h, sub, s));
+  CKK(dgk_rslope(h, NULL, s));
+  CKK(dgk_plm_r(h, NULL, sub, s));
+  CKK(dgk_source(h, NULL, sub, s));
+  CKK(dgk_flux_phi(h, NULL, sub, s));
+  CKK(dgk_flux_r(h, NULL, sub, s));
+  CKK(dgk_update_rec(h, sub, rec, idx, s));
+  return DGPU_OK;
+}
+
 static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
   struct dgpu_diff *Dd = D;
   const int nbK = D->tab_K;
-  double *const *tabS = (double *const *)D->tab_buf;
-  InstState *const *istS = (InstState *const *)D->tab_ist;
-  double *const *tabM = (double *const *)(D->tab_buf + nbK + 1);
-  InstState *const *istM = (InstState *const *)(D->tab_ist + nbK + 1);
+  const int set = (which == G_SEG1 || which == G_REV1) ? 1 : 0;
+  double *const *tabS = (double *const *)D->tab_buf[set];
+  InstState *const *istS = (InstState *const *)D->tab_ist[set];
+  double *const *tabM = (double *const *)(D->tab_buf[set] + nbK + 1);
+  InstState *const *istM = (InstState *const *)(D->tab_ist[set] + nbK + 1);
   switch (which) {
     case G_OBJ: /* one step, its objective and dt into slot *idx, ++*idx */
       if (dctx_launch_step(c)) return -1;
@@ -293,40 +408,50 @@ static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
           dgk_rslope(&c->d, NULL, c->stream) || dgk_plm_r(&c->d, NULL, 1, c->stream) ||
           dgk_set_dt(&c->d, Dd->dtin, Dd->d_idx, c->stream) || dgk_source(&c->d, NULL, 1, c->stream) ||
           dgk_flux_phi(&c->d, NULL, 1, c->stream) || dgk_flux_r(&c->d, NULL, 1, c->stream) ||
-          dgk_update(&c->d, NULL, 1, 7, c->stream) || dctx_substep(c, NULL, 2, 1))
+          dgk_update(&c->d, NULL, 1, 7, c->stream) || dctx_substep(c, NULL, 2, DCTX_FULL, NULL, NULL))
         return -1;
       if (dgk_objective(&c->d, NULL, Dd->o_part, Dd->o_val, NULL, Dd->d_idx, c->stream)) return -1;
       return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
     case G_TAN: /* one tangent step */
-      if (dctx_substep(c, &Dd->t, 1, 1) || dctx_substep(c, &Dd->t, 2, 1)) return -1;
+      if (dctx_substep(c, &Dd->t, 1, DCTX_FULL, NULL, NULL) || dctx_substep(c, &Dd->t, 2, DCTX_FULL, NULL, NULL))
+        return -1;
       if (dgk_objective(&c->d, &Dd->t, Dd->o_part, Dd->o_val, Dd->o_dot, Dd->d_idx, c->stream)) return -1;
       return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
-    case G_SEG: /* replay one step of a segment, storing its substep inputs in slot *idx */
-      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 1, c->stream) || dctx_substep(c, NULL, 1, 1) ||
-          dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 1, c->stream) || dctx_substep(c, NULL, 2, 1))
+    case G_SEG0:
+    case G_SEG1: /* replay one step of a segment on the shadow buffers (stream s2),
+                    storing its substep inputs in slot *idx2 of the set */
+      if (dgk_snap_tab(&Dd->sh, tabS, istS, Dd->d_idx2, 0, 1, Dd->s2) ||
+          shadow_substep(c, &Dd->sh, Dd->s2, 1, Dd->rec[set], Dd->d_idx2) ||
+          dgk_snap_tab(&Dd->sh, tabM, istM, Dd->d_idx2, 0, 1, Dd->s2) ||
+          shadow_substep(c, &Dd->sh, Dd->s2, 2, Dd->rec[set], Dd->d_idx2))
         return -1;
-      return dgk_add_int(Dd->d_idx, 1, c->stream);
-    case G_REV: /* reverse step *idx of the segment (step n = *base + *idx) */
+      return dgk_add_int(Dd->d_idx2, 1, Dd->s2);
+    case G_REV0:
+    case G_REV1: /* reverse step *idx of the segment (step n = *base + *idx) */
       if (dgk_adj_objective(&c->d, &Dd->J, tabS, istS, Dd->d_idx, 1, Dd->wts, Dd->d_base, c->stream)) return -1;
-      if (dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 0, c->stream) || dctx_substep(c, NULL, 2, 0) ||
-          dgk_adj_substep(&c->d, &Dd->J, 2, c->stream, c->side, c->fork[0], c->fork[1]))
+      if (dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 0, c->stream) ||
+          dctx_substep(c, NULL, 2, DCTX_ADJPREP, NULL, NULL) ||
+          dgk_adj_substep(&c->d, &Dd->J, 2, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
         return -1;
-      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 0, c->stream) || dctx_substep(c, NULL, 1, 0) ||
-          dgk_adj_substep(&c->d, &Dd->J, 1, c->stream, c->side, c->fork[0], c->fork[1]))
+      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 0, c->stream) ||
+          dctx_substep(c, NULL, 1, DCTX_ADJPREP, NULL, NULL) ||
+          dgk_adj_substep(&c->d, &Dd->J, 1, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
         return -1;
       return dgk_add_int(Dd->d_idx, -1, c->stream);
   }
   return -1;
 }
 
+/* Captures graph `which` on its stream the first time, then launches it. */
 static int launch_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
+  cudaStream_t s = (which == G_SEG0 || which == G_SEG1) ? D->s2 : c->stream;
   if (!D->have[which]) {
     cudaGraph_t g;
     int rc;
     cudaError_t e;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     rc = record_graph(c, D, which);
-    e = cudaStreamEndCapture(c->stream, &g);
+    e = cudaStreamEndCapture(s, &g);
     if (rc) {
       if (e == cudaSuccess) cudaGraphDestroy(g);
       return fail(c, DGPU_ERR_CUDA, "differentiation step capture failed (%d)", which);
@@ -337,7 +462,7 @@ static int launch_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
     if (e != cudaSuccess) return fail(c, DGPU_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     D->have[which] = 1;
   }
-  CK(cudaGraphLaunch(D->g[which], c->stream));
+  CK(cudaGraphLaunch(D->g[which], s));
   return DGPU_OK;
 }
 
@@ -445,10 +570,10 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   wts[0] = weights ? weights[0] : 1.0;
   wts[1] = weights ? weights[1] : 0.0;
   if ((rc = diff_get(c, &D)) || (rc = ensure_obj(c, D, nsteps)) || (rc = ensure_adj(c, D)) ||
-      (rc = ensure_snaps(c, D, nck, K)))
+      (rc = ensure_snaps(c, D, nck, K)) || (rc = ensure_shadow(c, D)))
     return rc;
   ck = D->snaps;
-  fin = D->snaps + nck + 2 * K + 1;
+  fin = D->snaps + nck + 4 * K + 2;
   if ((rc = dq_consts(c, dq))) return rc;
   CK(cudaMemcpyAsync(D->j_dq, dq, sizeof(dq), cudaMemcpyHostToDevice, c->stream));
 
@@ -480,21 +605,36 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   free(w);
   if (rc) return rc;
 
-  /* reverse sweep, segment by segment */
+  /* reverse sweep, segment by segment: the replay of segment seg - 1 (shadow
+   * buffers, stream s2, stored-state set (seg - 1) % 2) runs while segment seg
+   * is reversed (context buffers, the context's stream, set seg % 2) */
   CK(cudaMemsetAsync(D->J.lW, 0, sizeof(double) * 15 * N, c->stream));
   CK(cudaMemsetAsync(D->J.acc, 0, sizeof(double) * 8, c->stream));
-  for (seg = nck - 1; seg >= 0; --seg) {
-    int n0 = seg * K, n1 = n0 + K < nsteps ? n0 + K : nsteps;
-    CKK(dgk_snap(&c->d, ck[seg].buf, ck[seg].ist, 0, c->stream));
-    CKK(dgk_set_int(D->d_idx, 0, c->stream));
-    for (n = n0; n < n1; ++n)
-      if ((rc = launch_graph(c, D, G_SEG))) return rc;
-    /* the segment's end state in slot n1 - n0 */
-    CKK(dgk_snap_tab(&c->d, (double *const *)D->tab_buf, (InstState *const *)D->tab_ist, D->d_idx, 0, 1, c->stream));
-    CKK(dgk_add_int(D->d_idx, -1, c->stream));
-    CKK(dgk_set_int(D->d_base, n0, c->stream));
-    for (n = n1 - 1; n >= n0; --n)
-      if ((rc = launch_graph(c, D, G_REV))) return rc;
+  CK(cudaEventRecord(D->e_rev, c->stream));
+  for (seg = nck; seg >= 0; --seg) {
+    /* replay segment seg - 1 once the reverse of seg + 1 (same set) is done */
+    if (seg - 1 >= 0) {
+      const int rs = seg - 1, n0 = rs * K, n1 = n0 + K < nsteps ? n0 + K : nsteps, set = rs & 1;
+      CK(cudaStreamWaitEvent(D->s2, D->e_rev, 0));
+      CKK(dgk_snap(&D->sh, ck[rs].buf, ck[rs].ist, 0, D->s2));
+      CKK(dgk_set_int(D->d_idx2, 0, D->s2));
+      for (n = n0; n < n1; ++n)
+        if ((rc = launch_graph(c, D, set ? G_SEG1 : G_SEG0))) return rc;
+      /* the segment's end state in slot n1 - n0 */
+      CKK(dgk_snap_tab(&D->sh, (double *const *)D->tab_buf[set], (InstState *const *)D->tab_ist[set], D->d_idx2, 0,
+                       1, D->s2));
+    }
+    /* reverse segment seg, replayed in the previous iteration */
+    if (seg < nck) {
+      const int n0 = seg * K, n1 = n0 + K < nsteps ? n0 + K : nsteps, set = seg & 1;
+      CK(cudaStreamWaitEvent(c->stream, D->e_rep, 0));
+      CKK(dgk_set_int(D->d_idx, n1 - n0 - 1, c->stream));
+      CKK(dgk_set_int(D->d_base, n0, c->stream));
+      for (n = n1 - 1; n >= n0; --n)
+        if ((rc = launch_graph(c, D, set ? G_REV1 : G_REV0))) return rc;
+      CK(cudaEventRecord(D->e_rev, c->stream));
+    }
+    if (seg - 1 >= 0) CK(cudaEventRecord(D->e_rep, D->s2));
   }
   /* the initial cons are cell_calc_cons of the initial prims */
   CKK(dgk_snap(&c->d, ck[0].buf, ck[0].ist, 0, c->stream));

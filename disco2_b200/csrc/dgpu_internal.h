@@ -197,6 +197,10 @@ int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream);
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
+/* k_update recording the conserved sum and new widths into rec (adjoint replay) */
+int dgk_update_rec(const DevPtrs *d, int substep, double *rec, const int *rec_idx, void *stream);
+/* the per-annulus constants of k_source only (ann_c) */
+int dgk_ann_consts(const DevPtrs *d, int substep, void *stream);
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream);
 /* differentiation (dgpu_adjoint.cu) */
 int dgk_objective(const DevPtrs *d, const TanPtrs *t, double *part, double *out, double *out_d, const int *idx,
@@ -211,11 +215,12 @@ int dgk_snap_tab(const DevPtrs *d, double *const *bufs, InstState *const *ists, 
 int dgk_adj_rows(const DevPtrs *d);
 int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double *const *bufs, InstState *const *ists,
                       const int *idx, int off, const double *wts, const int *base, void *stream);
-int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, void *stream, void *side, void *ev_fork,
-                    void *ev_join);
+int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, const double *rec, const int *idx,
+                    void *stream, void *side, void *ev_fork, void *ev_join);
 int dgk_adj_calc_cons(const DevPtrs *d, const AdjPtrs *J, void *stream);
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
 int dgk_update_blocks(int n_cells);
+int dgk_block_size(void);
 int dgk_aos_to_soa(double *soa, int nq, int stride, int base, const double *aos, int n, void *stream);
 int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa, int n, void *stream);
 #ifdef __cplusplus

@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, TanPt
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
 template <typename T>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, TanPtrs tp, int substep) {
+__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
   __shared__ double sh_md[2][BLK / 32];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, Tan
     d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
   }
   double md0 = 0.0, md1 = 0.0;
-  if (t < N) {
+  if (t < N && cells) {
     const int g = t;
     const int a = d.cell_ann[g];
     const Annulus &A = d.ann[a];
@@ -827,8 +827,11 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, Tan
 }
 
 template <typename T>
+// rec (the adjoint's segment replay, else NULL): the conserved sum before
+// cons2prim and the new width of each cell go to slot 2 * (*rec_idx) +
+// substep - 1 of rec ([slot][6][n_cells]).
 __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
-                                                                  int tail) {
+                                                                  int tail, double *rec, const int *rec_idx) {
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -850,6 +853,12 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, Tan
       if (substep == 1) d.rktiph[g] = rk;
       (substep == 1 ? d.tiph1 : d.tiph0)[g] = tn;
       d.dphi[g] = dphi_n;
+      if (rec) {
+        double *rs = rec + (size_t)(2 * (*rec_idx) + substep - 1) * 6 * N;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) rs[(size_t)q * N + g] = val(c[q]);
+        rs[(size_t)5 * N + g] = dphi_n;
+      }
       // cell_calc_prim -> cell_cons2prim (src/Cell/cell_conversion.c:57-122)
       const double r = .5 * (A.rm + A.rp);
       const double dV = A.dv_half * dphi_n * P.dz;
@@ -1034,6 +1043,7 @@ int dgk_soa_to_aos(double *aos, int nq, int stride, int base, const double *soa,
 }
 
 int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
+int dgk_block_size(void) { return BLK; }
 
 // t == NULL: the forward kernels; otherwise their tangent instances.
 #define DGK_LAUNCH(kern, grid, smem, stream, ...)                                                  \
@@ -1073,18 +1083,31 @@ int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
 }
 int dgk_source(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   int n = d->n_cells > d->n_ann ? d->n_cells : d->n_ann;
-  DGK_LAUNCH(k_source, (n + BLK - 1) / BLK, 0, stream, substep);
+  DGK_LAUNCH(k_source, (n + BLK - 1) / BLK, 0, stream, substep, 1);
   return (int)cudaGetLastError();
 }
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream) {
   int tail = stop >= 7 ? 2 : (stop >= 5 ? 1 : 0);
-  DGK_LAUNCH(k_update, dgk_update_blocks(d->n_cells), 0, stream, substep, stop, tail);
+  DGK_LAUNCH(k_update, dgk_update_blocks(d->n_cells), 0, stream, substep, stop, tail, (double *)NULL,
+             (const int *)NULL);
+  return (int)cudaGetLastError();
+}
+int dgk_update_rec(const DevPtrs *d, int substep, double *rec, const int *rec_idx, void *stream) {
+  static const TanPtrs none = {};
+  k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, 7, 2, rec,
+                                                                                      rec_idx);
+  return (int)cudaGetLastError();
+}
+int dgk_ann_consts(const DevPtrs *d, int substep, void *stream) {
+  static const TanPtrs none = {};
+  k_source<double><<<(d->n_ann + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, 0);
   return (int)cudaGetLastError();
 }
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
   int tail = stop >= 5 ? 1 : 0;
   static const TanPtrs none = {};
-  k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop, tail);
+  k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop, tail,
+                                                                                      nullptr, nullptr);
   return (int)cudaGetLastError();
 }
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream) {
