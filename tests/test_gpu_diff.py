@@ -184,18 +184,45 @@ def test_gradient_matches_reference_finite_differences():
         grads.append(ctx.adjoint(ref["nsteps"], ref["window_start"], ckpt_every=25, weights=w))
         ctx.close()
     assert np.allclose([grads[0]["J"][0], grads[1]["J"][1]], ref["J"], rtol=1e-8, atol=0)
-    fd = ref["fd"]["1e-08"]
     rows = []
     for k in range(2):
         g = grads[k]
-        rows.append(("q", k, g["dq"], fd["q"][k]))
-        rows.append(("alpha", k, g["dalpha"], fd["alpha"][k]))
-        for d in range(len(fd["sigma"])):
+        vals = [("q", g["dq"]), ("alpha", g["dalpha"])]
+        for d in range(len(ref["fd"]["1e-08"]["sigma"])):
             u = np.random.default_rng(1000 + d).standard_normal(prim0.shape[0])
             dirv = np.zeros_like(prim0)
             dirv[:, 0] = prim0[:, 0] * u
             dirv[:, 1] = prim0[:, 1] * u
-            rows.append((f"sigma{d}", k, float(np.sum(g["dprim"] * dirv)), fd["sigma"][d][k]))
-    for name, k, a, f in rows:
-        print(f"{name:8s} {'torque' if k == 0 else 'mdot':6s} adjoint={a:+.9e} reference_fd={f:+.9e} "
-              f"rel={abs(a - f) / max(abs(f), 1e-300):.2e}")
+            vals.append((f"sigma{d}", float(np.sum(g["dprim"] * dirv))))
+        for name, a in vals:
+            f8 = ref["fd"]["1e-08"][name][k] if not name.startswith("sigma") else \
+                ref["fd"]["1e-08"]["sigma"][int(name[5:])][k]
+            f6 = ref["fd"]["1e-06"][name][k] if not name.startswith("sigma") else \
+                ref["fd"]["1e-06"]["sigma"][int(name[5:])][k]
+            rows.append((name, k, a, f8, abs(a - f8) / abs(f8), abs(a - f6) / abs(f6)))
+    for name, k, a, f8, r8, r6 in rows:
+        print(f"{name:8s} {'torque' if k == 0 else 'mdot':6s} adjoint={a:+.9e} reference_fd(1e-8)={f8:+.9e} "
+              f"rel={r8:.2e}   rel vs step 1e-6: {r6:.2e}")
+    r8 = np.array([r[4] for r in rows])
+    # 500 steps of limiter and Riemann-state switching: the central differences
+    # carry kink and round-off errors of up to a few 1e-4 (see the 1e-6 column)
+    assert np.median(r8) < 5e-5, np.median(r8)
+    assert np.max(r8) < 1e-3, np.max(r8)
+
+
+def test_autograd_wrapper_matches_adjoint(base):
+    """The torch.autograd.Function of the check harness: backward of a scalar
+    function of J is one dgpu_adjoint call with the incoming weights."""
+    import torch
+    from disco2_b200.autograd import DiskRun
+    prim0 = torch.tensor(base["prim"], requires_grad=True)
+    q = torch.tensor(Q0, dtype=torch.float64, requires_grad=True)
+    a = torch.tensor(ALPHA0, dtype=torch.float64, requires_grad=True)
+    J = DiskRun.apply(prim0, q, a, _cbd(), NSTEPS, W0)
+    assert np.array_equal(J.detach().numpy(), base["J"])
+    (J[0] + 2.0 * J[1]).backward()
+    ctx = _ctx(base)
+    g = ctx.adjoint(NSTEPS, W0, ckpt_every=25, weights=(1.0, 2.0))
+    ctx.close()
+    assert q.grad.item() == g["dq"] and a.grad.item() == g["dalpha"]
+    assert np.array_equal(prim0.grad.numpy(), g["dprim"])
