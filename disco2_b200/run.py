@@ -1,11 +1,13 @@
 """Run a named workload for a few RK2 steps on cuda:0.
 
     python -m disco2_b200.run --workload circumbinary --steps 3 [--timed] [--batch N]
+    python -m disco2_b200.run --workload circumbinary --num-r 192 --steps 0 --adjoint 10 --ckpt 5
 
 Used for profiling (ncu attaches to this process) and as a minimal example of
 the C ABI from Python.  --timed adds one step launched kernel by kernel
 with CUDA events and prints the per-kernel device times.  --batch N steps N
-copies of the disk in one context.
+copies of the disk in one context.  --adjoint N then runs the gradient of an
+N-step run (objectives over its second half, checkpoints every --ckpt steps).
 """
 from __future__ import annotations
 
@@ -24,13 +26,19 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--timed", action="store_true")
     ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--adjoint", type=int, default=0)
+    ap.add_argument("--ckpt", type=int, default=25)
     args = ap.parse_args()
     p = WORKLOADS[args.workload]() if args.num_r is None else WORKLOADS[args.workload](num_r=args.num_r)
     sims = [lib.Sim(p) for _ in range(args.batch)]
     ctx = lib.Context(sims)
     for k in range(args.batch):
         ctx.init_state(k)
-    ctx.step(args.steps)
+    if args.steps:
+        ctx.step(args.steps)
+    if args.adjoint:
+        g = ctx.adjoint(args.adjoint, args.adjoint // 2, ckpt_every=args.ckpt)
+        print(f"adjoint: J={g['J']} dJ/dq={g['dq']:.9e} dJ/dalpha={g['dalpha']:.9e}")
     if args.timed:
         ms = ctx.step_timed(1)
         names = lib.Context.KERNELS
