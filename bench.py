@@ -227,6 +227,8 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
     stream = torch.cuda.Stream()
 
     def timed(ctx):
+        if args.tune_steps > 0:
+            ctx.autotune(args.tune_steps)
         ctx.step(2, sync=True)  # warm-up, graph capture
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(k_steps)]
@@ -266,7 +268,7 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
             "cells": int(sum(s.num_cells for s in sims_all)), "interior_cells": int(tot),
             "steps": k_steps, "value": v_b, "unit": UNIT, "ms_per_step": ms_b / k_steps,
             "sequential_value": v_s, "batched_over_sequential": v_b / v_s,
-            "how": "one context holding every disk of the rank vs one context per disk run "
+            "how": "one context holding every disk of the rank vs one context per disk run (each autotuned) "
                    "back to back, same steps, L2 flushed before each step"}
 
 
@@ -322,6 +324,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--tune-steps", type=int, default=3,
+                    help="steps per launch-shape candidate for the autotuner (0: built-in shapes)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=500)
     args = ap.parse_args()
@@ -361,6 +365,8 @@ def main():
     ctx = lib.Context(sim, device=local, stream=stream.cuda_stream)
     ctx.init_state(0)
     L = lib.load()
+    # launch shapes of the heavy kernels timed on this disk (state restored)
+    tuned = ctx.autotune(args.tune_steps) if args.tune_steps > 0 else None
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     uuid = None
@@ -474,7 +480,8 @@ def main():
             "config": {"workload": desc, "cells": ncell, "interior_cells": nin,
                        "annuli": sim.num_annuli, "r_faces": nfaces,
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single disk"},
+                       "parallelism": f"replicas x{world}" if world > 1 else "single disk",
+                       "blocks_per_sm": tuned},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profiled_traffic(dom) if args.workload == "circumbinary" else None,

@@ -724,6 +724,81 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
   return dctx_read_err(c);
 }
 
+/* The autotuner: a coordinate search over the resident blocks per SM of the
+ * five heavy kernels (the register budget the compiler gets), each timed on
+ * the context's own disks by dgpu_step_rk2_timed from the same saved state.
+ * The instances differ only in register allocation, so the results are
+ * bitwise the same whatever is chosen. */
+#define TUNE_NCAND 4
+static const int tune_cand[TUNE_NCAND] = {2, 3, 4, 5};
+/* kernel_ms slot of each tuned kernel in substep 1 (substep 2 is +8) */
+static const int tune_slot[DGPU_TUNE_N] = {3, 5, 6, 4, 7};
+
+int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
+  double *buf = NULL, ms[DGPU_STEP_KERNELS];
+  InstState *ist = NULL;
+  int k, v, rc = DGPU_OK;
+  static const int order[DGPU_TUNE_N] = {DGPU_TUNE_UPDATE, DGPU_TUNE_FLUXR, DGPU_TUNE_FLUXPHI, DGPU_TUNE_SOURCE,
+                                         DGPU_TUNE_PLM};
+  if (!c || steps < 0) return DGPU_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (steps == 0) {
+    /* apply the given choice */
+    if (!choice) return fail(c, DGPU_ERR_ARG, "steps == 0 needs a choice to apply");
+    for (k = 0; k < DGPU_TUNE_N; ++k) {
+      if (choice[k] != 0 && (choice[k] < 2 || choice[k] > 5))
+        return fail(c, DGPU_ERR_ARG, "blocks per SM must be 0 or 2..5, got %d", choice[k]);
+    }
+    for (k = 0; k < DGPU_TUNE_N; ++k) c->d.tune[k] = choice[k];
+  } else {
+    /* save the state, time each candidate from it, restore it */
+    if (cudaMalloc((void **)&buf, sizeof(double) * 19 * (size_t)c->n_cells) != cudaSuccess ||
+        cudaMalloc((void **)&ist, sizeof(InstState) * (size_t)c->n_inst) != cudaSuccess) {
+      cudaFree(buf);
+      cudaGetLastError();
+      return fail(c, DGPU_ERR_NOMEM, "autotune: device allocation failed");
+    }
+    if (dgk_snap(&c->d, buf, ist, 1, c->stream)) rc = fail(c, DGPU_ERR_CUDA, "autotune: state save failed");
+    for (k = 0; k < DGPU_TUNE_N && rc == DGPU_OK; ++k) {
+      const int kk = order[k];
+      double best = 1e300;
+      int bestv = c->d.tune[kk];
+      for (v = 0; v < TUNE_NCAND && rc == DGPU_OK; ++v) {
+        double t;
+        c->d.tune[kk] = tune_cand[v];
+        if (dgk_snap(&c->d, buf, ist, 0, c->stream)) {
+          rc = fail(c, DGPU_ERR_CUDA, "autotune: state restore failed");
+          break;
+        }
+        memset(ms, 0, sizeof(ms));
+        if ((rc = dgpu_step_rk2_timed(c, 1, ms))) break; /* warm-up */
+        memset(ms, 0, sizeof(ms));
+        if ((rc = dgpu_step_rk2_timed(c, steps, ms))) break;
+        t = ms[tune_slot[kk]] + ms[tune_slot[kk] + 8];
+        if (t < best) {
+          best = t;
+          bestv = tune_cand[v];
+        }
+      }
+      c->d.tune[kk] = bestv;
+    }
+    if (rc == DGPU_OK && dgk_snap(&c->d, buf, ist, 0, c->stream))
+      rc = fail(c, DGPU_ERR_CUDA, "autotune: state restore failed");
+    if (rc == DGPU_OK) rc = dgpu_synchronize(c);
+    cudaFree(buf);
+    cudaFree(ist);
+    if (rc) return rc;
+  }
+  /* the step graph holds the old launch shapes */
+  if (c->have_graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->have_graph = 0;
+  }
+  if (choice)
+    for (k = 0; k < DGPU_TUNE_N; ++k) choice[k] = c->d.tune[k];
+  return DGPU_OK;
+}
+
 int dgpu_stage(dgpu_ctx *c, int phase) {
   if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);

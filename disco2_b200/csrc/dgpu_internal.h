@@ -108,6 +108,14 @@ typedef struct {
   double gx[2], gy[2], gc[2], gs[2], rkx[2], rky[2];
 } InstState;
 
+/* Kernels whose launch shape the autotuner chooses (DevPtrs.tune). */
+#define DGPU_TUNE_PLM 0
+#define DGPU_TUNE_FLUXPHI 1
+#define DGPU_TUNE_FLUXR 2
+#define DGPU_TUNE_SOURCE 3
+#define DGPU_TUNE_UPDATE 4
+#define DGPU_TUNE_N 5
+
 /* Device pointers and sizes handed to every kernel. */
 typedef struct {
   int n_inst, n_ann, n_cells, n_slots, n_runs;
@@ -138,6 +146,7 @@ typedef struct {
   double *mdot_part;      /* [n_blocks_update][2] per-block sink sums */
   unsigned int *counters; /* last-block counters */
   int *err;               /* error flags */
+  int tune[DGPU_TUNE_N];  /* host-side launch choice of the tuned kernels: resident blocks per SM (0: built-in) */
 } DevPtrs;
 
 /* Forward-mode tangent: d/de of the state and of the substep intermediates

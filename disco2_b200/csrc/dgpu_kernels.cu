@@ -39,8 +39,14 @@
 #ifndef DGPU_MINB_FLUX
 #define DGPU_MINB_FLUX 4
 #endif
+#ifndef DGPU_MINB_FLUXR
+#define DGPU_MINB_FLUXR 3
+#endif
+#ifndef DGPU_MINB_SOURCE
+#define DGPU_MINB_SOURCE 3
+#endif
 #ifndef DGPU_MINB_UPDATE
-#define DGPU_MINB_UPDATE 3
+#define DGPU_MINB_UPDATE 4
 #endif
 
 namespace {
@@ -423,8 +429,8 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, TanPtrs tp, int substep) {
+template <typename T, int MB = DGPU_MINB_PLM>
+__global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells, NS = d.n_slots;
   unsigned long long key = ~0ull;
@@ -553,8 +559,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_PLM) k_plm_r(DevPtrs d, TanPtrs
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
 // phi faces: thread per cell j, face (j, j+1) (riemann_setup_p, Riemann_setup.c:46-80)
-template <typename T>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
+template <typename T, int MB = DGPU_MINB_FLUX>
+__global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
@@ -612,8 +618,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_phi(DevPtrs d, Tan
 }
 
 // r faces: thread per face slot (riemann_setup_rz, Riemann_setup.c:11-44)
-template <typename T>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
+template <typename T, int MB = DGPU_MINB_FLUXR>
+__global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   const double fac = substep == 1 ? 1.0 : 0.5;
@@ -689,8 +695,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FLUX) k_flux_r(DevPtrs d, TanPt
 // so this kernel runs concurrently with k_flux.  Its first n_ann threads also
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
-template <typename T>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
+template <typename T, int MB = DGPU_MINB_SOURCE>
+__global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
   __shared__ double sh_md[2][BLK / 32];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -826,11 +832,11 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_source(DevPtrs d, Tan
   }
 }
 
-template <typename T>
 // rec (the adjoint's segment replay, else NULL): the conserved sum before
 // cons2prim and the new width of each cell go to slot 2 * (*rec_idx) +
 // substep - 1 of rec ([slot][6][n_cells]).
-__global__ void __launch_bounds__(BLK, DGPU_MINB_UPDATE) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
+template <typename T, int MB = DGPU_MINB_UPDATE>
+__global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
                                                                   int tail, double *rec, const int *rec_idx) {
   __shared__ bool last;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1052,6 +1058,24 @@ int dgk_block_size(void) { return BLK; }
     if (t) kern<Dual><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, *t, __VA_ARGS__);       \
     else kern<double><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, none_, __VA_ARGS__);    \
   } while (0)
+// The same for the kernels the autotuner sizes: the forward instance with
+// d->tune[which] resident blocks per SM (0: the built-in choice).
+#define DGK_LAUNCH_TUNED(kern, which, grid, stream, ...)                                  \
+  do {                                                                                   \
+    static const TanPtrs none_ = {};                                                     \
+    cudaStream_t s_ = (cudaStream_t)(stream);                                            \
+    if (t) {                                                                             \
+      kern<Dual><<<(grid), BLK, 0, s_>>>(*d, *t, __VA_ARGS__);                            \
+    } else {                                                                             \
+      switch (d->tune[which]) {                                                          \
+        case 2: kern<double, 2><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__); break;   \
+        case 3: kern<double, 3><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__); break;   \
+        case 4: kern<double, 4><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__); break;   \
+        case 5: kern<double, 5><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__); break;   \
+        default: kern<double><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__);           \
+      }                                                                                  \
+    }                                                                                    \
+  } while (0)
 
 int dgk_cellprep(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   DGK_LAUNCH(k_cellprep, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
@@ -1069,27 +1093,27 @@ int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream) {
   return (int)cudaGetLastError();
 }
 int dgk_plm_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
-  DGK_LAUNCH(k_plm_r, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
+  DGK_LAUNCH_TUNED(k_plm_r, DGPU_TUNE_PLM, (d->n_cells + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
-  DGK_LAUNCH(k_flux_phi, (d->n_cells + BLK - 1) / BLK, 0, stream, substep);
+  DGK_LAUNCH_TUNED(k_flux_phi, DGPU_TUNE_FLUXPHI, (d->n_cells + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   if (d->n_slots <= 0) return 0;
-  DGK_LAUNCH(k_flux_r, (d->n_slots + BLK - 1) / BLK, 0, stream, substep);
+  DGK_LAUNCH_TUNED(k_flux_r, DGPU_TUNE_FLUXR, (d->n_slots + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_source(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   int n = d->n_cells > d->n_ann ? d->n_cells : d->n_ann;
-  DGK_LAUNCH(k_source, (n + BLK - 1) / BLK, 0, stream, substep, 1);
+  DGK_LAUNCH_TUNED(k_source, DGPU_TUNE_SOURCE, (n + BLK - 1) / BLK, stream, substep, 1);
   return (int)cudaGetLastError();
 }
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream) {
   int tail = stop >= 7 ? 2 : (stop >= 5 ? 1 : 0);
-  DGK_LAUNCH(k_update, dgk_update_blocks(d->n_cells), 0, stream, substep, stop, tail, (double *)NULL,
-             (const int *)NULL);
+  DGK_LAUNCH_TUNED(k_update, DGPU_TUNE_UPDATE, dgk_update_blocks(d->n_cells), stream, substep, stop, tail,
+                   (double *)NULL, (const int *)NULL);
   return (int)cudaGetLastError();
 }
 int dgk_update_rec(const DevPtrs *d, int substep, double *rec, const int *rec_idx, void *stream) {

@@ -51,6 +51,7 @@ SIGNATURES = {
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
     "dgpu_torque": (_I, [_P, _I, _dp]),
     "dgpu_face_list_noalloc": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _ip, _P]),
+    "dgpu_autotune": (_I, [_P, _I, _ip]),
     "dgpu_objective": (_I, [_P, _I, _I, _dp, _dp, _dp]),
     "dgpu_tangent": (_I, [_P, _I, _I, _D, _D, _dp, _dp, _dp]),
     "dgpu_adjoint": (_I, [_P, _I, _I, _I, _dp, _dp, _dp, _dp, _dp]),
@@ -257,6 +258,16 @@ class Context:
         v = C.c_double()
         self._ck(load().dgpu_torque(self._h, inst, C.byref(v)))
         return v.value
+
+    TUNED = ("plm_r", "flux_phi", "flux_r", "source", "update")
+
+    def autotune(self, steps: int = 3, choice=None) -> dict:
+        """Time each launch shape of the heavy kernels on this context's disks
+        and keep the fastest (steps == 0: apply `choice`); returns the blocks
+        per SM chosen for each tuned kernel."""
+        ch = (C.c_int * 5)(*(choice if choice is not None else [0] * 5))
+        self._ck(load().dgpu_autotune(self._h, steps, ch))
+        return dict(zip(self.TUNED, list(ch)))
 
     # ---- differentiation (one disk per context) ----
     def objective(self, nsteps: int, window_start: int, dt=None, return_dt: bool = False):

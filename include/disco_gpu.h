@@ -114,6 +114,17 @@ int dgpu_synchronize(dgpu_ctx *ctx);
  * For measurement only: inside the step graph merge runs beside cellprep, and
  * source and flux_phi beside flux_r. */
 int dgpu_step_rk2_timed(dgpu_ctx *ctx, int nsteps, double *kernel_ms);
+/* Autotuner (no counterpart in the reference): chooses, for the five heavy
+ * step kernels, how many blocks of 256 threads each SM should hold (2..5, the
+ * register budget per thread), by timing every choice on this context's own
+ * disks from its current state with dgpu_step_rk2_timed (1 warm-up + `steps`
+ * steps per choice), one kernel after the other.  The state, t and the
+ * GravMass are restored afterwards, and results are bitwise the same under
+ * every choice.  choice[5] (may be NULL) receives the chosen values in the
+ * order plm_r, flux_phi, flux_r, source, update; with steps == 0 the given
+ * choice[5] is applied instead (0 = the built-in value).  The next
+ * dgpu_step_rk2 captures a new step graph.  Synchronous. */
+int dgpu_autotune(dgpu_ctx *ctx, int steps, int *choice);
 /* Stage parity: the prologue of timestep_rk2 and the first substep
  * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`
  * (0 faces/clean_pi/set_w/RK blend, 1 PLM, 2 phi fluxes, 3 r fluxes,
