@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CC = shutil.which("gcc") or "gcc"
 
 C_SOURCES = ["dgpu_sim.c", "dgpu_ctx.c", "dgpu_diff.c"]
-CU_SOURCES = ["dgpu_kernels.cu", "dgpu_adjoint.cu"]
+CU_SOURCES = ["dgpu_kernels.cu", "dgpu_adjoint.cu", "dgpu_diag.cu"]
 HEADERS = ["dgpu_internal.h", "dgpu_sim.h", "dgpu_ctx.h", "dgpu_device.cuh", "dgpu_step.cuh", "dgpu_adjoint.cuh"]
 
 NVCC_FLAGS = [

@@ -188,6 +188,7 @@ void dgpu_destroy(dgpu_ctx *c) {
   cudaSetDevice(c->device);
   if (c->have_graph) cudaGraphExecDestroy(c->graph);
   dctx_diff_free(c);
+  if (c->d_diag) cudaFree(c->d_diag);
   {
     void *ps[] = {c->d_par, c->d_ist, c->d_ann, c->d_cell_ann, c->d_slot_ann, c->d.prim, c->d.cons,
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
@@ -878,6 +879,45 @@ int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, dou
   }
   free(nf); free(fL); free(fR); free(fd); free(fc);
   return DGPU_OK;
+}
+
+int dgpu_diagnostics(dgpu_ctx *c, int inst, double *vector, double *scalar, double *equat, double *extra) {
+  const struct dgpu_sim *s;
+  const DiskParams *p;
+  int nvec, neq, nextra, nrow, i, imin, imax, first = 0, ncell = 0, rc = check_inst(c, inst);
+  size_t need, nr;
+  double *rows, *dv, *ds, *de, *dx;
+  if (rc) return rc;
+  s = c->sims[inst];
+  p = &c->h_par[inst];
+  dgk_diag_sizes(&nvec, &neq, &nextra, &nrow);
+  imin = s->ng_min[0];
+  imax = s->NR - s->ng_max[0];
+  for (i = 0; i < s->NR; ++i) {
+    if (i < imin) first += s->N_p[i];
+    else if (i < imax) ncell += s->N_p[i];
+  }
+  nr = (size_t)(imax - imin);
+  need = (size_t)s->NR * nrow + nr * nvec + 16 + (size_t)ncell * neq + nextra;
+  if (c->diag_cap < need) {
+    if (c->d_diag) cudaFree(c->d_diag);
+    c->d_diag = NULL;
+    c->diag_cap = 0;
+    CK(cudaMalloc((void **)&c->d_diag, sizeof(double) * need));
+    c->diag_cap = need;
+  }
+  rows = c->d_diag;
+  dv = rows + (size_t)s->NR * nrow;
+  ds = dv + nr * nvec;
+  de = ds + 16;
+  dx = de + (size_t)ncell * neq;
+  CKK(dgk_diagnostics(&c->d, inst, s->NR, rows, dv, ds, equat ? de : NULL, p->cell_base + first, dx,
+                      s->Z_Max - s->Z_Min, s->R_Min, s->R_Max, c->stream));
+  if (vector) CK(cudaMemcpyAsync(vector, dv, sizeof(double) * nr * nvec, cudaMemcpyDeviceToHost, c->stream));
+  if (scalar) CK(cudaMemcpyAsync(scalar, ds, sizeof(double) * 16, cudaMemcpyDeviceToHost, c->stream));
+  if (equat) CK(cudaMemcpyAsync(equat, de, sizeof(double) * (size_t)ncell * neq, cudaMemcpyDeviceToHost, c->stream));
+  if (extra) CK(cudaMemcpyAsync(extra, dx, sizeof(double) * nextra, cudaMemcpyDeviceToHost, c->stream));
+  return dgpu_synchronize(c);
 }
 
 int dgpu_torque(dgpu_ctx *c, int inst, double *torque) {

@@ -34,6 +34,8 @@ struct dgpu_ctx {
   cudaGraphExec_t graph;
   int have_graph;
   struct dgpu_diff *diff;
+  double *d_diag;     /* diagnostics buffers (allocated on first use) */
+  size_t diag_cap;    /* their size in doubles */
   char err[512];
 };
 

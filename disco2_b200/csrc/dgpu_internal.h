@@ -227,6 +227,10 @@ int dgk_adj_objective(const DevPtrs *d, const AdjPtrs *J, double *const *bufs, I
 int dgk_adj_substep(const DevPtrs *d, const AdjPtrs *J, int substep, const double *rec, const int *idx,
                     void *stream, void *side, void *ev_fork, void *ev_join);
 int dgk_adj_calc_cons(const DevPtrs *d, const AdjPtrs *J, void *stream);
+/* diagnostics (dgpu_diag.cu) */
+int dgk_diag_sizes(int *nvec, int *neq, int *nextra, int *nrow);
+int dgk_diagnostics(const DevPtrs *d, int inst, int n_ann_disk, double *rows, double *vector, double *scalar,
+                    double *equat, int eq_first, double *extra, double zspan, double rmin, double rmax, void *stream);
 int dgk_torque(const DevPtrs *d, int inst, double *part, double *out, int n_inst_cells, void *stream);
 int dgk_update_blocks(int n_cells);
 int dgk_block_size(void);

@@ -52,6 +52,7 @@ SIGNATURES = {
     "dgpu_torque": (_I, [_P, _I, _dp]),
     "dgpu_face_list_noalloc": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _ip, _P]),
     "dgpu_autotune": (_I, [_P, _I, _ip]),
+    "dgpu_diagnostics": (_I, [_P, _I, _dp, _dp, _dp, _dp]),
     "dgpu_objective": (_I, [_P, _I, _I, _dp, _dp, _dp]),
     "dgpu_tangent": (_I, [_P, _I, _I, _D, _D, _dp, _dp, _dp]),
     "dgpu_adjoint": (_I, [_P, _I, _I, _I, _dp, _dp, _dp, _dp, _dp]),
@@ -258,6 +259,18 @@ class Context:
         v = C.c_double()
         self._ck(load().dgpu_torque(self._h, inst, C.byref(v)))
         return v.value
+
+    def diagnostics(self, inst: int = 0) -> dict:
+        """diagnostics_set's reductions of the current state (before dtout)."""
+        s = self.sims[inst]
+        nr = int(s.param("NumR"))
+        N_p, _ = s.grid()
+        ncell = int(sum(N_p[1:1 + nr]))  # one inner ghost annulus (sim_alloc_arr, single rank)
+        out = {"vector": np.zeros((nr, 17)), "scalar": np.zeros(16), "equat": np.zeros((ncell, 18)),
+               "extra": np.zeros(14)}
+        self._ck(load().dgpu_diagnostics(self._h, inst, _dptr(out["vector"]), _dptr(out["scalar"]),
+                                         _dptr(out["equat"]), _dptr(out["extra"])))
+        return out
 
     TUNED = ("plm_r", "flux_phi", "flux_r", "source", "update")
 

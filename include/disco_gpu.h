@@ -179,6 +179,28 @@ int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double
  * diagnostic). */
 int dgpu_torque(dgpu_ctx *ctx, int inst, double *torque);
 
+/* ---- Diagnostics -----------------------------------------------------------------
+ * The reductions of diagnostics_set (src/Diagnostics/diagnostics_set.c:13-298)
+ * on the current state of a disk, before the reference's weighting by the time
+ * since the last measurement (dtout), which the caller applies when it
+ * accumulates time averages.  Any pointer may be NULL.
+ *   vector[nr][17]: per non-ghost annulus (nr = NumR), the phi average times
+ *     dz/(Z_Max - Z_Min) of r, rho, P, v_r, v_phi (frame included), v_z,
+ *     v_phi - w, Cool, passive scalar, E_hydro, KE, rho e, 0, 0, 0, 0, 0
+ *     (VectorDiag / dtout; Cool and the passive scalar are 0 here: no cooling,
+ *     NUM_Q = 5);
+ *   scalar[16]: sum over annuli of vector[i][n+1] (rp^2 - rm^2) divided by
+ *     (R_Max^2 - R_Min^2) (ScalarDiag / dtout);
+ *   equat[cells][18]: the equatorial row of every non-ghost cell, in (k, i, j)
+ *     order (EquatDiag);
+ *   extra[14]: the DiagMdot line after t (Mdot_near_req1, r_near_req1,
+ *     mass_inside_1, mass_inner_wedge, Mdot_0, Mdot_1, Macc_0, Macc_1, mass
+ *     within 0.2 of mass 0 and 1, within 0.4 of mass 0 and 1), then the masses
+ *     within 0.1 of mass 0 and 1.  The reference's quirks are kept: its
+ *     Mdot_near_req1 is built from the v_z column, and its inner wedge sums the
+ *     first N_p(outer ghost) cells of the disk with the radii of annulus 0. */
+int dgpu_diagnostics(dgpu_ctx *ctx, int inst, double *vector, double *scalar, double *equat, double *extra);
+
 /* ---- Differentiation (a context holding one disk) ------------------------------
  * No counterpart in the reference.  A run advances the context's disk by
  * nsteps RK2 steps from its current state (leaving it at the final state,

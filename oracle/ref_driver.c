@@ -27,6 +27,13 @@
  *       timestep_rk2 (src/TimeStep/timestep_algorithm.c:13-39) in its order
  *       with timestep_set_dt replaced by the next dt of the file.
  *
+ *   disco_ref diag <par> <nsteps> <out.bin> [--load in.bin]
+ *       creates the reference's Diagnostics at t = 0, runs nsteps steps and
+ *       calls diagnostics_set (src/Diagnostics/diagnostics_set.c:13-298) once
+ *       (its measuring time is moved to now); it appends to DiagMdot.dat in
+ *       the working directory.  Dump: "DDIAG1\0\0", int32 nr neq, double t,
+ *       VectorDiag[nr][17], ScalarDiag[16], EquatDiag[neq][18].
+ *
  *   disco_ref stage <par> <phase> <out.bin> [--load in.bin]
  *       runs the prologue of timestep_rk2 and then the body of
  *       timestep_substep (src/TimeStep/timestep_routines.c:16-113), calling
@@ -47,11 +54,13 @@
 #define FACE_PRIVATE_DEFS
 #define TIMESTEP_PRIVATE_DEFS
 #define PLANET_PRIVATE_DEFS
+#define DIAGNOSTICS_PRIVATE_DEFS
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
 #include "Headers/Cell.h"
+#include "Headers/Diagnostics.h"
 #include "Headers/Face.h"
 #include "Headers/GravMass.h"
 #include "Headers/MPIsetup.h"
@@ -388,6 +397,26 @@ int main(int argc, char **argv) {
     }
     fclose(fo);
     if (fd) fclose(fd);
+  } else if (!strcmp(mode, "diag")) {
+    struct Diagnostics *D = diagnostics_create(s, ts, mpi);
+    FILE *f;
+    int nr = sim_N_global(s, R_DIR), n;
+    for (step = 0; step < nsteps; ++step) timestep_rk2(ts, s, cells, gm, mpi);
+    D->tdiag_measure = -1.0;
+    diagnostics_set(D, cells, s, ts, mpi, gm);
+    f = fopen(out, "wb");
+    if (!f) {
+      fprintf(stderr, "cannot open %s\n", out);
+      return 2;
+    }
+    wr(f, "DDIAG1\0", 1, 8);
+    wr(f, &nr, sizeof(int), 1);
+    wr(f, &D->N_eq_cells, sizeof(int), 1);
+    wr(f, &ts->t, sizeof(double), 1);
+    for (n = 0; n < nr; ++n) wr(f, D->VectorDiag[n], sizeof(double), 17);
+    wr(f, D->ScalarDiag, sizeof(double), 16);
+    for (n = 0; n < D->N_eq_cells; ++n) wr(f, D->EquatDiag[n], sizeof(double), 18);
+    fclose(f);
   } else if (!strcmp(mode, "stage")) {
     /* prologue of timestep_rk2 (timestep_algorithm.c:13-24), then one substep */
     cell_clear_w(cells, s);
