@@ -22,7 +22,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from disco2_b200 import configs  # noqa: E402
-from oracle import oracle  # noqa: E402
+try:  # run as a script (repo root on the path) or imported by a test (oracle/ on the path)
+    from oracle import oracle  # noqa: E402
+except ImportError:
+    import oracle  # noqa: E402
 
 NSTEPS = 5
 WORKLOADS = {"cbd32": lambda: configs.circumbinary(num_r=32), "kepler24": lambda: configs.kepler_ring(num_r=24)}

@@ -31,7 +31,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from disco2_b200 import configs  # noqa: E402
-from oracle import oracle  # noqa: E402
+try:  # run as a script (repo root on the path) or imported by a test (oracle/ on the path)
+    from oracle import oracle  # noqa: E402
+except ImportError:
+    import oracle  # noqa: E402
 
 NUM_R, NSTEPS, WINDOW = 192, 500, 250
 Q0, ALPHA0 = 1.0, 0.1

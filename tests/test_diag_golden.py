@@ -10,11 +10,10 @@ import tempfile
 import numpy as np
 import pytest
 
-HERE = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.dirname(HERE))
+import oracle
+from disco2_b200 import configs
 
-from disco2_b200 import configs  # noqa: E402
-from oracle import oracle  # noqa: E402
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def test_fixture_shapes():
