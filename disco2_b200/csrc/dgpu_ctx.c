@@ -159,8 +159,6 @@ static int check_supported(const struct dgpu_sim *s, int k, char *err, int n) {
     return snprintf(err, (size_t)n, "disk %d: bad w_analytic_type", k), DGPU_ERR_PARFILE;
   if (s->RiemannSolver != DR_HLLC && s->RiemannSolver != DR_HLL)
     return snprintf(err, (size_t)n, "disk %d: bad RiemannSolver", k), DGPU_ERR_PARFILE;
-  if (s->BoundTypeR == DB_OUTFLOW)
-    return snprintf(err, (size_t)n, "disk %d: outflow radial boundaries are not implemented", k), DGPU_ERR_UNSUPPORTED;
   if (s->GravMassType < 0 || s->GravMassType > 2)
     return snprintf(err, (size_t)n, "disk %d: bad GravMassType", k), DGPU_ERR_PARFILE;
   if (s->BoundTypeR == DB_FIXED || s->DAMP_TIME > 0.0) {
@@ -194,7 +192,7 @@ void dgpu_destroy(dgpu_ctx *c) {
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
                   c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.rr, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
-                  c->d.mdot_part, c->d.counters, c->d.err, c->d_stage, c->d_torque};
+                  c->d.mdot_part, c->d.counters, c->d.err, c->d.obuf, c->d_stage, c->d_torque};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
       if (ps[k]) cudaFree(ps[k]);
   }
@@ -214,7 +212,7 @@ void dgpu_destroy(dgpu_ctx *c) {
 int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dgpu_ctx **out) {
   struct dgpu_ctx *c;
   int k, i, rc, ok = 1;
-  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0;
+  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0, n_ob = 0;
   int *h_cell_ann, *h_slot_ann;
   if (!sims || n < 1 || !out) return fail(NULL, DGPU_ERR_ARG, "bad arguments to dgpu_create");
   for (k = 0; k < n; ++k) {
@@ -257,6 +255,13 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
       dsim_fill_annulus(s, i, a);
       a->inst = k;
       a->cell_off = cells;
+      /* the outflow boundary reads annuli 1 and NR-3 and writes 0, NR-2 and NR-1 */
+      if (s->BoundTypeR == DB_OUTFLOW && (i >= s->NR - 3 || (s->NoInnerBC != 1 && i <= 1))) {
+        a->ob_off = n_ob;
+        n_ob += s->N_p[i];
+      } else {
+        a->ob_off = -1;
+      }
       for (j = 0; j < s->N_p[i]; ++j) h_cell_ann[cells + j] = ann + i;
       cells += s->N_p[i];
       if (i < s->NR - 1) {
@@ -277,6 +282,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   }
   c->n_slots = slots;
   c->n_runs = runs;
+  c->n_ob = n_ob;
   h_slot_ann = (int *)malloc(sizeof(int) * (size_t)(slots > 0 ? slots : 1));
   for (i = 0; i < c->n_ann; ++i) {
     int f;
@@ -350,6 +356,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.mdot_part = (double *)dmalloc(sizeof(double) * 2 * (size_t)c->n_upd_blocks, &ok);
     c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
     c->d.err = (int *)dmalloc(sizeof(int), &ok);
+    if (n_ob > 0) c->d.obuf = (double *)dmalloc(sizeof(double) * 5 * (size_t)n_ob, &ok);
     c->d_stage = (double *)dmalloc(sizeof(double) * 5 * (size_t)maxcells, &ok);
     c->d_torque = (double *)dmalloc(sizeof(double) * ((size_t)maxcells / dgk_block_size() + 8), &ok);
   }
@@ -374,6 +381,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   c->d.n_cells = c->n_cells;
   c->d.n_slots = c->n_slots;
   c->d.n_runs = c->n_runs;
+  c->d.n_ob = c->n_ob;
   c->d.par = c->d_par;
   c->d.ist = c->d_ist;
   c->d.ann = c->d_ann;
@@ -634,6 +642,7 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double
   CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
   if (mode == DCTX_REC) CKK(dgk_update_rec(&c->d, sub, rec, rec_idx, c->stream));
   else CKK(dgk_update(&c->d, t, sub, 7, c->stream));
+  if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
   return DGPU_OK;
 }
 
@@ -658,6 +667,7 @@ int dctx_launch_step(struct dgpu_ctx *c) {
     CK(cudaEventRecord(c->fork[3], c->side));
     CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
     CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
+    if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
   }
   return DGPU_OK;
 }
@@ -712,6 +722,7 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
       CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
+      if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
     }
     CK(cudaEventSynchronize(ev[DGPU_STEP_KERNELS]));
@@ -814,6 +825,7 @@ int dgpu_stage(dgpu_ctx *c, int phase) {
     CKK(dgk_flux_r(&c->d, NULL, 1, c->stream));
   }
   CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
+  if (phase >= 6 && c->n_ob > 0) CKK(dgk_outflow(&c->d, phase, c->stream));
   /* from phase 5 on the advanced phi edges live in the substep's output buffer */
   if (phase >= 5)
     CK(cudaMemcpyAsync(c->d.tiph0, c->d.tiph1, sizeof(double) * (size_t)c->n_cells,

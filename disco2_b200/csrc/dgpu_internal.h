@@ -44,6 +44,8 @@ enum { DR_HLLC, DR_HLL };
 #define DGPU_AK_SINK_SUM 8   /* counted in the Mdot sum (cell_source.c:80-88,181) */
 #define DGPU_AK_IC 16        /* boundary profile ic[] is defined for this annulus */
 #define DGPU_AK_MDOT 32      /* innermost non-ghost annulus: the accretion-rate objective */
+#define DGPU_AK_OUT_DST 64   /* rewritten by the outflow radial boundary (cell_boundary.c:14-139):
+                                k_outflow applies its damping and cell_calc_cons */
 
 /* Per-disk parameters (constant during a run). */
 typedef struct {
@@ -63,6 +65,7 @@ typedef struct {
   int init_type;
   int has_damp;     /* DAMP_TIME > 0 */
   int num_sinks;    /* GravMassType (cell_source.c:177) */
+  int outflow;      /* bit 0: outflow radial boundary; bit 1: also the inner annulus (NoInnerBC != 1) */
   double gamma, plm, cfl, visc, g_eps;
   double rho_floor, cs_floor, cs_cap, vel_cap;
   double t_max, poro_r1, orb_tscale, orb_t0;
@@ -80,7 +83,8 @@ typedef struct {
   int face_cap;
   int run_base;     /* run starts of pair (i, i+1): slab start, capacity */
   int run_cap;
-  int pad;
+  int ob_off;       /* first cell of this annulus in DevPtrs.obuf; -1: the outflow boundary
+                       neither reads nor writes it */
   double rm, rp, r; /* FacePos(i-1), FacePos(i), 0.5*(rp+rm) */
   double dr;        /* rp - rm */
   double dv_half;   /* .5*(rp*rp-rm*rm)   (cell_calc_cons dV factor) */
@@ -146,6 +150,9 @@ typedef struct {
   double *mdot_part;      /* [n_blocks_update][2] per-block sink sums */
   unsigned int *counters; /* last-block counters */
   int *err;               /* error flags */
+  double *obuf;           /* [5][n_ob] prims, before damping, of the annuli the outflow boundary
+                             reads or writes (k_update writes them, k_outflow finishes them) */
+  int n_ob;
   int tune[DGPU_TUNE_N];  /* host-side launch choice of the tuned kernels: resident blocks per SM (0: built-in) */
 } DevPtrs;
 
@@ -206,6 +213,9 @@ int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream);
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream);
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
+/* the outflow radial boundary, its damping and cell_calc_cons on the annuli
+ * it rewrites (one block per disk); after k_update, for stop >= 6 */
+int dgk_outflow(const DevPtrs *d, int stop, void *stream);
 /* k_update recording the conserved sum and new widths into rec (adjoint replay) */
 int dgk_update_rec(const DevPtrs *d, int substep, double *rec, const int *rec_idx, void *stream);
 /* the per-annulus constants of k_source only (ann_c) */

@@ -870,9 +870,16 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
       const double dV = A.dv_half * dphi_n * P.dz;
       T pr[5];
       cons2prim(c, dV, r, P, pr);
-      if (stop >= 6) bc_damp(d, A, a, pr);
+      // the outflow boundary reads these prims before any damping; the
+      // annuli it rewrites are damped and converted by k_outflow
+      if (A.ob_off >= 0 && stop >= 6) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) d.obuf[(size_t)q * d.n_ob + A.ob_off + (g - A.cell_off)] = val(pr[q]);
+      }
+      const bool own = !(A.kind & DGPU_AK_OUT_DST);
+      if (stop >= 6 && own) bc_damp(d, A, a, pr);
       // cell_calc_cons (src/Cell/cell_conversion.c:35-55)
-      if (stop >= 7) prim2cons(pr, c, r, dV, P.gamma);
+      if (stop >= 7 && own) prim2cons(pr, c, r, dV, P.gamma);
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         stq<T>(d.prim, tp.prim, q, N, g, pr[q]);
@@ -966,6 +973,79 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   prim2cons(p, c, r, dV, P.gamma);
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
+}
+
+// One pass of cell_boundary_outflow_r (src/Cell/cell_boundary.c:14-139) over
+// the r faces of annulus pair (i, i+1) of the substep's face list: every cell
+// of the rewritten annulus (i when outer == 0, else i+1) takes the sum, in face
+// order, of prim * dA of the cells across its faces, divided by
+// dz * FacePos(i) * dphi.  The reference's build constants EXTRAP_BC, SS_BCS,
+// diode and KEP_BNDRY are 0 (header.h); its inner term
+// (prim - 0 * grad * (...) / 2.) * dA is prim * dA for a finite slope.  A cell
+// with no face keeps its own value, divided (the reference zeroes only the
+// cells its face loop visits).
+__device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int i, int outer) {
+  const int a = P.ann_base + i + outer;
+  const Annulus &A = d.ann[a];
+  const Annulus &S = d.ann[P.ann_base + i + 1 - outer];  // the annulus read
+  const double rf = d.ann[P.ann_base + i].f_r;           // FacePos(i)
+  const size_t NB = d.n_ob;
+  for (int j = threadIdx.x; j < A.np; j += blockDim.x) {
+    const int g = A.cell_off + j;
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    int nface = 0;
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int side) {
+      if (side != outer) return;
+      const int o = S.ob_off + ((outer ? F.cL : F.cR) - S.cell_off);
+      const double dA = F.r * F.dphi * F.dperp;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) s[q] += d.obuf[q * NB + o] * dA;
+      ++nface;
+    });
+    const double dA = P.dz * rf * d.dphi[g];
+    const size_t self = (size_t)A.ob_off + j;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
+  }
+}
+
+// The outflow radial boundary of one disk per block, in the reference's order:
+// annulus 0 from annulus 1 (unless NoInnerBC == 1), NR-2 from NR-3, NR-1 from
+// the new NR-2; each pass reads the previous one's results.  Then the
+// rewritten annuli get cell_bc_damp and, for stop 7, cell_calc_cons.
+__global__ void __launch_bounds__(BLK) k_outflow(DevPtrs d, int stop) {
+  const DiskParams &P = d.par[blockIdx.x];
+  if (!(P.outflow & 1)) return;
+  const int NR = P.NR, N = d.n_cells;
+  const size_t NB = d.n_ob;
+  if (P.outflow & 2) outflow_pass(d, P, 0, 0);
+  __syncthreads();
+  outflow_pass(d, P, NR - 3, 1);
+  __syncthreads();
+  outflow_pass(d, P, NR - 2, 1);
+  __syncthreads();
+  for (int k = 0; k < 3; ++k) {
+    const int i = k == 0 ? 0 : NR - 3 + k;
+    const int a = P.ann_base + i;
+    const Annulus &A = d.ann[a];
+    if (!(A.kind & DGPU_AK_OUT_DST)) continue;
+    const double r = .5 * (A.rm + A.rp);
+    for (int j = threadIdx.x; j < A.np; j += blockDim.x) {
+      const int g = A.cell_off + j;
+      double pr[5], c[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) pr[q] = d.obuf[q * NB + A.ob_off + j];
+      bc_damp(d, A, a, pr);
+#pragma unroll
+      for (int q = 0; q < 5; ++q) d.prim[(size_t)q * N + g] = pr[q];
+      if (stop >= 7) {
+        const double dV = A.dv_half * d.dphi[g] * P.dz;
+        prim2cons(pr, c, r, dV, P.gamma);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+      }
+    }
+  }
 }
 
 // Torque on the binary: -sum over non-ghost cells of r*rho*dV*F_phi, with the
@@ -1132,6 +1212,11 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
   static const TanPtrs none = {};
   k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop, tail,
                                                                                       nullptr, nullptr);
+  return (int)cudaGetLastError();
+}
+int dgk_outflow(const DevPtrs *d, int stop, void *stream) {
+  if (d->n_ob <= 0 || stop < 6) return 0;
+  k_outflow<<<d->n_inst, BLK, 0, (cudaStream_t)stream>>>(*d, stop);
   return (int)cudaGetLastError();
 }
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream) {

@@ -445,6 +445,7 @@ void dsim_fill_params(const struct dgpu_sim *s, DiskParams *p) {
   p->init_type = s->InitialDataType;
   p->has_damp = s->DAMP_TIME > 0.0;
   p->num_sinks = s->GravMassType;
+  p->outflow = s->BoundTypeR == DB_OUTFLOW ? (1 | (s->NoInnerBC != 1 ? 2 : 0)) : 0;
   p->gamma = s->Adiabatic_Index;
   p->plm = s->PLM;
   p->cfl = s->CFL;
@@ -505,6 +506,10 @@ void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a) {
     if ((s->NoInnerBC != 1 && i < s->ng_min[0]) || (i > NR - s->ng_max[0] - 1))
       a->kind |= DGPU_AK_BC_FIXED;
   }
+  /* cell_boundary_outflow_r rewrites annulus 0 (unless NoInnerBC == 1) and
+   * the last two annuli, whatever the ghost counts (cell_boundary.c:24-138) */
+  if (s->BoundTypeR == DB_OUTFLOW && ((s->NoInnerBC != 1 && i == 0) || i >= NR - 2))
+    a->kind |= DGPU_AK_OUT_DST;
   a->damp_rate = 0.0;
   if (s->DAMP_TIME > 0.0) {
     double R0 = 1. / s->DAMP_TIME / 2. / M_PI;

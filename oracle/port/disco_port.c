@@ -1087,8 +1087,38 @@ static void gm_move(Port *p, double t, double dt) { /* gravMass_move (GravMass_m
   p->gom[1] = omega;
 }
 
+/* cell_boundary_outflow_r (cell_boundary.c:14-139) with the reference's build
+ * constants EXTRAP_BC = SS_BCS = diode = KEP_BNDRY = 0 (header.h): a boundary
+ * cell takes the dA-weighted sum of its neighbours' prims over the r faces of
+ * the substep's face list, divided by dz * r_face * dphi.  The extrapolation
+ * term 0 * grad * (...) / 2 is +-0 for a finite slope, and x - (+-0) == x, so
+ * the inner sum is prim * dA like the outer one.  The inner ghost annulus 0
+ * (unless NoInnerBC == 1) comes from annulus 1; then annulus NR-2 from NR-3,
+ * then NR-1 from the new NR-2 -- also when NR-2 is not a ghost annulus. */
+static void outflow_pair(Port *p, int i, int outer) {
+  int n, q, j;
+  const int dst = outer ? i + 1 : i;
+  const double dz = p->zf[1] - p->zf[0];
+  for (n = p->nri[i]; n < p->nri[i + 1]; ++n)
+    for (q = 0; q < 5; ++q) p->prim[q][outer ? p->fR[n] : p->fL[n]] = 0.0;
+  for (n = p->nri[i]; n < p->nri[i + 1]; ++n) {
+    const int to = outer ? p->fR[n] : p->fL[n], from = outer ? p->fL[n] : p->fR[n];
+    for (q = 0; q < 5; ++q) p->prim[q][to] += p->prim[q][from] * p->fdA[n];
+  }
+  for (j = 0; j < p->N_p[dst]; ++j) {
+    const int g = p->off[dst] + j;
+    const double dA = dz * FP(p, i) * p->dphi[g];
+    for (q = 0; q < 5; ++q) p->prim[q][g] /= dA;
+  }
+}
+
 static void boundary_and_damp(Port *p, double dt) {
   int i, j, q;
+  if (p->BoundTypeR == 1) {
+    if (p->NoInnerBC != 1) outflow_pair(p, 0, 0);
+    outflow_pair(p, p->NR - 3, 1);
+    outflow_pair(p, p->NR - 2, 1);
+  }
   /* cell_boundary_fixed_r (cell_boundary.c:208-231) */
   if (p->BoundTypeR == 0) {
     for (i = 0; i < p->NR; ++i) {

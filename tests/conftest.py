@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-CASES = ("gresho16", "kepler24", "cbd32")
+CASES = ("gresho16", "kepler24", "cbd32", "kepler24out", "cbd32out", "kepler12noin", "kepler1out")
 
 
 def pytest_configure(config):

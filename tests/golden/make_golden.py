@@ -31,6 +31,16 @@ CASES = {
     "gresho16": configs.gresho(num_r=16),
     "kepler24": configs.kepler_ring(num_r=24),
     "cbd32": configs.circumbinary(num_r=32),
+    # outflow radial boundary (cell_boundary_outflow_r): one ghost annulus a
+    # side, so the boundary also overwrites the last non-ghost annulus NR-2
+    "kepler24out": configs.kepler_ring(num_r=24, BoundTypeR=1),
+    # two ghost annuli a side, outer damping zone applied after the boundary
+    "cbd32out": configs.circumbinary(num_r=32, BoundTypeR=1, ng=2),
+    # no inner boundary (annulus 0 reaches the origin): outer boundary only
+    "kepler12noin": configs.kepler_ring(num_r=12, BoundTypeR=1, NoInnerBC=1),
+    # three annuli: annulus 0 is written by the inner boundary and then read
+    # by the outer one, annulus 1 is read by the inner one and then written
+    "kepler1out": configs.kepler_ring(num_r=1, R_Min=1.0, R_Max=1.2, BoundTypeR=1),
 }
 STEPS = (1, 5, 100)
 PHASES = (0, 1, 2, 3, 4, 5, 6, 7)
@@ -111,12 +121,16 @@ def face_cases(par: str, st0: oracle.State, rng: np.random.Generator) -> dict:
     return out
 
 
-def main() -> None:
+def main(names: list[str]) -> None:
+    """Writes the fixtures of the named cases (all cases when none is named);
+    each case draws its face layouts from its own seeded generator."""
     if not oracle.have_ref():
         oracle.build(ref=True, port=False)
-    rng = np.random.default_rng(20251203)
     with tempfile.TemporaryDirectory() as td:
-        for name, p in CASES.items():
+        for k, (name, p) in enumerate(CASES.items()):
+            if names and name not in names:
+                continue
+            rng = np.random.default_rng(20251203 + k)
             par = configs.write_parfile(p, os.path.join(td, name + ".par"))
             data = {"parfile": np.array(configs.parfile_text(p))}
             st0, fc0, _ = oracle.run(par, 0, faces=True)
@@ -144,4 +158,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -154,11 +154,15 @@ def test_adjoint_independent_of_checkpoint_spacing(base):
         assert np.array_equal(st["prim"], out[0][1]["prim"])
 
 
-def test_differentiation_refuses_unsupported():
-    s = lib.Sim(configs.gresho(num_r=16))  # C_RIGID mesh
+@pytest.mark.parametrize("par,msg", [
+    (configs.gresho(num_r=16), "C_RIGID"),
+    (configs.kepler_ring(num_r=16, BoundTypeR=1), "outflow"),
+])
+def test_differentiation_refuses_unsupported(par, msg):
+    s = lib.Sim(par)
     ctx = lib.Context(s)
     ctx.init_state(0)
-    with pytest.raises(lib.DiscoError):
+    with pytest.raises(lib.DiscoError, match=msg):
         ctx.objective(4, 2)
     ctx.close()
 

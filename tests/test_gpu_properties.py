@@ -91,6 +91,65 @@ def test_batched_context_equals_single_disks():
         single.close()
 
 
+def _z_span(sim) -> float:
+    """dz of the single z layer as sim_set_rz computes it (sim_set.c:130-141)."""
+    zs = sim.param("ZLogScale")
+    zmin, zmax = sim.param("Z_Min"), sim.param("Z_Max")
+    sgn = lambda x: (x > 0) - (x < 0)  # noqa: E731
+    z1max = sgn(zmax) * zs * math.log(1.0 + abs(zmax) / zs)
+    z1min = sgn(zmin) * zs * math.log(1.0 + abs(zmin) / zs)
+    zf = [sgn(z1) * zs * (math.exp(abs(z1) / zs) - 1.0)
+          for z1 in (z1min, z1min + (z1max - z1min) / 1.0)]
+    return zf[1] - zf[0]
+
+
+def test_outflow_boundary_full_size():
+    """The outflow radial boundary on the full 256-annulus ring: from the prims
+    after cons2prim (phase 5), the annuli 0, NR-2 and NR-1 after phase 6 are,
+    bit for bit, the dA-weighted sums over the substep's face list divided by
+    dz * FacePos(i) * dphi, computed here in face order; every other annulus
+    is unchanged (no damping zone)."""
+    sim = lib.Sim(configs.kepler_ring(BoundTypeR=1))
+    ctx = lib.Context(sim)
+    ctx.init_state(0)
+    ctx.step(3)
+    st = ctx.get_state(0)
+    f = ctx.face_list(0)
+    ctx.set_state(0, st["prim"], st["tiph"], st["dphi"])
+    ctx.stage(5)
+    p5 = ctx.get_state(0)
+    ctx.set_state(0, st["prim"], st["tiph"], st["dphi"])
+    ctx.stage(6)
+    p6 = ctx.get_state(0)["prim"]
+    N_p, rf = sim.grid()
+    NR = len(N_p)
+    off = np.concatenate([[0], np.cumsum(N_p)])
+    dz = _z_span(sim)
+    want = p5["prim"].copy()
+    nri = list(f["nri"]) + [len(f["L"])]
+
+    def pair(i, outer):
+        dst = i + outer
+        acc = {}
+        for n in range(nri[i], nri[i + 1]):
+            to, frm = (f["R"][n], f["L"][n]) if outer else (f["L"][n], f["R"][n])
+            acc.setdefault(to, [0.0] * 5)
+            for q in range(5):
+                acc[to][q] += float(want[frm, q]) * float(f["dA"][n])
+        for g in range(off[dst], off[dst + 1]):
+            dA = dz * float(rf[i + 1]) * float(p5["dphi"][g])
+            src = acc.get(g, [float(v) for v in want[g]])
+            want[g] = [v / dA for v in src]
+
+    pair(0, 0)
+    pair(NR - 3, 1)
+    pair(NR - 2, 1)
+    assert np.array_equal(p6, want)
+    inner = slice(off[1], off[NR - 2])
+    assert np.array_equal(p6[inner], p5["prim"][inner])
+    ctx.close()
+
+
 def test_batched_sweep_runs():
     """A reduced circumbinary sweep (uneven N_r and N_phi, different q, alpha,
     h/r, outer radius) steps in one context; every disk keeps finite state and

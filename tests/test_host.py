@@ -69,7 +69,7 @@ def test_optional_initial_data_keys_default():
     ({"NumZ": 4}, "NumZ"),
     ({"NUM_N": 1}, "NUM_N"),
     ({"w_numeric_type": 1}, "w_numeric_type"),
-    ({"BoundTypeR": 1}, "outflow"),
+    ({"RiemannSolver": 7}, "RiemannSolver"),
     ({"InitialDataType": 0}, "single-cell"),
 ])
 def test_unsupported_options_refused_before_any_device_work(over, msg):
