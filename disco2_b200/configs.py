@@ -108,10 +108,139 @@ def circumbinary_sweep(n: int = 48, seed: int = 3) -> list[dict]:
     return out
 
 
+# The reference's own test problems (parfiles/code_tests/*.par) and the other
+# initial-data families of src/Cell/initial_data/, as 2-D disks.
+
+def shear_test(num_r: int = 128, **over) -> dict:
+    """Viscous shear layer (SHEAR) on a uniform grid, the settings of
+    parfiles/code_tests/shear.par: outflow radial boundary, cooling on."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 0, "GravMassType": 0, "MassRatio": 0.0, "NumR": num_r, "ng": 2,
+        "R_Min": 1.0, "R_Max": 10.0, "BoundTypeR": 1, "NoInnerBC": 0, "w_numeric_type": 0,
+        "RiemannSolver": 0, "Adiabatic_Index": 1.3333333333333, "Cooling": 1,
+        "Explicit_Viscosity": 0.05, "ViscConst": 1, "RhoSinkOn": 0, "PoRho_r1": 1.0, "CFL": 0.1,
+        "PLM": 1.0, "w_analytic_type": 0, "Grav_2D": 1, "G_EPS": 0.0, "PHI_ORDER": 2,
+        "Rho_Floor": 1.0e-5, "Cs_Floor": 1.0e-4, "Cs_Cap": 100.0, "Vel_Cap": 100.0,
+        "DAMP_TIME": -1.0, "RLogScale": 1.0e6, "ZLogScale": 1.0e6, "HiResSigma": 1.0e6,
+        "HiResR0a": 1.0e6, "HiResR0b": 1.0e6, "HiResFac": 0.0,
+    })
+    p.update(over)
+    return p
+
+
+def sstest(num_r: int = 128, **over) -> dict:
+    """Shakura-Sunyaev disk around a point mass (SSTEST), the settings of
+    parfiles/code_tests/SStest.par: two cells per annulus, log grid, no inner
+    boundary, outflow, cooling, sink and a damping zone."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 2, "GravMassType": 1, "MassRatio": 0.0, "NumR": num_r, "ng": 2,
+        "R_Min": 0.05, "R_Max": 100.0, "NP_CONST": 2, "NPCAP": 2, "BoundTypeR": 1,
+        "NoInnerBC": 1, "w_numeric_type": 0, "RiemannSolver": 0, "Cooling": 1,
+        "Explicit_Viscosity": 0.1, "ViscConst": 0, "RhoSinkOn": 1, "PoRho_r1": 0.01, "CFL": 0.1,
+        "PLM": 1.0, "w_analytic_type": 1, "Grav_2D": 1, "G_EPS": 0.0, "PHI_ORDER": 2,
+        "Rho_Floor": 1.0e-6, "Cs_Floor": 1.0e-5, "Cs_Cap": 1.0, "Vel_Cap": 10.0,
+        "DAMP_TIME": 0.001, "RDAMP_INNER": 0.0, "RDAMP_OUTER": 90.0, "RLogScale": 1.0,
+        "ZLogScale": 1000.0, "HiResSigma": 1.0e4, "HiResR0a": 1.0e5, "HiResR0b": 1.0e5,
+        "HiResFac": 0.0,
+    })
+    p.update(over)
+    return p
+
+
+def vortex_test(num_r: int = 64, **over) -> dict:
+    """Isentropic vortex (VORTEX) on the rigidly rotating mesh, the settings of
+    parfiles/code_tests/vortex.par without its passive scalar (NUM_N 0)."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 1, "GravMassType": 0, "MassRatio": 1.0, "NumR": num_r, "ng": 2,
+        "R_Min": 0.015, "R_Max": 0.9, "BoundTypeR": 0, "NoInnerBC": 1, "w_numeric_type": 2,
+        "RiemannSolver": 0, "Cooling": 0, "Explicit_Viscosity": -1.0, "ViscConst": 0,
+        "RhoSinkOn": 0, "PoRho_r1": 1.0, "CFL": 0.5, "PLM": 1.0, "w_analytic_type": 0,
+        "Rho_Floor": 1.0e-5, "Cs_Floor": 1.0e-4, "Cs_Cap": 100.0, "Vel_Cap": 100.0,
+        "DAMP_TIME": -1.0e-5, "RLogScale": 1.0e5, "ZLogScale": 1.0e5, "HiResSigma": 1.0e5,
+        "HiResR0a": 1.0e5, "HiResR0b": 1.0e5, "HiResFac": 0.0,
+    })
+    p.update(over)
+    return p
+
+
+def torus_2d(num_r: int = 80, **over) -> dict:
+    """Constant-angular-momentum torus (TORUS) in the midplane: the settings of
+    parfiles/torus.par with one z layer (the reference parfile is 3-D)."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 3, "GravMassType": 1, "MassRatio": 0.0, "NumR": num_r, "ng": 2,
+        "R_Min": 0.2, "R_Max": 3.0, "NPCAP": 20, "BoundTypeR": 1, "NoInnerBC": 0,
+        "w_numeric_type": 6, "RiemannSolver": 0, "Cooling": 0, "Explicit_Viscosity": -1.0,
+        "PoRho_r1": 1.0, "CFL": 0.5, "PLM": 1.0, "w_analytic_type": 4, "Grav_2D": 0,
+        "G_EPS": 0.1, "PHI_ORDER": 2, "Rho_Floor": 1.0e-7, "Cs_Floor": 1.0e-6, "Cs_Cap": 2.0,
+        "Vel_Cap": 2.0, "DAMP_TIME": -1.0, "RLogScale": 1.0e4, "ZLogScale": 1.0e4,
+        "HiResSigma": 1.0e4, "HiResR0a": 1.0e4, "HiResR0b": 1.0e4, "HiResFac": 0.0,
+    })
+    p.update(over)
+    return p
+
+
+def milos_macfadyen(num_r: int = 128, **over) -> dict:
+    """Circumbinary disk of MacFadyen & Milosavljevic (MILOS_MACFADYEN): binary,
+    Keplerian mesh, no inner boundary, outflow, an outer damping zone."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 4, "GravMassType": 2, "MassRatio": 1.0, "NumR": num_r, "ng": 2,
+        "R_Min": 0.5, "R_Max": 20.0, "BoundTypeR": 1, "NoInnerBC": 1, "w_numeric_type": 3,
+        "RiemannSolver": 0, "Adiabatic_Index": 1.001, "Explicit_Viscosity": 0.1, "ViscConst": 0,
+        "PoRho_r1": 0.01, "CFL": 0.5, "PLM": 1.0, "w_analytic_type": 0, "G_EPS": 0.05,
+        "PHI_ORDER": 4, "Rho_Floor": 1.0e-6, "Cs_Floor": 1.0e-5, "Cs_Cap": 1.0, "Vel_Cap": 10.0,
+        "DAMP_TIME": 1.0, "RDAMP_INNER": 0.0, "RDAMP_OUTER": 16.0, "RLogScale": 5.0,
+    })
+    p.update(over)
+    return p
+
+
+def rad_dom(num_r: int = 128, **over) -> dict:
+    """Radiation-dominated alpha disk (RAD_DOM) around a point mass, fixed
+    radial boundaries."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 5, "GravMassType": 1, "MassRatio": 0.0, "NumR": num_r, "ng": 2,
+        "R_Min": 1.0, "R_Max": 20.0, "BoundTypeR": 0, "w_numeric_type": 0, "RiemannSolver": 1,
+        "Explicit_Viscosity": 0.1, "ViscConst": 0, "PoRho_r1": 0.01, "CFL": 0.4,
+        "w_analytic_type": 1, "Rho_Floor": 1.0e-6, "Cs_Floor": 1.0e-5, "Cs_Cap": 10.0,
+        "Vel_Cap": 10.0, "RLogScale": 1.0,
+    })
+    p.update(over)
+    return p
+
+
+def middle(num_r: int = 128, **over) -> dict:
+    """Alpha disk with a central cavity (MIDDLE) around a point mass, outflow
+    radial boundary and an outer damping zone."""
+    p = dict(_BASE)
+    p.update({
+        "InitialDataType": 6, "GravMassType": 1, "MassRatio": 0.0, "NumR": num_r, "ng": 2,
+        "R_Min": 0.5, "R_Max": 10.0, "BoundTypeR": 1, "NoInnerBC": 0, "w_numeric_type": 0,
+        "RiemannSolver": 0, "Explicit_Viscosity": 0.1, "ViscConst": 0, "PoRho_r1": 0.01,
+        "CFL": 0.4, "w_analytic_type": 1, "Rho_Floor": 1.0e-6, "Cs_Floor": 1.0e-5,
+        "Cs_Cap": 1.0, "Vel_Cap": 10.0, "DAMP_TIME": 1.0, "RDAMP_INNER": 0.0, "RDAMP_OUTER": 8.0,
+        "RLogScale": 1.0,
+    })
+    p.update(over)
+    return p
+
+
 WORKLOADS = {
     "gresho": gresho,
     "kepler_ring": kepler_ring,
     "circumbinary": circumbinary,
+    "shear": shear_test,
+    "sstest": sstest,
+    "vortex": vortex_test,
+    "torus": torus_2d,
+    "milos_macfadyen": milos_macfadyen,
+    "rad_dom": rad_dom,
+    "middle": middle,
 }
 
 

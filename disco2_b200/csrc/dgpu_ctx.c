@@ -8,6 +8,7 @@
  * once into a CUDA graph and replayed; no host synchronisation happens inside
  * a step (dt, t and the GravMass orbit live on the device).
  */
+#define _DEFAULT_SOURCE
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -125,19 +126,25 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
     return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
   }
   dsim_initial_tiph(s, t, d);
-  rc = DGPU_OK;
-  if (prim) {
+  /* the reference sets the GravMasses up before the gas (main.c:95-96); the
+   * initialisers leave every phi in [0, 2pi], so gravMass_clean_pi after the
+   * gas changes nothing the gas could have read */
+  rc = dsim_initial_gravmass(s, g);
+  if (rc != DGPU_OK) rc = fail(NULL, rc, "bad GravMassType");
+  else if (gm) memcpy(gm, g, sizeof(g));
+  if (rc == DGPU_OK && prim) {
+    /* cell_init_torus re-seeds rand() with srand(666 + rank) */
+    struct random_data rd;
+    char state[128];
+    memset(&rd, 0, sizeof(rd));
+    memset(state, 0, sizeof(state));
+    initstate_r(666, state, sizeof(state), &rd);
     for (i = 0; i < s->NR && rc == DGPU_OK; ++i)
       for (j = 0; j < s->N_p[i]; ++j, ++idx)
-        if (dsim_grid_init(s, i, idx, prim + 5 * idx) != 0) {
+        if (dsim_grid_init(s, i, idx, t[idx], d[idx], g, &rd, prim + 5 * idx) != 0) {
           rc = fail(NULL, DGPU_ERR_UNSUPPORTED, "InitialDataType %d has no whole-grid initialiser here", s->InitialDataType);
           break;
         }
-  }
-  if (rc == DGPU_OK) {
-    rc = dsim_initial_gravmass(s, g);
-    if (rc != DGPU_OK) rc = fail(NULL, rc, "bad GravMassType");
-    else if (gm) memcpy(gm, g, sizeof(g));
   }
   if (t != tiph) free(t);
   if (d != dphi) free(d);

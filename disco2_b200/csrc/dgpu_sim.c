@@ -346,6 +346,53 @@ static void newic_profile(const struct dgpu_sim *s, int i, double *prim) {
   prim[D_UZZ] = 0.0;
 }
 
+/* The radiation-dominated disk of cell_init_rad_dom.c:13-76 (single-cell and
+ * whole-grid forms give the same values: omega - 1/r^1.5 and
+ * omega - sqrt(1)/r^1.5 round alike; the file's global `blah` is 0). */
+static void rad_dom_profile(const struct dgpu_sim *s, double r, double *prim) {
+  const double blah = 0.0;
+  double xi = 0.005, a_o_M = 100;
+  double alpha = s->Explicit_Viscosity;
+  double gam = s->Adiabatic_Index;
+  double rho0 = 2. / (9. * xi * alpha * gam) * sqrt(a_o_M);
+  double P0 = 8. * xi / (9. * alpha * gam) * sqrt(a_o_M);
+  double rho = rho0 * pow(r, 1.5);
+  double P = P0 * pow(r, -1.5);
+  double o2 = 1. / r / r / r - 3. / 2. * P / rho / r / r;
+  double omega = sqrt(o2);
+  double vr = -1.5 * alpha * gam * (P / rho) * sqrt(r) - blah * pow(r, -4.5);
+  prim[D_RHO] = rho;
+  prim[D_PPP] = P;
+  prim[D_URR] = vr;
+  prim[D_UPP] = omega - 1. / pow(r, 1.5);
+  prim[D_UZZ] = 0.0;
+}
+
+/* The disk of cell_init_middle.c:12-91; the whole-grid form (grid = 1) also
+ * zeroes v_r inside r = 1. */
+static void middle_profile(const struct dgpu_sim *s, double r, int grid, double *prim) {
+  const int w_idx = 8; /* w_a_milos_index (header.h) */
+  double alpha = s->Explicit_Viscosity;
+  double r0 = 2.5;
+  int d = 10;
+  double rho = pow(r, -3. / 5.) * exp(-pow(r / r0, -d));
+  double P = s->PoRho_r1 * pow(r, -3. / 2.) * exp(-pow(r / r0, -d));
+  double r_drP_o_P = -1.5 + d * pow(r / r0, -d);
+  double o2, omega, a = 1.0, vr;
+  if (rho < 1.e-3) rho = 1.e-3;
+  if (P < 1.e-6) P = 1.e-6;
+  o2 = 1. / r / r / r * pow(1. + 3. / 16. / r / r, 2) + r_drP_o_P * P / rho / r / r;
+  omega = sqrt(o2);
+  omega = (pow(r, w_idx) * omega + pow(a, w_idx - 1.5)) / (pow(r, w_idx) + pow(a, w_idx));
+  vr = -3. * alpha / r / omega * P / rho * (2. + r_drP_o_P);
+  if (grid && r < 1.) vr = 0.0;
+  prim[D_RHO] = rho;
+  prim[D_PPP] = P;
+  prim[D_URR] = vr;
+  prim[D_UPP] = omega - dsim_rOm_a(s, r, a) / r;
+  prim[D_UZZ] = 0.0;
+}
+
 int dsim_single_init(const struct dgpu_sim *s, int i, double *prim) {
   double rm = dsim_rface(s, i - 1);
   double rp = dsim_rface(s, i);
@@ -387,7 +434,32 @@ int dsim_single_init(const struct dgpu_sim *s, int i, double *prim) {
       prim[D_UZZ] = 0.0;
       return 1;
     }
+    case DI_MILOS_MACFADYEN: {
+      /* cell_single_init_milos_macfadyen
+       * (src/Cell/initial_data/cell_init_milos_macfadyen.c:11-36) */
+      double Mach = 1. / sqrt(s->PoRho_r1);
+      double gam = s->Adiabatic_Index;
+      double rho0 = 1.0, rs = 10., delta_exp = 3.0, xi_exp = 2.0;
+      double rho = rho0 * (pow(rs / r, delta_exp)) * exp(-pow(rs / r, xi_exp));
+      double PoRho = 1. / Mach / Mach / gam;
+      prim[D_RHO] = rho;
+      prim[D_PPP] = PoRho * rho;
+      prim[D_URR] = 0.0;
+      prim[D_UPP] = 0.0;
+      prim[D_UZZ] = 0.0;
+      return 1;
+    }
+    case DI_RAD_DOM:
+      /* cell_single_init_rad_dom (src/Cell/initial_data/cell_init_rad_dom.c:13-36) */
+      rad_dom_profile(s, r, prim);
+      return 1;
+    case DI_MIDDLE:
+      /* cell_single_init_middle (src/Cell/initial_data/cell_init_middle.c:12-45) */
+      middle_profile(s, r, 0, prim);
+      return 1;
     default:
+      /* SHEAR: the profile depends on the cell's phi; TORUS: the reference
+       * exits (cell_init_torus.c:12-15) */
       return -1;
   }
 }
@@ -402,11 +474,125 @@ static double noise_u(int seed, long idx) {
   return 2.0 * ((double)(z >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
 }
 
-int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double *prim) {
+/* gravMass_dist (src/GravMass/GravMass_access.c:25-31) on gm[2][6]. */
+static double gm_dist(const double *gm, int p, double r, double phi, double z) {
+  double xbh = gm[6 * p] * cos(gm[6 * p + 1]);
+  double ybh = gm[6 * p] * sin(gm[6 * p + 1]);
+  double x = r * cos(phi);
+  double y = r * sin(phi);
+  return sqrt((x - xbh) * (x - xbh) + (y - ybh) * (y - ybh) + z * z);
+}
+
+int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, double dphi, const double *gm,
+                   struct random_data *rnd, double *prim) {
   double rm = dsim_rface(s, i - 1);
   double rp = dsim_rface(s, i);
   double r = 0.5 * (rm + rp);
   int t = s->InitialDataType;
+  if (t == DI_SHEAR) {
+    /* cell_init_shear (src/Cell/initial_data/cell_init_shear.c:57-116) */
+    double rho = 1.0, Pp = 0.01, v0 = 1.0, t0 = 0.25;
+    double ph = tiph - .5 * dphi;
+    double x = r * cos(ph) - 3.;
+    double y = r * sin(ph);
+    double nu = s->Explicit_Viscosity > 0.0 ? s->Explicit_Viscosity : 0.05;
+    double vy = 0.0, omega;
+    if (fabs(y) < 50.) vy = v0 / sqrt(2. * M_PI * nu * t0) * exp(-x * x / (4. * nu * t0));
+    omega = vy * cos(ph) / r;
+    prim[D_RHO] = rho;
+    prim[D_PPP] = Pp;
+    prim[D_URR] = vy * sin(ph);
+    prim[D_UPP] = omega - dsim_rOm_a(s, r, 1.) / r;
+    prim[D_UZZ] = 0.0;
+    return 0;
+  }
+  if (t == DI_TORUS) {
+    /* cell_init_torus (src/Cell/initial_data/cell_init_torus.c:17-89) for the
+     * single z layer (z = 0); one rand() per cell after srand(666).  The
+     * magnetic terms of the file are never stored, and its Pp = rho branch
+     * follows a clamp that already holds PoRho >= 1e-5, so neither is here. */
+    double gam = s->Adiabatic_Index, M = 1.0, r_inner = 0.7, r_max = 1.0, q = 2.;
+    double sx = 2. * q - q;
+    double GammaFac = (gam - 1.) / gam;
+    double Phi_inner = -1.0 / r_inner, Phi_max = -1.0 / r_max;
+    double Rho_norm = pow(GammaFac * (Phi_inner - Phi_max + pow(r_inner, -sx) / sx - pow(1.0, -sx) / sx), 1.0 / (gam - 1.0));
+    double z = 0.0;
+    double R = sqrt(r * r + z * z);
+    double Phi = -M / R;
+    double omega = pow(r, -q);
+    double PoRho = GammaFac * (Phi_inner - Phi + pow(r_inner, -sx) / sx - pow(r, -sx) / sx);
+    double rho, Pp, delta;
+    int32_t v;
+    if (PoRho < 1.0e-5) PoRho = 1.0e-5;
+    rho = pow(PoRho, 1.0 / (gam - 1.0)) / Rho_norm;
+    Pp = pow(PoRho, 1.0 / GammaFac) / Rho_norm;
+    random_r(rnd, &v);
+    delta = .02 * ((double)v / (double)RAND_MAX - .5);
+    prim[D_RHO] = rho;
+    prim[D_PPP] = Pp;
+    prim[D_URR] = 0.0;
+    prim[D_UPP] = omega * (1. + delta) - pow(r, -2.);
+    prim[D_UZZ] = 0.0;
+    return 0;
+  }
+  if (t == DI_MILOS_MACFADYEN) {
+    /* cell_init_milos_macfadyen (src/Cell/initial_data/cell_init_milos_macfadyen.c:38-151) */
+    double rs = 10.0, rho0 = 1.0, Mach = 1. / sqrt(s->PoRho_r1);
+    double delta_exp = 3.0, xi_exp = 2.0, gam = s->Adiabatic_Index;
+    double cp = 1. / Mach, fac = 0.0001, Mtotal = 1.0, sep = 1.0, massratio = s->MassRatio;
+    double M0, M1, r0, r1, eps0, eps1, alpha = s->Explicit_Viscosity;
+    double cs, ph, d0, d1, cs0, cs1, PoRho, Pot1, Pot2, rho, omega, O2, vr, Pp;
+    int n = s->PHI_ORDER;
+    if (fabs(massratio) > 1.e-8) {
+      M0 = Mtotal / (1. + massratio);
+      M1 = Mtotal / (1. + 1. / massratio);
+      r0 = M1 / Mtotal * sep;
+      r1 = M0 / Mtotal * sep;
+    } else {
+      M0 = 1.0;
+      M1 = 0.0;
+      r0 = 0.0;
+      r1 = 0.0;
+    }
+    eps0 = s->G_EPS * r0;
+    eps1 = s->G_EPS * r1;
+    cs = r < 1. ? 1. / Mach : sqrt(1. / r) / Mach;
+    ph = tiph - 0.5 * dphi;
+    d0 = gm_dist(gm, 0, r, ph, 0.);
+    d1 = gm_dist(gm, 1, r, ph, 0.);
+    cs0 = d0 < 0.5 ? sqrt(1. / .5) / Mach * sqrt(M0) : sqrt(1. / d0) / Mach * sqrt(M0);
+    cs1 = d1 < 0.5 ? sqrt(1. / .5) / Mach * sqrt(M1) : sqrt(1. / d1) / Mach * sqrt(M1);
+    PoRho = (cs0 * cs0 + cs1 * cs1) / gam;
+    Pot1 = M0 / pow(pow(d0, n) + pow(eps0, n), 1. / n);
+    Pot2 = M1 / pow(pow(d1, n) + pow(eps1, n), 1. / n);
+    rho = rho0 * (pow(rs / r, delta_exp)) * exp(-pow(rs / r, xi_exp));
+    omega = sqrt(1.) / pow(r, 1.5);
+    omega *= 1. + 3. / 16. / r / r;
+    O2 = omega * omega + cs * cs / r / r * (2. * rs * rs / r / r - 3.);
+    if (r < 3.0) {
+      omega = 1. / pow(r, 1.5);
+      vr = 0.0;
+    } else {
+      omega = sqrt(O2);
+      vr = -3.0 / sqrt(r) * alpha * (1.0 / Mach) * (1.0 / Mach) * (1.0 - delta_exp + xi_exp * pow(r / rs, -xi_exp));
+    }
+    if (rho < (100. * s->Rho_Floor)) rho = 100. * s->Rho_Floor;
+    Pp = PoRho * rho;
+    prim[D_RHO] = rho * exp(fac * (Pot1 + Pot2) / cp / cp);
+    prim[D_PPP] = Pp * exp(fac * (Pot1 + Pot2) / cp / cp);
+    prim[D_URR] = vr;
+    prim[D_UPP] = omega - sqrt(1.) / pow(r, 1.5);
+    prim[D_UZZ] = 0.0;
+    return 0;
+  }
+  if (t == DI_RAD_DOM) {
+    rad_dom_profile(s, r, prim);
+    return 0;
+  }
+  if (t == DI_MIDDLE) {
+    middle_profile(s, r, 1, prim);
+    return 0;
+  }
   if (t == DI_GRESHO || t == DI_KEPLER_RING || t == DI_CIRCUMBINARY) {
     double f = 1. + s->IC_Noise * noise_u(s->IC_Seed, idx);
     newic_profile(s, i, prim);

@@ -62,9 +62,15 @@ double dsim_dtOm_a(const struct dgpu_sim *s, double r, double a);
  * initial data type has no axisymmetric single-cell form here. */
 int dsim_single_init(const struct dgpu_sim *s, int i, double *prim);
 
-/* Whole-grid initial data for cell j of annulus i with global (k,i,j) cell
- * number idx (noise included).  Returns 0 or -1 (unsupported type). */
-int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double *prim);
+/* Whole-grid initial data (cell_init_*) for cell j of annulus i with global
+ * (k,i,j) cell number idx (noise included).  tiph, dphi: the cell's phi edge
+ * and width after cell_create and cell_clean_pi; gm: the GravMass state
+ * (dsim_initial_gravmass); rnd: the generator of cell_init_torus, seeded like
+ * srand(666), drawn once per cell for that type only.  Returns 0 or -1
+ * (unsupported type). */
+struct random_data;
+int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, double dphi, const double *gm,
+                   struct random_data *rnd, double *prim);
 
 /* Fill the per-annulus table entries that depend only on the Sim. */
 void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a);

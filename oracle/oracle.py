@@ -19,6 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "disco_ref")
 PORT_BIN = os.path.join(HERE, "_build", "disco_port")
 PORT_LIB = os.path.join(HERE, "_build", "libdisco_port.so")
+# the restatement built with every libm result in the step moved by one ulp
+# (the sensitivity of a case to last-ulp differences; tests only)
+PORT_ULP_BIN = os.path.join(HERE, "_build", "disco_port_ulp")
 REFSRC = "/root/reference/src"
 
 
@@ -39,6 +42,14 @@ def have_ref() -> bool:
 
 def have_port() -> bool:
     return os.path.exists(PORT_BIN)
+
+
+def _exe(impl: str) -> str:
+    return {"ref": REF_BIN, "port": PORT_BIN, "port_ulp": PORT_ULP_BIN}[impl]
+
+
+def build_port_ulp() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "port-ulp"], check=True)
 
 
 @dataclass
@@ -142,7 +153,7 @@ def read_faces(path: str) -> Faces:
 def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = None,
         faces: bool = False, dtlog: bool = False, workdir: str | None = None):
     """Run `nsteps` RK2 steps; returns (final State, Faces|None, dt log array|None)."""
-    exe = REF_BIN if impl == "ref" else PORT_BIN
+    exe = _exe(impl)
     if not os.path.exists(exe):
         raise FileNotFoundError(f"oracle binary missing: {exe} (run oracle.build())")
     with tempfile.TemporaryDirectory(dir=workdir) as td:
@@ -167,7 +178,7 @@ def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = No
 
 def stage(parfile: str, phase: int, *, impl: str = "ref", load: State | None = None) -> State:
     """Run the prologue of one RK2 step and the first substep up to `phase`."""
-    exe = REF_BIN if impl == "ref" else PORT_BIN
+    exe = _exe(impl)
     with tempfile.TemporaryDirectory() as td:
         out = os.path.join(td, "out.bin")
         cmd = [exe, "stage", parfile, str(phase), out]

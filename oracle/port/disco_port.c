@@ -28,6 +28,29 @@ enum { HLLC, HLL };
 
 static double FP(const Port *p, int i) { return p->rf[i + 1]; } /* sim_FacePos(i, R_DIR) */
 
+#ifdef PORT_ULP_NOISE
+/* Sensitivity build (tests only, a separate binary): once the first substep
+ * starts, every libm result moves one ulp up or down, pseudo-randomly.  The
+ * spread this causes is the part of a case's result that any implementation
+ * whose transcendentals differ in the last ulp (the GPU's device libm) cannot
+ * pin down; the grid and the initial data are left exact. */
+static int ulp_on = 0;
+static unsigned long long ulp_state = 0x9E3779B97F4A7C15ULL;
+static double ulp_noise(double x) {
+  if (!ulp_on || !isfinite(x) || x == 0.0) return x;
+  ulp_state = ulp_state * 6364136223846793005ULL + 1442695040888963407ULL;
+  return (ulp_state >> 63) ? nextafter(x, INFINITY) : nextafter(x, -INFINITY);
+}
+#define pow(a, b) ulp_noise(pow(a, b))
+#define exp(a) ulp_noise(exp(a))
+#define log(a) ulp_noise(log(a))
+#define sin(a) ulp_noise(sin(a))
+#define cos(a) ulp_noise(cos(a))
+#define ULP_NOISE_START() (ulp_on = 1)
+#else
+#define ULP_NOISE_START() ((void)0)
+#endif
+
 /* ---------------- parfile (readvar, src/Sim/sim_readpar.c:10-46) ---------------- */
 static int readvar(const char *file, const char *name, double *out) {
   FILE *f = fopen(file, "r");
@@ -218,6 +241,22 @@ static double noise_u(int seed, long idx) {
   return 2.0 * ((double)(z >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
 }
 
+/* cell_init_middle.c:12-91; grid != 0: the whole-grid form (v_r = 0 inside r = 1) */
+static void middle(const Port *p, double r, int grid, double *prim) {
+  double r0 = 2.5, a = 1.0, al = p->Explicit_Viscosity;
+  int d = 10;
+  double rh = pow(r, -3. / 5.) * exp(-pow(r / r0, -d));
+  double Pq = p->PoRho_r1 * pow(r, -3. / 2.) * exp(-pow(r / r0, -d));
+  double rdp = -1.5 + d * pow(r / r0, -d), om, vr;
+  if (rh < 1.e-3) rh = 1.e-3;
+  if (Pq < 1.e-6) Pq = 1.e-6;
+  om = sqrt(1. / r / r / r * pow(1. + 3. / 16. / r / r, 2) + rdp * Pq / rh / r / r);
+  om = (pow(r, WA_MILOS) * om + pow(a, WA_MILOS - 1.5)) / (pow(r, WA_MILOS) + pow(a, WA_MILOS));
+  vr = -3. * al / r / om * Pq / rh * (2. + rdp);
+  if (grid && r < 1.) vr = 0.0;
+  prim[RHO] = rh; prim[PPP] = Pq; prim[URR] = vr; prim[UPP] = om - rOm_a(p, r, a) / r; prim[UZZ] = 0.0;
+}
+
 /* single-cell initial data of annulus i: 1 = set, 0 = left unchanged */
 static int single_init(const Port *p, int i, double *prim) {
   double rm = FP(p, i - 1), rp = FP(p, i);
@@ -244,6 +283,25 @@ static int single_init(const Port *p, int i, double *prim) {
       prim[UPP] = pow(r, -1.5) - rOm_a(p, r, a) / r; prim[UZZ] = 0.0;
       return 1;
     }
+    case MILOS_MACFADYEN: { /* cell_single_init_milos_macfadyen, initial_data/cell_init_milos_macfadyen.c:11-36 */
+      double Mach = 1. / sqrt(p->PoRho_r1), rs = 10.;
+      double rh = 1.0 * (pow(rs / r, 3.0)) * exp(-pow(rs / r, 2.0));
+      prim[RHO] = rh; prim[PPP] = 1. / Mach / Mach / gam * rh; prim[URR] = 0.0; prim[UPP] = 0.0; prim[UZZ] = 0.0;
+      return 1;
+    }
+    case RAD_DOM: { /* cell_single_init_rad_dom, initial_data/cell_init_rad_dom.c:13-36 */
+      double xi = 0.005, aM = 100., al = p->Explicit_Viscosity, zero = 0.0;
+      double rho0 = 2. / (9. * xi * al * gam) * sqrt(aM), P0 = 8. * xi / (9. * al * gam) * sqrt(aM);
+      double rh = rho0 * pow(r, 1.5), Pq = P0 * pow(r, -1.5);
+      double om = sqrt(1. / r / r / r - 3. / 2. * Pq / rh / r / r);
+      prim[RHO] = rh; prim[PPP] = Pq;
+      prim[URR] = -1.5 * al * gam * (Pq / rh) * sqrt(r) - zero * pow(r, -4.5);
+      prim[UPP] = om - 1. / pow(r, 1.5); prim[UZZ] = 0.0;
+      return 1;
+    }
+    case MIDDLE: /* cell_single_init_middle, initial_data/cell_init_middle.c:12-45 */
+      middle(p, r, 0, prim);
+      return 1;
     case GRESHO:
       rho = 1.0;
       if (r < 0.2) { vphi = 5. * r; P = 5. + 12.5 * r * r; }
@@ -271,6 +329,75 @@ static int single_init(const Port *p, int i, double *prim) {
   prim[RHO] = rho; prim[PPP] = P; prim[URR] = 0.0;
   prim[UPP] = vphi / r - rOm_a(p, r, 1.) / r; prim[UZZ] = 0.0;
   return 1;
+}
+
+/* gravMass_dist (GravMass/GravMass_access.c:25-31) */
+static double bh_dist(const Port *p, int k, double r, double phi) {
+  double xb = p->gr[k] * cos(p->gphi[k]), yb = p->gr[k] * sin(p->gphi[k]);
+  double x = r * cos(phi), y = r * sin(phi);
+  return sqrt((x - xb) * (x - xb) + (y - yb) * (y - yb) + 0. * 0.);
+}
+
+/* whole-grid initial data that differs from the single-cell form, for cell g
+ * of annulus i: 1 = set here, 0 = use single_init */
+static int grid_cell(const Port *p, int i, int g, double *prim) {
+  double r = 0.5 * (FP(p, i - 1) + FP(p, i)), gam = p->Adiabatic_Index;
+  double ph = p->tiph[g] - .5 * p->dphi[g];
+  switch (p->InitialDataType) {
+    case SHEAR: { /* cell_init_shear, initial_data/cell_init_shear.c:57-116 */
+      double nu = p->Explicit_Viscosity > 0.0 ? p->Explicit_Viscosity : 0.05, t0 = 0.25, vy = 0.0;
+      double x = r * cos(ph) - 3., y = r * sin(ph);
+      if (fabs(y) < 50.) vy = 1.0 / sqrt(2. * M_PI * nu * t0) * exp(-x * x / (4. * nu * t0));
+      prim[RHO] = 1.0; prim[PPP] = 0.01; prim[URR] = vy * sin(ph);
+      prim[UPP] = vy * cos(ph) / r - rOm_a(p, r, 1.) / r; prim[UZZ] = 0.0;
+      return 1;
+    }
+    case TORUS: { /* cell_init_torus, initial_data/cell_init_torus.c:17-89, z = 0 */
+      double q = 2., sx = 2. * q - q, gf = (gam - 1.) / gam, ri = 0.7;
+      double norm = pow(gf * (-1.0 / ri - -1.0 / 1.0 + pow(ri, -sx) / sx - pow(1.0, -sx) / sx), 1.0 / (gam - 1.0));
+      double pr = gf * (-1.0 / ri - -1.0 / sqrt(r * r + 0.0 * 0.0) + pow(ri, -sx) / sx - pow(r, -sx) / sx);
+      double delta;
+      if (pr < 1.0e-5) pr = 1.0e-5;
+      delta = .02 * ((double)rand() / (double)RAND_MAX - .5);
+      prim[RHO] = pow(pr, 1.0 / (gam - 1.0)) / norm; prim[PPP] = pow(pr, 1.0 / gf) / norm;
+      prim[URR] = 0.0; prim[UPP] = pow(r, -q) * (1. + delta) - pow(r, -2.); prim[UZZ] = 0.0;
+      return 1;
+    }
+    case MILOS_MACFADYEN: { /* cell_init_milos_macfadyen, initial_data/cell_init_milos_macfadyen.c:38-151 */
+      double rs = 10.0, Mach = 1. / sqrt(p->PoRho_r1), cp = 1. / Mach, mr = p->MassRatio;
+      double M0 = 1.0, M1 = 0.0, r0 = 0.0, r1 = 0.0, cs, d0, d1, c0, c1, pot, rh, om, vr;
+      int n = p->PHI_ORDER;
+      if (fabs(mr) > 1.e-8) {
+        M0 = 1.0 / (1. + mr); M1 = 1.0 / (1. + 1. / mr);
+        r0 = M1 / 1.0 * 1.0; r1 = M0 / 1.0 * 1.0;
+      }
+      cs = r < 1. ? 1. / Mach : sqrt(1. / r) / Mach;
+      d0 = bh_dist(p, 0, r, ph);
+      d1 = bh_dist(p, 1, r, ph);
+      c0 = (d0 < 0.5 ? sqrt(1. / .5) : sqrt(1. / d0)) / Mach * sqrt(M0);
+      c1 = (d1 < 0.5 ? sqrt(1. / .5) : sqrt(1. / d1)) / Mach * sqrt(M1);
+      pot = M0 / pow(pow(d0, n) + pow(p->G_EPS * r0, n), 1. / n) + M1 / pow(pow(d1, n) + pow(p->G_EPS * r1, n), 1. / n);
+      rh = 1.0 * (pow(rs / r, 3.0)) * exp(-pow(rs / r, 2.0));
+      om = sqrt(1.) / pow(r, 1.5) * (1. + 3. / 16. / r / r);
+      if (r < 3.0) {
+        om = 1. / pow(r, 1.5);
+        vr = 0.0;
+      } else {
+        om = sqrt(om * om + cs * cs / r / r * (2. * rs * rs / r / r - 3.));
+        vr = -3.0 / sqrt(r) * p->Explicit_Viscosity * (1.0 / Mach) * (1.0 / Mach) * (1.0 - 3.0 + 2.0 * pow(r / rs, -2.0));
+      }
+      if (rh < (100. * p->Rho_Floor)) rh = 100. * p->Rho_Floor;
+      prim[RHO] = rh * exp(0.0001 * pot / cp / cp);
+      prim[PPP] = (c0 * c0 + c1 * c1) / gam * rh * exp(0.0001 * pot / cp / cp);
+      prim[URR] = vr; prim[UPP] = om - sqrt(1.) / pow(r, 1.5); prim[UZZ] = 0.0;
+      return 1;
+    }
+    case MIDDLE:
+      middle(p, r, 1, prim);
+      return 1;
+    default:
+      return 0;
+  }
 }
 
 /* ---------------- conversions (src/Cell/cell_conversion.c) ---------------- */
@@ -404,10 +531,21 @@ int port_setup(Port *p) {
     p->gM[1] = M1; p->gr[1] = M0 / Mtotal * sep; p->gphi[1] = M_PI; p->gom[1] = sqrt(om2);
   }
   /* initial data (cell_init_*; ref_newic.c for 7..9) */
+  srand(666); /* cell_init_torus re-seeds */
   for (i = 0; i < p->NR; i++) {
     double rm = FP(p, i - 1), rp = FP(p, i), r = 0.5 * (rm + rp);
     double prof[5];
     int st = single_init(p, i, prof);
+    if (p->InitialDataType == SHEAR || p->InitialDataType == TORUS || p->InitialDataType == MILOS_MACFADYEN ||
+        p->InitialDataType == MIDDLE) {
+      for (j = 0; j < p->N_p[i]; j++, idx++) {
+        int g = p->off[i] + j;
+        double c[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        grid_cell(p, i, g, c);
+        for (q = 0; q < 5; ++q) p->prim[q][g] = c[q];
+      }
+      continue;
+    }
     if (st < 0) {
       fprintf(stderr, "port: InitialDataType %d is not restated\n", p->InitialDataType);
       return 1;
@@ -968,7 +1106,11 @@ static void add_src(Port *p, double dt) {
           if (i >= imin && i < imax) Md[k] += dr * dV;
         }
       }
-      if (p->Cooling == 1) {
+      if (p->Cooling == 1 && p->InitialDataType == SHEAR) { /* cell_source.c:189-193 */
+        double ct = (Pp - .01) / (p->Adiabatic_Index - 1.) * dV / 1.e-2;
+        if (ct < 0.0) ct = 0.0;
+        p->cons[TAU][g] -= ct * dt;
+      } else if (p->Cooling == 1) { /* cell_source.c:195-201 */
         double cap = p->cons[TAU][g] * 1.0;
         double ct = 9. / 4. * p->Explicit_Viscosity * pow(p->PoRho_r1, -3) / rho * pow(Pp / rho, 4.) * dt * dV;
         if (ct > cap) ct = cap;
@@ -1153,6 +1295,7 @@ static void boundary_and_damp(Port *p, double dt) {
 void port_substep(Port *p, double fac, int stop) {
   double dt = fac * p->dt;
   int g, q, k;
+  ULP_NOISE_START();
   port_build_faces(p);
   clean_pi(p);
   for (k = 0; k < 2; ++k) {

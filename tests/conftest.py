@@ -14,7 +14,18 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-CASES = ("gresho16", "kepler24", "cbd32", "kepler24out", "cbd32out", "kepler12noin", "kepler1out")
+CASES = ("gresho16", "kepler24", "cbd32", "kepler24out", "cbd32out", "kepler12noin", "kepler1out",
+         "shear12", "sstest32", "vortex16", "torus16", "milos16", "raddom16", "middle16")
+
+# Cases whose result moves further than the default bars under last-ulp
+# differences of the transcendentals: (max relative after 1 and 5 steps, L1
+# relative after 100 steps).  In the Shakura-Sunyaev test the cooling term is
+# capped at the cell's energy (cell_source.c:195-201), so tau - cooling cancels
+# to a small remainder, and the sink (cell_source.c:15-47) acts on the same
+# cells.  The oracle built with one-ulp noise on every libm result of the step
+# (oracle/Makefile, port-ulp) lands within these bars and outside the default
+# ones (tests/test_oracle.py checks both).
+CASE_TOL = {"sstest32": (1e-9, 1e-7)}
 
 
 def pytest_configure(config):

@@ -41,6 +41,15 @@ CASES = {
     # three annuli: annulus 0 is written by the inner boundary and then read
     # by the outer one, annulus 1 is read by the inner one and then written
     "kepler1out": configs.kepler_ring(num_r=1, R_Min=1.0, R_Max=1.2, BoundTypeR=1),
+    # the reference's test problems (parfiles/code_tests) and the other
+    # initial-data families (src/Cell/initial_data), reduced in size
+    "shear12": configs.shear_test(num_r=12),
+    "sstest32": configs.sstest(num_r=32),
+    "vortex16": configs.vortex_test(num_r=16, R_Min=0.1),
+    "torus16": configs.torus_2d(num_r=16),
+    "milos16": configs.milos_macfadyen(num_r=16),
+    "raddom16": configs.rad_dom(num_r=16),
+    "middle16": configs.middle(num_r=16),
 }
 STEPS = (1, 5, 100)
 PHASES = (0, 1, 2, 3, 4, 5, 6, 7)
@@ -110,7 +119,10 @@ def face_cases(par: str, st0: oracle.State, rng: np.random.Generator) -> dict:
             while x < 0.0:
                 x += 2 * np.pi
             d4[a + j] = x
-    layouts["jitter"] = (t4, d4)
+    # with fewer than 3 cells in an annulus a jittered layout can leave an inner
+    # cell ahead of every outer edge, where build_jloop's advance loop never ends
+    if st0.N_p.min() >= 3:
+        layouts["jitter"] = (t4, d4)
     for name, (tt, dd) in layouts.items():
         st = oracle.State(st0.NR, st0.NZ, st0.NQ, st0.N, 0.0, 0.0, st0.gm, st0.N_p, st0.r_faces,
                           st0.prim, st0.cons, tt, dd)
