@@ -130,6 +130,31 @@ template <typename T>
 HD T ldq(const double *v, const double *d, int q, int n, int g) {
   return Fld<T>::ld(v, d, (size_t)q * n + g);
 }
+
+// Loads of data that no thread of the running kernel writes (or that only
+// the loading thread writes, after the load).  On the device they take the
+// read-only path (ld.global.nc), so the compiler may issue them ahead of the
+// kernel's stores instead of one dependent round trip after another.
+template <typename X>
+HD X rd(const X *p) {
+#ifdef __CUDA_ARCH__
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+HD double ldr(const double *p, int q, int n, int g) { return rd(p + (size_t)q * n + g); }
+template <typename T> struct FldR;
+template <> struct FldR<double> {
+  static HD double ld(const double *v, const double *, size_t i) { return rd(v + i); }
+};
+template <> struct FldR<Dual> {
+  static HD Dual ld(const double *v, const double *d, size_t i) { return Dual(rd(v + i), rd(d + i)); }
+};
+template <typename T>
+HD T ldqr(const double *v, const double *d, int q, int n, int g) {
+  return FldR<T>::ld(v, d, (size_t)q * n + g);
+}
 template <typename T>
 HD void stq(double *v, double *d, int q, int n, int g, const T &x) {
   Fld<T>::st(v, d, (size_t)q * n + g, x);
@@ -605,13 +630,13 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
   const int j = g - A.cell_off;
   if (A.i > 0) {
     const Annulus &Q = d.ann[a - 1];
-    const int4 rr = reinterpret_cast<const int4 *>(d.rr)[g];
+    const int4 rr = rd(reinterpret_cast<const int4 *>(d.rr) + g);
     auto one = [&](int n) {
       RFace F;
-      F.cL = d.fL[Q.face_base + n];
+      F.cL = rd(d.fL + Q.face_base + n);
       F.cR = g;
-      F.dphi = d.fdphi[Q.face_base + n];
-      F.cm = d.fcm[Q.face_base + n];
+      F.dphi = rd(d.fdphi + Q.face_base + n);
+      F.cm = rd(d.fcm + Q.face_base + n);
       F.r = Q.f_r;
       F.dl = Q.f_dl;
       F.dr = Q.f_dr;
@@ -623,26 +648,26 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
       for (int n = rr.z; n < rr.w; ++n) one(n);
     } else {
       // three or more runs (the outer pointer went round more than twice)
-      const int T = d.pair_T[a - 1];
-      const int jpmin = d.pair_jpmin[a - 1];
+      const int T = rd(d.pair_T + a - 1);
+      const int jpmin = rd(d.pair_jpmin + a - 1);
       int dd = j - jpmin;
       if (dd < 0) dd += A.np;
       const int *runs = d.runs + Q.run_base;
       for (int s = dd; s <= T; s += A.np)
-        for (int n = runs[s]; n < runs[s + 1]; ++n) one(n);
+        for (int n = rd(runs + s); n < rd(runs + s + 1); ++n) one(n);
     }
   }
   if (A.i < NR - 1) {
-    const int nf = d.pair_nf[a];
-    int n0 = d.fstart[g];
-    int n1 = (j + 1 < A.np) ? d.fstart[g + 1] : nf;
+    const int nf = rd(d.pair_nf + a);
+    int n0 = rd(d.fstart + g);
+    int n1 = (j + 1 < A.np) ? rd(d.fstart + g + 1) : nf;
     if (nf <= 0) n1 = n0;
     for (int n = n0; n < n1; ++n) {
       RFace F;
       F.cL = g;
-      F.cR = d.fR[A.face_base + n];
-      F.dphi = d.fdphi[A.face_base + n];
-      F.cm = d.fcm[A.face_base + n];
+      F.cR = rd(d.fR + A.face_base + n);
+      F.dphi = rd(d.fdphi + A.face_base + n);
+      F.cm = rd(d.fcm + A.face_base + n);
       F.r = A.f_r;
       F.dl = A.f_dl;
       F.dr = A.f_dr;

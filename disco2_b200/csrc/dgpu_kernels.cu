@@ -405,15 +405,15 @@ template <typename T>
 __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= d.n_slots) return;
-  const int cL = d.fL[slot];
+  const int cL = rd(d.fL + slot);
   if (cL < 0) return;  // slot past the face list of its pair
-  const int cR = d.fR[slot];
-  const int a = d.slot_ann[slot];
+  const int cR = rd(d.fR + slot);
+  const int a = rd(d.slot_ann + slot);
   const Annulus &A = d.ann[a];
   const int N = d.n_cells, NS = d.n_slots;
-  const double cm = d.fcm[slot];
-  double pL = d.tiphw[cL] - .5 * d.dphi[cL];
-  double pR = d.tiphw[cR] - .5 * d.dphi[cR];
+  const double cm = rd(d.fcm + slot);
+  double pL = rd(d.tiphw + cL) - .5 * rd(d.dphi + cL);
+  double pR = rd(d.tiphw + cR) - .5 * rd(d.dphi + cR);
   double dpL = cm - pL;
   dpL = wrap_pm(dpL, d.err);
   double dpR = pR - cm;
@@ -423,8 +423,8 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   const double den = A.f_dr + A.f_dl;
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    T WL = ldq<T>(d.prim, tp.prim, q, N, cL) + dpL * ldq<T>(d.gradp, tp.gradp, q, N, cL);
-    T WR = ldq<T>(d.prim, tp.prim, q, N, cR) - dpR * ldq<T>(d.gradp, tp.gradp, q, N, cR);
+    T WL = ldqr<T>(d.prim, tp.prim, q, N, cL) + dpL * ldqr<T>(d.gradp, tp.gradp, q, N, cL);
+    T WR = ldqr<T>(d.prim, tp.prim, q, N, cR) - dpR * ldqr<T>(d.gradp, tp.gradp, q, N, cR);
     stq<T>(d.fS, tp.fS, q, NS, slot, (WR - WL) / den);
   }
 }

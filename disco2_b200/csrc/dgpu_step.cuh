@@ -61,13 +61,13 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
   // cell_copy (substep 1) + cell_adjust_RK_cons (cell_misc.c:28-57)
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
-    T cq = ldq<T>(d.cons, tp.cons, q, N, g);
+    T cq = ldqr<T>(d.cons, tp.cons, q, N, g);
     T rk;
     if (substep == 1) {
       rk = cq;
       if (write_rk) stq<T>(d.rkcons, tp.rkcons, q, N, g, cq);
     } else {
-      rk = ldq<T>(d.rkcons, tp.rkcons, q, N, g);
+      rk = ldqr<T>(d.rkcons, tp.rkcons, q, N, g);
     }
     c[q] = (1.0 - RK) * cq + RK * rk;
   }
@@ -78,20 +78,20 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     const double r = .5 * (A.rp + A.rm);
     auto addL = [&](int f) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.fphi, tp.fphi, q, N, f);
+      for (int q = 0; q < 5; ++q) c[q] -= ldqr<T>(d.fphi, tp.fphi, q, N, f);
       if (P.has_visc) {
-        c[D_SRR] -= ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
-        c[D_LLL] -= ldq<T>(d.fphi, tp.fphi, 6, N, f);
-        c[D_TAU] -= ldq<T>(d.fphi, tp.fphi, 7, N, f);
+        c[D_SRR] -= ldqr<T>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] -= ldqr<T>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] -= ldqr<T>(d.fphi, tp.fphi, 7, N, f);
       }
     };
     auto addR = [&](int f) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.fphi, tp.fphi, q, N, f);
+      for (int q = 0; q < 5; ++q) c[q] += ldqr<T>(d.fphi, tp.fphi, q, N, f);
       if (P.has_visc) {
-        c[D_SRR] += ldq<T>(d.fphi, tp.fphi, 5, N, f) / r;
-        c[D_LLL] += ldq<T>(d.fphi, tp.fphi, 6, N, f);
-        c[D_TAU] += ldq<T>(d.fphi, tp.fphi, 7, N, f);
+        c[D_SRR] += ldqr<T>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] += ldqr<T>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] += ldqr<T>(d.fphi, tp.fphi, 7, N, f);
       }
     };
     if (j == 0) {
@@ -109,21 +109,21 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int asR) {
       if (asR) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] += ldq<T>(d.frf, tp.frf, q, NS, slot);
+        for (int q = 0; q < 5; ++q) c[q] += ldqr<T>(d.frf, tp.frf, q, NS, slot);
         if (P.has_visc) {
           double rR = F.r + F.dr;
-          c[D_SRR] += ldq<T>(d.frf, tp.frf, 5, NS, slot) / rR;
-          c[D_LLL] += ldq<T>(d.frf, tp.frf, 6, NS, slot);
-          c[D_TAU] += ldq<T>(d.frf, tp.frf, 7, NS, slot);
+          c[D_SRR] += ldqr<T>(d.frf, tp.frf, 5, NS, slot) / rR;
+          c[D_LLL] += ldqr<T>(d.frf, tp.frf, 6, NS, slot);
+          c[D_TAU] += ldqr<T>(d.frf, tp.frf, 7, NS, slot);
         }
       } else {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] -= ldq<T>(d.frf, tp.frf, q, NS, slot);
+        for (int q = 0; q < 5; ++q) c[q] -= ldqr<T>(d.frf, tp.frf, q, NS, slot);
         if (P.has_visc) {
           double rL = F.r - F.dl;
-          c[D_SRR] -= ldq<T>(d.frf, tp.frf, 5, NS, slot) / rL;
-          c[D_LLL] -= ldq<T>(d.frf, tp.frf, 6, NS, slot);
-          c[D_TAU] -= ldq<T>(d.frf, tp.frf, 7, NS, slot);
+          c[D_SRR] -= ldqr<T>(d.frf, tp.frf, 5, NS, slot) / rL;
+          c[D_LLL] -= ldqr<T>(d.frf, tp.frf, 6, NS, slot);
+          c[D_TAU] -= ldqr<T>(d.frf, tp.frf, 7, NS, slot);
         }
       }
     });
@@ -131,20 +131,20 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
   if (stop == 3) return false;
   // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
   // increments come from k_source; added here in the reference's order
-  c[D_SRR] += ldq<T>(d.src, tp.src, 0, N, g);
-  c[D_SRR] += ldq<T>(d.src, tp.src, 1, N, g);
-  c[D_LLL] += ldq<T>(d.src, tp.src, 2, N, g);
-  c[D_SZZ] += ldq<T>(d.src, tp.src, 3, N, g);
-  c[D_TAU] += ldq<T>(d.src, tp.src, 4, N, g);
+  c[D_SRR] += ldqr<T>(d.src, tp.src, 0, N, g);
+  c[D_SRR] += ldqr<T>(d.src, tp.src, 1, N, g);
+  c[D_LLL] += ldqr<T>(d.src, tp.src, 2, N, g);
+  c[D_SZZ] += ldqr<T>(d.src, tp.src, 3, N, g);
+  c[D_TAU] += ldqr<T>(d.src, tp.src, 4, N, g);
   if (P.rho_sink_on == 1) {
-    for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldq<T>(d.src, tp.src, 6 + p, N, g);
+    for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldqr<T>(d.src, tp.src, 6 + p, N, g);
   }
   const double rm = A.rm, rp = A.rp;
   const double r = .5 * (rp + rm);
   if (P.cooling == 1) {
     // cooling reads the running tau (cell_source.c:187-203)
-    const T rho = ldq<T>(d.prim, tp.prim, D_RHO, N, g), Pp = ldq<T>(d.prim, tp.prim, D_PPP, N, g);
-    const double dV = d.dphi[g] * .5 * A.dv_diff * P.dz;
+    const T rho = ldqr<T>(d.prim, tp.prim, D_RHO, N, g), Pp = ldqr<T>(d.prim, tp.prim, D_PPP, N, g);
+    const double dV = rd(d.dphi + g) * .5 * A.dv_diff * P.dz;
     if (P.init_type == DI_SHEAR) {
       T cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
       if (cooling_term < 0.0) cooling_term = 0.0;
@@ -158,7 +158,7 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
       c[D_TAU] -= cooling_term;
     }
   }
-  if (P.has_visc) c[D_TAU] += ldq<T>(d.src, tp.src, 5, N, g);
+  if (P.has_visc) c[D_TAU] += ldqr<T>(d.src, tp.src, 5, N, g);
   // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
   {
     const double a_sep = S.gr[0] + S.gr[1];
@@ -166,8 +166,8 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     const double Omega = rom / r;
     const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
     const int NA = d.n_ann;
-    const double kappa = d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
-    if (kappa > 0.) split_rotate(c, d.ann_c[NA + a], d.ann_c[2 * NA + a], dr_r2Om, kappa, Omega, r);
+    const double kappa = rd(d.ann_c + a);  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
+    if (kappa > 0.) split_rotate(c, rd(d.ann_c + NA + a), rd(d.ann_c + 2 * NA + a), dr_r2Om, kappa, Omega, r);
   }
   return stop > 4;
 }
@@ -182,13 +182,13 @@ __device__ __forceinline__ double mesh_advance(const DevPtrs &d, const Annulus &
   const int j = g - A.cell_off;
   const double r = .5 * (A.rm + A.rp);
   const double a_sep = S.gr[0] + S.gr[1];
-  const double w_total = d.w_ann[a] + frame_rom(P, A.rom, r, a_sep);
+  const double w_total = rd(d.w_ann + a) + frame_rom(P, A.rom, r, a_sep);
   const double *tin = substep == 1 ? d.tiph0 : d.tiph1;
   const int gm1 = j == 0 ? A.cell_off + A.np - 1 : g - 1;
-  rk = substep == 1 ? tin[g] : d.rktiph[g];
-  double rkm = substep == 1 ? tin[gm1] : d.rktiph[gm1];
-  tn = new_tiph(d.tiphw[g], rk, RK, w_total, dt, r, d.err);
-  double tnm = new_tiph(d.tiphw[gm1], rkm, RK, w_total, dt, r, d.err);
+  rk = substep == 1 ? rd(tin + g) : rd(d.rktiph + g);
+  double rkm = substep == 1 ? rd(tin + gm1) : rd(d.rktiph + gm1);
+  tn = new_tiph(rd(d.tiphw + g), rk, RK, w_total, dt, r, d.err);
+  double tnm = new_tiph(rd(d.tiphw + gm1), rkm, RK, w_total, dt, r, d.err);
   double dphi_n = tn - tnm;
   return wrap_pos(dphi_n, d.err);
 }

@@ -15,8 +15,7 @@ import argparse
 
 from . import configs, lib
 
-WORKLOADS = {"circumbinary": configs.circumbinary, "kepler_ring": configs.kepler_ring,
-             "gresho": configs.gresho}
+WORKLOADS = configs.WORKLOADS
 
 
 def main() -> None:
