@@ -173,6 +173,28 @@ def cpu_baseline_run(par_text: str, steps: int, warmup: int):
     return wall, kind
 
 
+def cpu_batch_baseline(par_texts, nins, steps: int):
+    """The sweep on the host: one reference (or restatement) process per disk,
+    as many at once as there are host cores, each timing `steps` RK2 steps
+    after its set-up.  Aggregate zone-updates/s = the steps' work over the
+    core-seconds they took, times the cores used."""
+    from concurrent.futures import ThreadPoolExecutor
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    cores = max(1, min(cores, len(par_texts)))
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        res = list(ex.map(lambda t: cpu_baseline_run(t, steps, 0), par_texts))
+    if any(r is None for r in res):
+        return None
+    core_s = sum(w for w, _ in res)
+    work = sum(n * steps for n in nins)
+    return {"value": work / core_s * cores, "unit": UNIT, "cores": cores, "kind": res[0][1],
+            "sample": f"{steps} RK2 step(s) of each of the {len(par_texts)} disks, one process "
+                      f"per disk, {cores} at a time ({core_s:.1f} core-seconds of steps)"}
+
+
 def interior_cells(sim) -> int:
     N_p, _ = sim.grid()
     ngmin = 1
@@ -263,13 +285,18 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
         tot = t.item()
     v_b = tot * k_steps / (ms_b / 1e3)
     v_s = tot * k_steps / (ms_seq / 1e3)
+    cpu = None
+    if world == 1 and not args.no_cpu and args.batch_cpu_steps > 0:
+        cpu = cpu_batch_baseline([configs.parfile_text(p) for p in sweep],
+                                 [interior_cells(s) for s in sims_all], args.batch_cpu_steps)
     return {"workload": "48 independent circumbinary disks from seed 3: q log-uniform [0.01,1], "
                         "alpha [0.01,0.1], h/r [0.05,0.1], N_r [128,512], R_out [10,30]",
             "cells": int(sum(s.num_cells for s in sims_all)), "interior_cells": int(tot),
             "steps": k_steps, "value": v_b, "unit": UNIT, "ms_per_step": ms_b / k_steps,
             "sequential_value": v_s, "batched_over_sequential": v_b / v_s,
             "how": "one context holding every disk of the rank vs one context per disk run (each autotuned) "
-                   "back to back, same steps, L2 flushed before each step"}
+                   "back to back, same steps, L2 flushed before each step",
+            "cpu_baseline": cpu}
 
 
 def run_adjoint(args):
@@ -324,6 +351,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--batch-cpu-steps", type=int, default=1,
+                    help="RK2 steps per disk of the sweep's host baseline (0: skip it)")
     ap.add_argument("--tune-steps", type=int, default=3,
                     help="steps per launch-shape candidate for the autotuner (0: built-in shapes)")
     ap.add_argument("--no-adjoint", action="store_true")
