@@ -678,6 +678,37 @@ __device__ __forceinline__ void for_cell_rfaces(const DevPtrs &d, const Annulus 
 }
 
 
+// The same faces as for_cell_rfaces, in the same order, as contiguous slot
+// ranges: f(first slot, end slot, side) with side 1 for the faces of pair
+// (i-1, i) (the cell is their outer cell) and 0 for those of pair (i, i+1).
+template <typename Fn>
+__device__ __forceinline__ void for_cell_rface_ranges(const DevPtrs &d, const Annulus &A, int a, int g, int NR,
+                                                      Fn f) {
+  const int j = g - A.cell_off;
+  if (A.i > 0) {
+    const Annulus &Q = d.ann[a - 1];
+    const int4 rr = rd(reinterpret_cast<const int4 *>(d.rr) + g);
+    if (rr.z != INT_MIN) {
+      f(Q.face_base + rr.x, Q.face_base + rr.y, 1);
+      f(Q.face_base + rr.z, Q.face_base + rr.w, 1);
+    } else {
+      const int T = rd(d.pair_T + a - 1);
+      const int jpmin = rd(d.pair_jpmin + a - 1);
+      int dd = j - jpmin;
+      if (dd < 0) dd += A.np;
+      const int *runs = d.runs + Q.run_base;
+      for (int s = dd; s <= T; s += A.np) f(Q.face_base + rd(runs + s), Q.face_base + rd(runs + s + 1), 1);
+    }
+  }
+  if (A.i < NR - 1) {
+    const int nf = rd(d.pair_nf + a);
+    int n0 = rd(d.fstart + g);
+    int n1 = (j + 1 < A.np) ? rd(d.fstart + g + 1) : nf;
+    if (nf <= 0) n1 = n0;
+    f(A.face_base + n0, A.face_base + n1, 0);
+  }
+}
+
 }  // namespace
 
 #endif

@@ -103,28 +103,52 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     }
   }
   if (stop == 2) return false;
-  // r faces in face-list order
+  // r faces in face-list order, two faces' increments loaded at a time
   {
     const int NS = d.n_slots;
-    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int asR) {
-      if (asR) {
+    const bool visc = P.has_visc;
+    for_cell_rface_ranges(d, A, a, g, P.NR, [&](int s, int e, int asR) {
+      // the outer cell's faces divide the viscous S_r part by its own radius
+      const Annulus &Q = asR ? d.ann[a - 1] : A;
+      const double rv = asR ? Q.f_r + Q.f_dr : Q.f_r - Q.f_dl;
+      auto apply = [&](const T *u) {
+        if (asR) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] += ldqr<T>(d.frf, tp.frf, q, NS, slot);
-        if (P.has_visc) {
-          double rR = F.r + F.dr;
-          c[D_SRR] += ldqr<T>(d.frf, tp.frf, 5, NS, slot) / rR;
-          c[D_LLL] += ldqr<T>(d.frf, tp.frf, 6, NS, slot);
-          c[D_TAU] += ldqr<T>(d.frf, tp.frf, 7, NS, slot);
-        }
-      } else {
+          for (int q = 0; q < 5; ++q) c[q] += u[q];
+          if (visc) {
+            c[D_SRR] += u[5] / rv;
+            c[D_LLL] += u[6];
+            c[D_TAU] += u[7];
+          }
+        } else {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) c[q] -= ldqr<T>(d.frf, tp.frf, q, NS, slot);
-        if (P.has_visc) {
-          double rL = F.r - F.dl;
-          c[D_SRR] -= ldqr<T>(d.frf, tp.frf, 5, NS, slot) / rL;
-          c[D_LLL] -= ldqr<T>(d.frf, tp.frf, 6, NS, slot);
-          c[D_TAU] -= ldqr<T>(d.frf, tp.frf, 7, NS, slot);
+          for (int q = 0; q < 5; ++q) c[q] -= u[q];
+          if (visc) {
+            c[D_SRR] -= u[5] / rv;
+            c[D_LLL] -= u[6];
+            c[D_TAU] -= u[7];
+          }
         }
+      };
+      int n = s;
+      for (; n + 1 < e; n += 2) {
+        T u[8], v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          if (q < 5 || visc) {
+            u[q] = ldqr<T>(d.frf, tp.frf, q, NS, n);
+            v[q] = ldqr<T>(d.frf, tp.frf, q, NS, n + 1);
+          }
+        }
+        apply(u);
+        apply(v);
+      }
+      if (n < e) {
+        T u[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < 5 || visc) u[q] = ldqr<T>(d.frf, tp.frf, q, NS, n);
+        apply(u);
       }
     });
   }
