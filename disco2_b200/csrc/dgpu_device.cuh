@@ -144,6 +144,17 @@ HD X rd(const X *p) {
 #endif
 }
 HD double ldr(const double *p, int q, int n, int g) { return rd(p + (size_t)q * n + g); }
+
+// Starts moving the line holding *p into L2 without waiting for it (no
+// register, no effect on results): the later load of the same line then
+// waits on L2 instead of HBM.  Every address given here is inside its array.
+__device__ __forceinline__ void pf(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+// The same for the n-plane SoA value of cell g in each plane.
+__device__ __forceinline__ void pf_planes(const double *p, int planes, int n, int g) {
+  for (int q = 0; q < planes; ++q) pf(p + (size_t)q * n + g);
+}
 template <typename T> struct FldR;
 template <> struct FldR<double> {
   static HD double ld(const double *v, const double *, size_t i) { return rd(v + i); }

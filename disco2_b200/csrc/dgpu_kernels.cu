@@ -844,6 +844,16 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
   const double RK = substep == 1 ? 0.0 : 0.5;
   const double fac = substep == 1 ? 1.0 : 0.5;
   if (g < N) {
+    // the cell's own planes, before the annulus lookups they do not depend on
+    pf_planes(d.cons, 5, N, g);
+    if (substep == 2) {
+      pf_planes(d.rkcons, 5, N, g);
+      pf(d.rktiph + g);
+    }
+    pf_planes(d.fphi, 8, N, g);
+    pf_planes(d.src, 8, N, g);
+    pf(d.tiphw + g);
+    pf((substep == 1 ? d.tiph0 : d.tiph1) + g);
     const int a = d.cell_ann[g];
     const Annulus A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
