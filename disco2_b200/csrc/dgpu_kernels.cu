@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
   __shared__ int sh_flag;
   extern __shared__ double sm[];  // staged phi edges and widths of the pair
   const int a = blockIdx.x;
-  const Annulus A = d.ann[a];
+  const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
   const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   if (t >= N) return;
   const int g = t;
   const int a = d.cell_ann[g];
-  const Annulus A = d.ann[a];
+  const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
   const InstState &S = d.ist[A.inst];
   const int j = g - A.cell_off;
@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     pf(d.tiphw + g);
     pf((substep == 1 ? d.tiph0 : d.tiph1) + g);
     const int a = d.cell_ann[g];
-    const Annulus A = d.ann[a];
+    const Annulus &A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
     const InstState &S = d.ist[A.inst];
     const double dt = fac * S.dt;
@@ -973,7 +973,7 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
   if (g >= N) return;
-  const Annulus A = d.ann[d.cell_ann[g]];
+  const Annulus &A = d.ann[d.cell_ann[g]];
   const DiskParams &P = d.par[A.inst];
   double r = .5 * (A.rp + A.rm);
   double dV = A.dv_half * d.dphi[g] * P.dz;
@@ -1070,7 +1070,7 @@ __global__ void __launch_bounds__(BLK) k_torque(DevPtrs d, int inst, double *par
   const int g = P.cell_base + blockIdx.x * blockDim.x + threadIdx.x;
   double v = 0.0;
   if (g < P.cell_base + P.n_cells) {
-    const Annulus A = d.ann[d.cell_ann[g]];
+    const Annulus &A = d.ann[d.cell_ann[g]];
     if (A.kind & DGPU_AK_CFL) {
       double dphi = d.dphi[g];
       double phi = d.tiph0[g] - .5 * dphi;
