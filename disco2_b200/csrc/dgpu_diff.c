@@ -68,6 +68,12 @@ struct dgpu_diff {
   void *sh_mem;
   cudaStream_t s2;
   cudaEvent_t e_rep, e_rev;
+  /* a second copy for the reverse step: substep 1's intermediates are rebuilt
+   * there (stream s3) while substep 2 is reversed on the context's buffers */
+  DevPtrs pp;
+  void *pp_mem;
+  cudaStream_t s3;
+  cudaEvent_t e_fork, e_join;
   /* step graphs (G_*), valid for tab_K */
   cudaGraphExec_t g[G_N];
   int have[G_N];
@@ -109,6 +115,10 @@ void dctx_diff_free(struct dgpu_ctx *c) {
   if (D->s2) cudaStreamDestroy(D->s2);
   if (D->e_rep) cudaEventDestroy(D->e_rep);
   if (D->e_rev) cudaEventDestroy(D->e_rev);
+  cudaFree(D->pp_mem);
+  if (D->s3) cudaStreamDestroy(D->s3);
+  if (D->e_fork) cudaEventDestroy(D->e_fork);
+  if (D->e_join) cudaEventDestroy(D->e_join);
   for (k = 0; k < D->n_snaps; ++k) {
     cudaFree(D->snaps[k].buf);
     cudaFree(D->snaps[k].ist);
@@ -285,13 +295,13 @@ static int ensure_snaps(struct dgpu_ctx *c, struct dgpu_diff *D, int nck, int K)
 /* The replay's buffers: every per-cell, per-face and per-annulus array the
  * step writes, and its own disk state and counters; the read-only tables and
  * the error flags are shared with the context. */
-static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
+/* Lays out in fresh device memory (*mem) a copy of every per-cell, per-face
+ * and per-disk buffer the step writes, in *h; the tables stay shared. */
+static int alloc_shadow(struct dgpu_ctx *c, DevPtrs *h, void **mem) {
   const size_t N = (size_t)c->n_cells, S = (size_t)(c->n_slots ? c->n_slots : 1), A = (size_t)c->n_ann;
   const size_t R = (size_t)(c->n_runs ? c->n_runs : 1), B = (size_t)c->n_upd_blocks;
   size_t sz[32], off[33], k = 0, n;
   char *m;
-  DevPtrs *h = &D->sh;
-  if (D->sh_mem) return DGPU_OK;
 #define SZ(bytes) sz[k++] = ((bytes) + 255) / 256 * 256
   SZ(8 * 25 * N);              /* 0: prim cons rkcons grad gradp */
   SZ(8 * 5 * N);               /* 1: tiph0 tiph1 tiphw rktiph dphi */
@@ -313,9 +323,9 @@ static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
 #undef SZ
   off[0] = 0;
   for (n = 0; n < k; ++n) off[n + 1] = off[n] + sz[n];
-  CK(cudaMalloc(&D->sh_mem, off[k]));
-  CK(cudaMemset(D->sh_mem, 0, off[k]));
-  m = (char *)D->sh_mem;
+  CK(cudaMalloc(mem, off[k]));
+  CK(cudaMemset(*mem, 0, off[k]));
+  m = (char *)*mem;
   *h = c->d;
   h->prim = (double *)(m + off[0]);
   h->cons = h->prim + 5 * N;
@@ -348,10 +358,19 @@ static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
   h->mdot_part = (double *)(m + off[14]);
   h->counters = (unsigned int *)(m + off[15]);
   h->ist = (InstState *)(m + off[16]);
+  return DGPU_OK;
+}
+
+static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
+  if (D->sh_mem) return DGPU_OK;
+  if (alloc_shadow(c, &D->sh, &D->sh_mem) || alloc_shadow(c, &D->pp, &D->pp_mem)) return DGPU_ERR_CUDA;
   CK(cudaMalloc((void **)&D->d_idx2, sizeof(int)));
   CK(cudaStreamCreateWithFlags(&D->s2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&D->e_rep, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&D->e_rev, cudaEventDisableTiming));
+  CK(cudaStreamCreateWithFlags(&D->s3, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&D->e_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&D->e_join, cudaEventDisableTiming));
   return DGPU_OK;
 }
 
@@ -388,6 +407,17 @@ static int shadow_substep(struct dgpu_ctx *c, DevPtrs *h, cudaStream_t s, int su
   CKK(dgk_flux_phi(h, NULL, sub, s));
   CKK(dgk_flux_r(h, NULL, sub, s));
   CKK(dgk_update_rec(h, sub, rec, idx, s));
+  return DGPU_OK;
+}
+
+/* The forward intermediates the reverse of a substep reads (cellprep, merge,
+ * face and cell r slopes, per-annulus constants) on buffers h, stream s. */
+static int prep_substep(struct dgpu_ctx *c, DevPtrs *h, cudaStream_t s, int sub) {
+  CKK(dgk_cellprep(h, NULL, sub, s));
+  CKK(dgk_merge(h, sub, s));
+  CKK(dgk_rslope(h, NULL, s));
+  CKK(dgk_plm_r(h, NULL, sub, s));
+  CKK(dgk_ann_consts(h, sub, s));
   return DGPU_OK;
 }
 
@@ -428,15 +458,22 @@ static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
         return -1;
       return dgk_add_int(Dd->d_idx2, 1, Dd->s2);
     case G_REV0:
-    case G_REV1: /* reverse step *idx of the segment (step n = *base + *idx) */
+    case G_REV1: /* reverse step *idx of the segment (step n = *base + *idx):
+                    substep 1's intermediates are rebuilt on the second buffer
+                    set (stream s3) while substep 2 is reversed */
       if (dgk_adj_objective(&c->d, &Dd->J, tabS, istS, Dd->d_idx, 1, Dd->wts, Dd->d_base, c->stream)) return -1;
+      if (cudaEventRecord(Dd->e_fork, c->stream) != cudaSuccess ||
+          cudaStreamWaitEvent(Dd->s3, Dd->e_fork, 0) != cudaSuccess)
+        return -1;
+      if (dgk_snap_tab(&Dd->pp, tabS, istS, Dd->d_idx, 0, 0, Dd->s3) || prep_substep(c, &Dd->pp, Dd->s3, 1)) return -1;
       if (dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 0, c->stream) ||
           dctx_substep(c, NULL, 2, DCTX_ADJPREP, NULL, NULL) ||
           dgk_adj_substep(&c->d, &Dd->J, 2, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
         return -1;
-      if (dgk_snap_tab(&c->d, tabS, istS, Dd->d_idx, 0, 0, c->stream) ||
-          dctx_substep(c, NULL, 1, DCTX_ADJPREP, NULL, NULL) ||
-          dgk_adj_substep(&c->d, &Dd->J, 1, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
+      if (cudaEventRecord(Dd->e_join, Dd->s3) != cudaSuccess ||
+          cudaStreamWaitEvent(c->stream, Dd->e_join, 0) != cudaSuccess)
+        return -1;
+      if (dgk_adj_substep(&Dd->pp, &Dd->J, 1, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
         return -1;
       return dgk_add_int(Dd->d_idx, -1, c->stream);
   }
