@@ -160,6 +160,9 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
   const int N = d.n_cells;
   if (g >= N) return;
   const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
+  pf_planes(d.prim, 5, N, g);
+  pf(d.dphi + g);
+  pf(traw + g);
   const int a = d.cell_ann[g];
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -446,6 +449,9 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
     }
   }
   if (g < N) {
+    pf(d.rr + 4 * (size_t)g);
+    pf(d.fstart + g);
+    pf(d.dphi + g);
     const int a = d.cell_ann[g];
     const Annulus A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
@@ -566,6 +572,13 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   const double fac = substep == 1 ? 1.0 : 0.5;
   if (t >= N) return;
   const int g = t;
+  // the cell's own planes (its right neighbour's share the lines) ahead of
+  // the annulus lookups
+  pf_planes(d.prim, 5, N, g);
+  pf_planes(d.gradp, 5, N, g);
+  pf_planes(d.grad, 5, N, g);
+  pf(d.tiphw + g);
+  pf(d.dphi + g);
   const int a = d.cell_ann[g];
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -731,6 +744,11 @@ __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int s
   double md0 = 0.0, md1 = 0.0;
   if (t < N && cells) {
     const int g = t;
+    pf_planes(d.prim, 5, N, g);
+    pf(d.grad + (size_t)D_UPP * N + g);
+    pf(d.gradp + (size_t)D_URR * N + g);
+    pf(d.tiphw + g);
+    pf(d.dphi + g);
     const int a = d.cell_ann[g];
     const Annulus &A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
@@ -851,7 +869,7 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
       pf(d.rktiph + g);
     }
     pf_planes(d.fphi, 8, N, g);
-    pf_planes(d.src, 8, N, g);
+    pf_planes(d.src, 6, N, g);
     pf(d.tiphw + g);
     pf((substep == 1 ? d.tiph0 : d.tiph1) + g);
     const int a = d.cell_ann[g];
