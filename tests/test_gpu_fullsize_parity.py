@@ -1,0 +1,62 @@
+"""Parity at the benchmark sizes: the device step against the oracle (the
+reference build where it was compiled, else the C restatement) on the same
+full-size disks, three RK2 steps from the same initial state.
+
+Bars as in test_gpu_parity.py: bit-exact where no device transcendental
+reaches the result (Gresho vortex, shear layer), max relative 1e-12 per
+array otherwise; the Shakura-Sunyaev test problem carries last-ulp
+differences further (its bar is CASE_TOL's).
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import CASE_TOL, max_rel
+from disco2_b200 import configs, lib
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 3
+# name -> (parameters, bit-exact, per-step bar)
+DISKS = {
+    "gresho_96": (configs.gresho(), True, 0.0),
+    "kepler_ring_256": (configs.kepler_ring(), False, 1e-12),
+    "circumbinary_400": (configs.circumbinary(), False, 1e-12),
+    "shear_128": (configs.shear_test(), True, 0.0),
+    "sstest_128": (configs.sstest(), False, CASE_TOL["sstest32"][0]),
+}
+
+
+@pytest.fixture(scope="module")
+def impl():
+    if not (oracle.have_ref() or oracle.have_port()):
+        oracle.build()
+    return "ref" if oracle.have_ref() else "port"
+
+
+@pytest.mark.parametrize("name", sorted(DISKS))
+def test_full_size_steps_match_the_oracle(name, impl):
+    p, exact, tol = DISKS[name]
+    with tempfile.TemporaryDirectory() as td:
+        par = configs.write_parfile(p, os.path.join(td, name + ".par"))
+        want, _, _ = oracle.run(par, STEPS, impl=impl)
+    sim = lib.Sim(p)
+    ctx = lib.Context(sim)
+    ctx.init_state(0)
+    ctx.step(STEPS)
+    got = ctx.get_state(0)
+    t, dt = ctx.time(0)
+    ctx.close()
+    for k in ("prim", "cons"):
+        a, b = got[k], getattr(want, k)
+        if exact:
+            assert np.array_equal(a, b), (k, float(np.abs(a - b).max()))
+        else:
+            assert max_rel(a, b) <= tol, (k, max_rel(a, b))
+    for k in ("tiph", "dphi"):
+        d = float(np.abs(got[k] - getattr(want, k)).max())
+        assert (d == 0.0) if exact else (d <= max(tol, 1e-12) * 2 * np.pi), (k, d)
+    assert abs(t - want.t) <= (0.0 if exact else max(tol, 1e-12) * abs(want.t))
