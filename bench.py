@@ -10,7 +10,7 @@ binary, alpha = 0.1 viscosity, HLLC, outer damping zone).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun (N > 1) every rank advances its own replica of the disk (the
-single-disk step does not shard): per-GPU work is fixed, the
+single-disk step does not shard without a radial domain split): per-GPU work is fixed, the
 reported value is the sum over ranks, timed as the maximum over ranks.
 Prints one JSON line (rank 0).
 """
@@ -35,7 +35,7 @@ PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 # Compulsory DRAM bytes per unit for each kernel as designed (each array
-# element touched once): per cell and per r-face of one substep (see DESIGN.md).
+# element touched once): per cell and per r-face of one substep.
 KERNELS = ["cellprep", "merge", "rslope", "plm_r", "source", "flux_phi", "flux_r", "update"]
 ALG_BYTES = {
     # name: (bytes per cell, bytes per r-face)
