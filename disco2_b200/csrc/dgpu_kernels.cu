@@ -411,6 +411,10 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   const int cL = rd(d.fL + slot);
   if (cL < 0) return;  // slot past the face list of its pair
   const int cR = rd(d.fR + slot);
+  pf_planes(d.prim, 5, d.n_cells, cL);
+  pf_planes(d.prim, 5, d.n_cells, cR);
+  pf_planes(d.gradp, 5, d.n_cells, cL);
+  pf_planes(d.gradp, 5, d.n_cells, cR);
   const int a = rd(d.slot_ann + slot);
   const Annulus &A = d.ann[a];
   const int N = d.n_cells, NS = d.n_slots;
