@@ -430,6 +430,8 @@ int dctx_read_err(struct dgpu_ctx *c) {
     return fail(c, DGPU_ERR_FACE_OVERFLOW, "face list overflowed its buffer (flags 0x%x)", e);
   if (e & DGPU_EF_WRAP_LIMIT)
     return fail(c, DGPU_ERR_NUMERIC, "a phi wrap loop did not terminate (non-finite phi edge; flags 0x%x)", e);
+  if (e & DGPU_EF_NONFINITE)
+    return fail(c, DGPU_ERR_NUMERIC, "non-finite state: a non-ghost cell's CFL time step is NaN (flags 0x%x)", e);
   if (e & DGPU_EF_VISC_VZ)
     return fail(c, DGPU_ERR_NUMERIC, "viscosity with nonzero v_z (the reference exits here, Riemann_routines.c:271-274)");
   return DGPU_OK;

@@ -36,6 +36,7 @@ enum { DR_HLLC, DR_HLL };
 #define DGPU_EF_WRAP_LIMIT 2
 #define DGPU_EF_VISC_VZ 4
 #define DGPU_EF_RUN_OVERFLOW 8
+#define DGPU_EF_NONFINITE 16   /* a non-ghost cell's CFL step is not a number (its state holds a NaN) */
 
 /* annulus kind bits */
 #define DGPU_AK_CFL 1        /* non-ghost: enters the CFL minimum (cell_mindt.c:38-42) */

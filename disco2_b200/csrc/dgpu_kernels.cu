@@ -528,6 +528,9 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
       }
       key = (unsigned long long)__double_as_longlong(dt);
       if (__longlong_as_double((long long)key) < 0.0 || dt != dt) key = ~0ull;
+      // the reference's minimum skips such a cell too (cell_mindt.c); here it
+      // is also reported
+      if (dt != dt) set_err(d.err, DGPU_EF_NONFINITE);
     }
   }
   if (substep != 1) return;

@@ -38,7 +38,8 @@ extern "C" {
 #define DGPU_ERR_UNSUPPORTED (-3)  /* option outside the implemented path (e.g. NumZ > 1) */
 #define DGPU_ERR_CUDA (-4)         /* a CUDA runtime call failed */
 #define DGPU_ERR_FACE_OVERFLOW (-5)/* face list exceeded its buffer (device flag) */
-#define DGPU_ERR_NUMERIC (-6)      /* device-detected condition the reference exit()s on */
+#define DGPU_ERR_NUMERIC (-6)      /* device-detected condition the reference exit()s on or
+                                      loops forever on, or a NaN in a non-ghost cell's state */
 #define DGPU_ERR_NOMEM (-7)        /* host or device allocation failed */
 
 typedef struct dgpu_sim dgpu_sim; /* host-side Sim: parameters + grid */

@@ -204,6 +204,22 @@ def test_torque_matches_host_formula():
     assert got == pytest.approx(tot, rel=1e-6)
 
 
+def test_nan_state_is_reported():
+    """A NaN in one interior cell spreads through its fluxes; the reference's
+    CFL minimum skips such cells and runs on, here the step also reports it."""
+    g = golden("kepler24")
+    sim = lib.Sim(str(g["parfile"]))
+    ctx = lib.Context(sim)
+    ctx.init_state(0)
+    st = ctx.get_state(0)
+    prim = st["prim"].copy()
+    prim[500, 0] = np.nan
+    ctx.set_state(0, prim, st["tiph"], st["dphi"])
+    with pytest.raises(lib.DiscoError, match="non-finite"):
+        ctx.step(2)
+    ctx.close()
+
+
 def test_nonfinite_phi_edge_is_reported_not_hung():
     """A non-finite phi edge makes the reference loop forever in its wrap loops;
     here the bounded loops set an error flag that surfaces as NUMERIC."""
