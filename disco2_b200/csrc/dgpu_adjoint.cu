@@ -204,9 +204,11 @@ __global__ void k_add_int(int *p, int dv) {
 
 // Stored states: 19 doubles per cell (prim, cons, rkcons, tiph0, tiph1,
 // rktiph, dphi) and the disk states.  save: context -> store; else back.
+// A stored state: prim, cons, rkcons (5 planes each), tiph0, tiph1, rktiph,
+// dphi, then the passive-scalar planes of prim, cons and rkcons (n_pass each).
 __device__ __forceinline__ void snap_copy_dev(const DevPtrs &d, double *sb, InstState *si, int save) {
-  const size_t N = (size_t)d.n_cells;
-  const size_t n = 19 * N;
+  const size_t N = (size_t)d.n_cells, NP = (size_t)d.n_pass * N;
+  const size_t n = 19 * N + 3 * NP;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double *c;
     if (i < 5 * N) c = d.prim + i;
@@ -215,7 +217,10 @@ __device__ __forceinline__ void snap_copy_dev(const DevPtrs &d, double *sb, Inst
     else if (i < 16 * N) c = d.tiph0 + (i - 15 * N);
     else if (i < 17 * N) c = d.tiph1 + (i - 16 * N);
     else if (i < 18 * N) c = d.rktiph + (i - 17 * N);
-    else c = d.dphi + (i - 18 * N);
+    else if (i < 19 * N) c = d.dphi + (i - 18 * N);
+    else if (i < 19 * N + NP) c = d.prim + 5 * N + (i - 19 * N);
+    else if (i < 19 * N + 2 * NP) c = d.cons + 5 * N + (i - 19 * N - NP);
+    else c = d.rkcons + 5 * N + (i - 19 * N - 2 * NP);
     if (save) sb[i] = *c;
     else *c = sb[i];
   }
@@ -803,7 +808,7 @@ int dgk_add_int(int *p, int dv, void *stream) {
 }
 
 static int snap_grid(const DevPtrs *d) {
-  long long n = 19LL * d->n_cells;
+  long long n = (19LL + 3LL * d->n_pass) * d->n_cells;
   long long b = (n + BLK - 1) / BLK;
   return (int)(b < 148 * 8 ? b : 148 * 8);
 }

@@ -141,7 +141,7 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
     initstate_r(666, state, sizeof(state), &rd);
     for (i = 0; i < s->NR && rc == DGPU_OK; ++i)
       for (j = 0; j < s->N_p[i]; ++j, ++idx)
-        if (dsim_grid_init(s, i, idx, t[idx], d[idx], g, &rd, prim + 5 * idx) != 0) {
+        if (dsim_grid_init(s, i, idx, t[idx], d[idx], g, &rd, prim + (size_t)s->NQ * idx) != 0) {
           rc = fail(NULL, DGPU_ERR_UNSUPPORTED, "InitialDataType %d has no whole-grid initialiser here", s->InitialDataType);
           break;
         }
@@ -156,7 +156,10 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
 static int check_supported(const struct dgpu_sim *s, int k, char *err, int n) {
   int i;
   if (s->NumZ != 1) return snprintf(err, (size_t)n, "disk %d: NumZ > 1 (3-D z faces) is not implemented", k), DGPU_ERR_UNSUPPORTED;
-  if (s->NUM_C != 5 || s->NUM_N != 0) return snprintf(err, (size_t)n, "disk %d: only NUM_C = 5, NUM_N = 0 is implemented", k), DGPU_ERR_UNSUPPORTED;
+  if (s->NUM_C != 5 || s->NUM_N < 0 || s->NUM_N > DGPU_MAX_PASSIVE)
+    return snprintf(err, (size_t)n, "disk %d: only NUM_C = 5 with NUM_N <= %d is implemented", k, DGPU_MAX_PASSIVE), DGPU_ERR_UNSUPPORTED;
+  if (s->NUM_N > 0 && s->DAMP_TIME > 0.0)
+    return snprintf(err, (size_t)n, "disk %d: passive scalars in a damping zone (the reference relaxes them toward an uninitialised value, cell_misc.c:119-124)", k), DGPU_ERR_UNSUPPORTED;
   if (s->NR < 3) return snprintf(err, (size_t)n, "disk %d: need at least 3 annuli", k), DGPU_ERR_UNSUPPORTED;
   for (i = 0; i < s->NR; ++i)
     if (s->N_p[i] < 2) return snprintf(err, (size_t)n, "disk %d: annulus %d has fewer than 2 cells", k, i), DGPU_ERR_UNSUPPORTED;
@@ -219,7 +222,7 @@ void dgpu_destroy(dgpu_ctx *c) {
 int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dgpu_ctx **out) {
   struct dgpu_ctx *c;
   int k, i, rc, ok = 1;
-  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0, n_ob = 0;
+  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0, n_ob = 0, n_pass = 0;
   int *h_cell_ann, *h_slot_ann;
   if (!sims || n < 1 || !out) return fail(NULL, DGPU_ERR_ARG, "bad arguments to dgpu_create");
   for (k = 0; k < n; ++k) {
@@ -241,6 +244,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     }
     ann += sims[k]->NR;
     cells += sims[k]->Ncells;
+    if (sims[k]->NUM_N > n_pass) n_pass = sims[k]->NUM_N;
     if (sims[k]->Ncells > maxcells) maxcells = sims[k]->Ncells;
   }
   c->n_ann = ann;
@@ -325,27 +329,29 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
       return fail(NULL, DGPU_ERR_CUDA, "stream/event creation failed");
     }
   }
+  c->n_pass = n_pass;
   {
     size_t N = (size_t)c->n_cells, S = (size_t)c->n_slots, A = (size_t)c->n_ann;
+    const size_t NQ = 5 + (size_t)n_pass, NF = 8 + (size_t)n_pass;
     c->d_par = (DiskParams *)dmalloc(sizeof(DiskParams) * (size_t)n, &ok);
     c->d_ist = (InstState *)dmalloc(sizeof(InstState) * (size_t)n, &ok);
     c->d_ann = (Annulus *)dmalloc(sizeof(Annulus) * A, &ok);
     c->d_cell_ann = (int *)dmalloc(sizeof(int) * N, &ok);
     c->d_slot_ann = (int *)dmalloc(sizeof(int) * (S ? S : 1), &ok);
-    c->d.prim = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
-    c->d.cons = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
-    c->d.rkcons = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
-    c->d.grad = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
-    c->d.gradp = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    c->d.prim = (double *)dmalloc(sizeof(double) * NQ * N, &ok);
+    c->d.cons = (double *)dmalloc(sizeof(double) * NQ * N, &ok);
+    c->d.rkcons = (double *)dmalloc(sizeof(double) * NQ * N, &ok);
+    c->d.grad = (double *)dmalloc(sizeof(double) * NQ * N, &ok);
+    c->d.gradp = (double *)dmalloc(sizeof(double) * NQ * N, &ok);
     c->d.tiph0 = (double *)dmalloc(sizeof(double) * N, &ok);
     c->d.tiph1 = (double *)dmalloc(sizeof(double) * N, &ok);
     c->d.tiphw = (double *)dmalloc(sizeof(double) * N, &ok);
     c->d.rktiph = (double *)dmalloc(sizeof(double) * N, &ok);
     c->d.dphi = (double *)dmalloc(sizeof(double) * N, &ok);
     c->d.w_ann = (double *)dmalloc(sizeof(double) * A, &ok);
-    c->d.fphi = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
-    c->d.frf = (double *)dmalloc(sizeof(double) * 8 * (S ? S : 1), &ok);
-    c->d.fS = (double *)dmalloc(sizeof(double) * 5 * (S ? S : 1), &ok);
+    c->d.fphi = (double *)dmalloc(sizeof(double) * NF * N, &ok);
+    c->d.frf = (double *)dmalloc(sizeof(double) * NF * (S ? S : 1), &ok);
+    c->d.fS = (double *)dmalloc(sizeof(double) * NQ * (S ? S : 1), &ok);
     c->d.src = (double *)dmalloc(sizeof(double) * 8 * N, &ok);
     c->d.fdp = (double *)dmalloc(sizeof(double) * 2 * (S ? S : 1), &ok);
     c->d.ann_c = (double *)dmalloc(sizeof(double) * 4 * A, &ok);
@@ -363,8 +369,8 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.mdot_part = (double *)dmalloc(sizeof(double) * 2 * (size_t)c->n_upd_blocks, &ok);
     c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
     c->d.err = (int *)dmalloc(sizeof(int), &ok);
-    if (n_ob > 0) c->d.obuf = (double *)dmalloc(sizeof(double) * 5 * (size_t)n_ob, &ok);
-    c->d_stage = (double *)dmalloc(sizeof(double) * 5 * (size_t)maxcells, &ok);
+    if (n_ob > 0) c->d.obuf = (double *)dmalloc(sizeof(double) * NQ * (size_t)n_ob, &ok);
+    c->d_stage = (double *)dmalloc(sizeof(double) * NQ * (size_t)maxcells, &ok);
     c->d_torque = (double *)dmalloc(sizeof(double) * ((size_t)maxcells / dgk_block_size() + 8), &ok);
   }
   if (!ok) {
@@ -389,6 +395,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   c->d.n_slots = c->n_slots;
   c->d.n_runs = c->n_runs;
   c->d.n_ob = c->n_ob;
+  c->d.n_pass = c->n_pass;
   c->d.par = c->d_par;
   c->d.ist = c->d_ist;
   c->d.ann = c->d_ann;
@@ -450,8 +457,9 @@ static int upload_disk(struct dgpu_ctx *c, int inst, const double *prim, const d
   const DiskParams *p = &c->h_par[inst];
   int n = p->n_cells, base = p->cell_base;
   if (prim) {
-    CK(cudaMemcpyAsync(c->d_stage, prim, sizeof(double) * 5 * (size_t)n, cudaMemcpyHostToDevice, c->stream));
-    CKK(dgk_aos_to_soa(c->d.prim, 5, c->n_cells, base, c->d_stage, n, c->stream));
+    const int nq = 5 + p->num_n;
+    CK(cudaMemcpyAsync(c->d_stage, prim, sizeof(double) * nq * (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    CKK(dgk_aos_to_soa(c->d.prim, nq, c->n_cells, base, c->d_stage, n, c->stream));
   }
   if (tiph) CK(cudaMemcpyAsync(c->d.tiph0 + base, tiph, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
   if (dphi) CK(cudaMemcpyAsync(c->d.dphi + base, dphi, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, c->stream));
@@ -475,13 +483,15 @@ int dgpu_get_state(dgpu_ctx *c, int inst, double *prim, double *cons, double *ti
   n = p->n_cells;
   base = p->cell_base;
   if (prim) {
-    CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, c->d.prim, n, c->stream));
-    CK(cudaMemcpyAsync(prim, c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    CKK(dgk_soa_to_aos(c->d_stage, 5 + p->num_n, c->n_cells, base, c->d.prim, n, c->stream));
+    CK(cudaMemcpyAsync(prim, c->d_stage, sizeof(double) * (5 + p->num_n) * (size_t)n, cudaMemcpyDeviceToHost,
+                       c->stream));
     if (cons) CK(cudaStreamSynchronize(c->stream));
   }
   if (cons) {
-    CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, c->d.cons, n, c->stream));
-    CK(cudaMemcpyAsync(cons, c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    CKK(dgk_soa_to_aos(c->d_stage, 5 + p->num_n, c->n_cells, base, c->d.cons, n, c->stream));
+    CK(cudaMemcpyAsync(cons, c->d_stage, sizeof(double) * (5 + p->num_n) * (size_t)n, cudaMemcpyDeviceToHost,
+                       c->stream));
   }
   if (tiph) CK(cudaMemcpyAsync(tiph, c->d.tiph0 + base, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
   if (dphi) CK(cudaMemcpyAsync(dphi, c->d.dphi + base, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
@@ -502,8 +512,9 @@ int dgpu_get_stage_data(dgpu_ctx *c, int inst, double *grad, double *gradp, doub
     int k;
     for (k = 0; k < 3; ++k) {
       if (!dsts[k]) continue;
-      CKK(dgk_soa_to_aos(c->d_stage, 5, c->n_cells, base, srcs[k], n, c->stream));
-      CK(cudaMemcpyAsync(dsts[k], c->d_stage, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+      CKK(dgk_soa_to_aos(c->d_stage, 5 + p->num_n, c->n_cells, base, srcs[k], n, c->stream));
+      CK(cudaMemcpyAsync(dsts[k], c->d_stage, sizeof(double) * (5 + p->num_n) * (size_t)n, cudaMemcpyDeviceToHost,
+                         c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
   }
@@ -596,7 +607,7 @@ int dgpu_init_state(dgpu_ctx *c, int inst) {
   int rc = check_inst(c, inst);
   if (rc) return rc;
   s = c->sims[inst];
-  prim = (double *)malloc(sizeof(double) * 5 * (size_t)s->Ncells);
+  prim = (double *)malloc(sizeof(double) * (size_t)s->NQ * (size_t)s->Ncells);
   tiph = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
   dphi = (double *)malloc(sizeof(double) * (size_t)s->Ncells);
   if (!prim || !tiph || !dphi) {
@@ -773,7 +784,7 @@ int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
     for (k = 0; k < DGPU_TUNE_N; ++k) c->d.tune[k] = choice[k];
   } else {
     /* save the state, time each candidate from it, restore it */
-    if (cudaMalloc((void **)&buf, sizeof(double) * 19 * (size_t)c->n_cells) != cudaSuccess ||
+    if (cudaMalloc((void **)&buf, sizeof(double) * (19 + 3 * (size_t)c->n_pass) * (size_t)c->n_cells) != cudaSuccess ||
         cudaMalloc((void **)&ist, sizeof(InstState) * (size_t)c->n_inst) != cudaSuccess) {
       cudaFree(buf);
       cudaGetLastError();

@@ -25,6 +25,7 @@ struct dgpu_ctx {
   Annulus *h_ann;
   int n_ann, n_cells, n_slots, n_runs, n_upd_blocks;
   int n_ob;              /* cells in d.obuf (0: no disk has an outflow radial boundary) */
+  int n_pass;            /* passive-scalar planes (largest NUM_N) */
   DevPtrs d;          /* device pointers */
   DiskParams *d_par;
   InstState *d_ist;

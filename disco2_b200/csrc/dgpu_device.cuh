@@ -334,7 +334,14 @@ HD void prim2cons(const T *p, T *U, double r, double dV, double gam) {
 }
 
 template <typename T>
-HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, double gam, int solver, T *F) {
+// np passive scalars (face states qL, qR) ride on the mass flux: their
+// physical flux and conserved value are q F_D and q U_D (riemann_set_flux,
+// Riemann_routines.c:184-189; cell_prim2cons, cell_conversion.c:28-31), their
+// HLL star state follows Toro's formulas like the others and their HLLC star
+// state is q U*_D (riemann_set_star_hllc, Riemann_routines.c:143-146).  The
+// differentiated runs carry no passive scalar (np = 0).
+HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, double gam, int solver, T *F,
+                     int np = 0, const double *qL = nullptr, const double *qR = nullptr, double *Fq = nullptr) {
   const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = 0.0;
   T vnL, cf2L, vnR, cf2R;
   {
@@ -366,6 +373,11 @@ HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, doub
     prim2cons(p, Uk, r, 1.0, gam);
 #pragma unroll
     for (int q = 0; q < 5; ++q) F[q] = Fk[q] - w * Uk[q];
+    for (int k = 0; k < np; ++k) {
+      const double qk = state == DS_LEFT ? qL[k] : qR[k];
+      const double Fkq = qk * val(Fk[D_DDD]), Ukq = qk * val(Uk[D_DDD]);
+      Fq[k] = Fkq - w * Ukq;
+    }
     return;
   }
   T Ustar[5], Fstar[5];
@@ -379,6 +391,14 @@ HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, doub
     for (int q = 0; q < 5; ++q) {
       Ustar[q] = (Sr * UR[q] - Sl * UL[q] + FL[q] - FR[q]) / (Sr - Sl);
       Fstar[q] = (Sr * FL[q] - Sl * FR[q] - Sr * Sl * (UL[q] - UR[q])) / (Sr - Sl);
+    }
+    for (int k = 0; k < np; ++k) {
+      const double sr = val(Sr), sl = val(Sl);
+      const double FLq = qL[k] * val(FL[D_DDD]), FRq = qR[k] * val(FR[D_DDD]);
+      const double ULq = qL[k] * val(UL[D_DDD]), URq = qR[k] * val(UR[D_DDD]);
+      const double Usq = (sr * URq - sl * ULq + FLq - FRq) / (sr - sl);
+      const double Fsq = (sr * FLq - sl * FRq - sr * sl * (ULq - URq)) / (sr - sl);
+      Fq[k] = Fsq - w * Usq;
     }
   } else {
     const T *prim = state == DS_LEFTSTAR ? pL : pR;
@@ -416,6 +436,13 @@ HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, doub
     Ustar[D_TAU] = Estar;
 #pragma unroll
     for (int q = 0; q < 5; ++q) Fstar[q] = Fk[q] + Sk * (Ustar[q] - Uk[q]);
+    for (int k = 0; k < np; ++k) {
+      const double qk = state == DS_LEFTSTAR ? qL[k] : qR[k];
+      const double Fkq = qk * val(Fk[D_DDD]), Ukq = qk * val(Uk[D_DDD]);
+      const double Usq = qk * val(Ustar[D_DDD]);
+      const double Fsq = Fkq + val(Sk) * (Usq - Ukq);
+      Fq[k] = Fsq - w * Usq;
+    }
   }
 #pragma unroll
   for (int q = 0; q < 5; ++q) F[q] = Fstar[q] - w * Ustar[q];

@@ -57,9 +57,9 @@ __global__ void __launch_bounds__(DIAG_BLK) k_diag_annulus(DevPtrs d, int inst, 
       const double KE = 0.5 * rho * v2;
       const double E_hydro = rhoe + KE;
       const double dV = 0.5 * (rp * rp - rm * rm) * dphi;
-      // cells with no cooling keep Cool = 0; with NUM_Q = 5 there is no
-      // passive scalar (the reference reads past prim[] there)
-      const double cool = 0.0, passive = 0.0;
+      // cells with no cooling keep Cool = 0; the passive column is prim[NUM_C]
+      // (with NUM_Q = 5 the reference reads past prim[] there; zero here)
+      const double cool = 0.0, passive = P.num_n > 0 ? ld(d.prim, 5, N, g) : 0.0;
       const double col[DIAG_NVEC] = {r, rho, press, vr, vp, vz, vp_minus_w, cool, passive, E_hydro, KE, rhoe,
                                      0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll

@@ -15,6 +15,7 @@
 #include <stdint.h>
 
 #define DGPU_NQ 5
+#define DGPU_MAX_PASSIVE 3  /* NUM_N at most */
 #define DGPU_FACE_SLACK 8
 #define DGPU_RUN_SLACK 8
 #define DGPU_WRAP_LIMIT 64
@@ -67,6 +68,7 @@ typedef struct {
   int has_damp;     /* DAMP_TIME > 0 */
   int num_sinks;    /* GravMassType (cell_source.c:177) */
   int outflow;      /* bit 0: outflow radial boundary; bit 1: also the inner annulus (NoInnerBC != 1) */
+  int num_n;        /* passive scalars (NUM_N): planes 5.. of prim, cons, rkcons, grad, gradp */
   double gamma, plm, cfl, visc, g_eps;
   double rho_floor, cs_floor, cs_cap, vel_cap;
   double t_max, poro_r1, orb_tscale, orb_t0;
@@ -151,9 +153,12 @@ typedef struct {
   double *mdot_part;      /* [n_blocks_update][2] per-block sink sums */
   unsigned int *counters; /* last-block counters */
   int *err;               /* error flags */
-  double *obuf;           /* [5][n_ob] prims, before damping, of the annuli the outflow boundary
-                             reads or writes (k_update writes them, k_outflow finishes them) */
+  double *obuf;           /* [5 + n_pass][n_ob] prims, before damping, of the annuli the outflow
+                             boundary reads or writes (k_update writes them, k_outflow finishes them) */
   int n_ob;
+  int n_pass;             /* passive-scalar planes (largest NUM_N of the disks): prim, cons, rkcons,
+                             grad and gradp hold 5 + n_pass planes, fS 5 + n_pass, fphi and frf
+                             8 + n_pass (the passive increments after the viscous ones) */
   int tune[DGPU_TUNE_N];  /* host-side launch choice of the tuned kernels: resident blocks per SM (0: built-in) */
 } DevPtrs;
 

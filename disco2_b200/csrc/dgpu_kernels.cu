@@ -180,6 +180,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
         pr = ldq<T>(d.prim, tp.prim, q, N, gr);
       stq<T>(d.gradp, tp.gradp, q, N, g, plm_p_slope(pl, pc, pr, dpL, dpR, P.plm));
     }
+    for (int q = 5; q < 5 + P.num_n; ++q)
+      d.gradp[(size_t)q * N + g] = plm_p_slope(ld(d.prim, q, N, gl), ld(d.prim, q, N, g), ld(d.prim, q, N, gr), dpL, dpR, P.plm);
   }
   if (g == P.cell_base) {
     InstState &S = d.ist[A.inst];
@@ -434,6 +436,11 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
     T WR = ldqr<T>(d.prim, tp.prim, q, N, cR) - dpR * ldqr<T>(d.gradp, tp.gradp, q, N, cR);
     stq<T>(d.fS, tp.fS, q, NS, slot, (WR - WL) / den);
   }
+  for (int q = 5; q < 5 + d.par[A.inst].num_n; ++q) {
+    const double WL = ldr(d.prim, q, N, cL) + dpL * ldr(d.gradp, q, N, cL);
+    const double WR = ldr(d.prim, q, N, cR) - dpR * ldr(d.gradp, q, N, cR);
+    d.fS[(size_t)q * NS + slot] = (WR - WL) / den;
+  }
 }
 
 template <typename T, int MB = DGPU_MINB_PLM>
@@ -466,8 +473,9 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
 #pragma unroll
       for (int q = 0; q < 5; ++q) gq[q] += ldq<T>(d.fS, tp.fS, q, NS, slot) * dA;
     });
+    double dAtot;
     {
-      double dz = P.dz, dp = d.dphi[g], dAtot;
+      double dz = P.dz, dp = d.dphi[g];
       if (A.i == 0) dAtot = dz * A.rp * dp;
       else if (A.i == P.NR - 1) dAtot = dz * A.rm * dp;
       else dAtot = dz * (A.rp + A.rm) * dp;
@@ -482,6 +490,21 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
         else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
       }
     });
+    // passive scalars: the same face-weighted slope and limiter
+    for (int q = 5; q < 5 + P.num_n; ++q) {
+      double gs = 0.0;
+      for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+        double dA = F.r * F.dphi * F.dperp;
+        gs += ld(d.fS, q, NS, slot) * dA;
+      });
+      gs /= dAtot;
+      for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+        const double Sq = ld(d.fS, q, NS, slot);
+        if (Sq * gs < 0.0) gs = 0.0;
+        else if (fabs(P.plm * Sq) < fabs(gs)) gs = P.plm * Sq;
+      });
+      d.grad[(size_t)q * N + g] = gs;
+    }
 #pragma unroll
     for (int q = 0; q < 5; ++q) stq<T>(d.grad, tp.grad, q, N, g, gq[q]);
 
@@ -605,11 +628,18 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   }
   const double w = d.w_ann[a];
   T F[5];
-  riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F);
+  double qL[DGPU_MAX_PASSIVE], qR[DGPU_MAX_PASSIVE], Fq[DGPU_MAX_PASSIVE];
+  const int np = P.num_n;
+  for (int s = 0; s < np; ++s) {
+    qL[s] = ld(d.prim, 5 + s, N, cL) + 0.5 * ld(d.gradp, 5 + s, N, cL) * dpL;
+    qR[s] = ld(d.prim, 5 + s, N, cR) - 0.5 * ld(d.gradp, 5 + s, N, cR) * dpR;
+  }
+  riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F, np, qL, qR, Fq);
   const double dt = fac * S.dt;
   const double k = dt * dA;
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.fphi, tp.fphi, q, N, g, k * F[q]);
+  for (int s = 0; s < np; ++s) d.fphi[(size_t)(8 + s) * N + g] = k * Fq[s];
   if (P.has_visc) {
     ViscIn<T> v;
 #pragma unroll
@@ -669,12 +699,19 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
             ldq<T>(d.gradp, tp.gradp, q, N, cR) * dpR;
   }
   T F[5];
-  riemann_flux(pL, pR, r, 0, 0.0, P.gamma, P.riemann, F);
+  double qL[DGPU_MAX_PASSIVE], qR[DGPU_MAX_PASSIVE], Fq[DGPU_MAX_PASSIVE];
+  const int np = P.num_n;
+  for (int s = 0; s < np; ++s) {
+    qL[s] = ld(d.prim, 5 + s, N, cL) + ld(d.grad, 5 + s, N, cL) * deltaL + ld(d.gradp, 5 + s, N, cL) * dpL;
+    qR[s] = ld(d.prim, 5 + s, N, cR) - ld(d.grad, 5 + s, N, cR) * deltaR - ld(d.gradp, 5 + s, N, cR) * dpR;
+  }
+  riemann_flux(pL, pR, r, 0, 0.0, P.gamma, P.riemann, F, np, qL, qR, Fq);
   const double dt = fac * S.dt;
   const double k = dt * dA;
   const int NS = d.n_slots;
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.frf, tp.frf, q, NS, slot, k * F[q]);
+  for (int s = 0; s < np; ++s) d.frf[(size_t)(8 + s) * NS + slot] = k * Fq[s];
   if (P.has_visc) {
     ViscIn<T> v;
 #pragma unroll
@@ -885,9 +922,13 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     const InstState &S = d.ist[A.inst];
     const double dt = fac * S.dt;
     T c[5];
+    double cp[DGPU_MAX_PASSIVE], pp[DGPU_MAX_PASSIVE];
+    const int np = P.num_n;
+    if (np > 0) passive_sum(d, A, a, g, substep, stop, np, cp);
     if (!update_sum(d, tp, A, a, g, substep, stop, dt, true, c)) {
 #pragma unroll
       for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
+      for (int k = 0; k < np; ++k) d.cons[(size_t)(5 + k) * N + g] = cp[k];
     } else {
       double tn, rk;
       const double dphi_n = mesh_advance(d, A, a, g, substep, dt, tn, rk);
@@ -905,20 +946,36 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
       const double dV = A.dv_half * dphi_n * P.dz;
       T pr[5];
       cons2prim(c, dV, r, P, pr);
+      // passive scalars: prim = cons / cons[DDD] (cell_conversion.c:98-101)
+      for (int k = 0; k < np; ++k) pp[k] = cp[k] / val(c[D_DDD]);
       // the outflow boundary reads these prims before any damping; the
       // annuli it rewrites are damped and converted by k_outflow
       if (A.ob_off >= 0 && stop >= 6) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) d.obuf[(size_t)q * d.n_ob + A.ob_off + (g - A.cell_off)] = val(pr[q]);
+        for (int k = 0; k < np; ++k) d.obuf[(size_t)(5 + k) * d.n_ob + A.ob_off + (g - A.cell_off)] = pp[k];
       }
       const bool own = !(A.kind & DGPU_AK_OUT_DST);
-      if (stop >= 6 && own) bc_damp(d, A, a, pr);
+      if (stop >= 6 && own) {
+        bc_damp(d, A, a, pr);
+        // cell_single_init_vortex's dye at the cell's new phi, in the fixed
+        // boundary (cell_init_vortex.c:22-35); no other family sets one
+        if (np > 0 && P.init_type == DI_VORTEX && (A.kind & DGPU_AK_BC_FIXED) && (A.kind & DGPU_AK_IC))
+          pp[0] = cos(tn - .5 * dphi_n) < 0.0 ? 0.0 : 1.0;
+      }
       // cell_calc_cons (src/Cell/cell_conversion.c:35-55)
-      if (stop >= 7 && own) prim2cons(pr, c, r, dV, P.gamma);
+      if (stop >= 7 && own) {
+        prim2cons(pr, c, r, dV, P.gamma);
+        for (int k = 0; k < np; ++k) cp[k] = pp[k] * val(c[D_DDD]);
+      }
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
         stq<T>(d.prim, tp.prim, q, N, g, pr[q]);
         stq<T>(d.cons, tp.cons, q, N, g, c[q]);
+      }
+      for (int k = 0; k < np; ++k) {
+        d.prim[(size_t)(5 + k) * N + g] = pp[k];
+        d.cons[(size_t)(5 + k) * N + g] = cp[k];
       }
     }
   }
@@ -1008,6 +1065,7 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   prim2cons(p, c, r, dV, P.gamma);
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
+  for (int q = 5; q < 5 + P.num_n; ++q) d.cons[(size_t)q * N + g] = ld(d.prim, q, N, g) * val(c[D_DDD]);
 }
 
 // One pass of cell_boundary_outflow_r (src/Cell/cell_boundary.c:14-139) over
@@ -1025,22 +1083,22 @@ __device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int i, int o
   const Annulus &S = d.ann[P.ann_base + i + 1 - outer];  // the annulus read
   const double rf = d.ann[P.ann_base + i].f_r;           // FacePos(i)
   const size_t NB = d.n_ob;
+  const int nq = 5 + P.num_n;
   for (int j = threadIdx.x; j < A.np; j += blockDim.x) {
     const int g = A.cell_off + j;
-    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double s[5 + DGPU_MAX_PASSIVE];
+    for (int q = 0; q < nq; ++q) s[q] = 0.0;
     int nface = 0;
     for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int side) {
       if (side != outer) return;
       const int o = S.ob_off + ((outer ? F.cL : F.cR) - S.cell_off);
       const double dA = F.r * F.dphi * F.dperp;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) s[q] += d.obuf[q * NB + o] * dA;
+      for (int q = 0; q < nq; ++q) s[q] += d.obuf[q * NB + o] * dA;
       ++nface;
     });
     const double dA = P.dz * rf * d.dphi[g];
     const size_t self = (size_t)A.ob_off + j;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
+    for (int q = 0; q < nq; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
   }
 }
 
@@ -1073,11 +1131,13 @@ __global__ void __launch_bounds__(BLK) k_outflow(DevPtrs d, int stop) {
       bc_damp(d, A, a, pr);
 #pragma unroll
       for (int q = 0; q < 5; ++q) d.prim[(size_t)q * N + g] = pr[q];
+      for (int q = 5; q < 5 + P.num_n; ++q) d.prim[(size_t)q * N + g] = d.obuf[q * NB + A.ob_off + j];
       if (stop >= 7) {
         const double dV = A.dv_half * d.dphi[g] * P.dz;
         prim2cons(pr, c, r, dV, P.gamma);
 #pragma unroll
         for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+        for (int q = 5; q < 5 + P.num_n; ++q) d.cons[(size_t)q * N + g] = d.obuf[q * NB + A.ob_off + j] * c[D_DDD];
       }
     }
   }

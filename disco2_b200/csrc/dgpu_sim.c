@@ -488,7 +488,10 @@ int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, doubl
   double rm = dsim_rface(s, i - 1);
   double rp = dsim_rface(s, i);
   double r = 0.5 * (rm + rp);
-  int t = s->InitialDataType;
+  int t = s->InitialDataType, q;
+  /* passive scalars: only cell_init_vortex sets one (below); the reference
+   * leaves them as cell_create's allocation gives them, zero here */
+  for (q = DGPU_NQ; q < s->NQ; ++q) prim[q] = 0.0;
   if (t == DI_SHEAR) {
     /* cell_init_shear (src/Cell/initial_data/cell_init_shear.c:57-116) */
     double rho = 1.0, Pp = 0.01, v0 = 1.0, t0 = 0.25;
@@ -603,8 +606,10 @@ int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, doubl
   if (t == DI_VORTEX) {
     /* cell_init_vortex leaves r >= R cells at cell_create's zeros */
     if (dsim_single_init(s, i, prim) == 0) {
-      int q;
       for (q = 0; q < DGPU_NQ; ++q) prim[q] = 0.0;
+    } else if (s->NQ > DGPU_NQ) {
+      /* the dye: 1 where cos(phi) >= 0 (cell_init_vortex.c:64-68) */
+      prim[DGPU_NQ] = cos(tiph - .5 * dphi) < 0.0 ? 0.0 : 1.0;
     }
     return 0;
   }
@@ -632,6 +637,7 @@ void dsim_fill_params(const struct dgpu_sim *s, DiskParams *p) {
   p->has_damp = s->DAMP_TIME > 0.0;
   p->num_sinks = s->GravMassType;
   p->outflow = s->BoundTypeR == DB_OUTFLOW ? (1 | (s->NoInnerBC != 1 ? 2 : 0)) : 0;
+  p->num_n = s->NUM_N;
   p->gamma = s->Adiabatic_Index;
   p->plm = s->PLM;
   p->cfl = s->CFL;

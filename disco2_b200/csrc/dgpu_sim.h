@@ -63,7 +63,7 @@ double dsim_dtOm_a(const struct dgpu_sim *s, double r, double a);
 int dsim_single_init(const struct dgpu_sim *s, int i, double *prim);
 
 /* Whole-grid initial data (cell_init_*) for cell j of annulus i with global
- * (k,i,j) cell number idx (noise included).  tiph, dphi: the cell's phi edge
+ * (k,i,j) cell number idx (noise included), NQ = 5 + NUM_N values.  tiph, dphi: the cell's phi edge
  * and width after cell_create and cell_clean_pi; gm: the GravMass state
  * (dsim_initial_gravmass); rnd: the generator of cell_init_torus, seeded like
  * srand(666), drawn once per cell for that type only.  Returns 0 or -1

@@ -196,6 +196,49 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
   return stop > 4;
 }
 
+// The conserved sums of a cell's passive scalars (planes 5.. of cons): the RK
+// blend and the phi and r face increments (planes 8.. of fphi and frf) in the
+// same order as update_sum; no source acts on them.  Writes rkcons in
+// substep 1.
+__device__ __forceinline__ void passive_sum(const DevPtrs &d, const Annulus &A, int a, int g, int substep,
+                                            int stop, int np, double *cp) {
+  const int N = d.n_cells, NS = d.n_slots;
+  const int j = g - A.cell_off;
+  const double RK = substep == 1 ? 0.0 : 0.5;
+  for (int k = 0; k < np; ++k) {
+    const double cq = ld(d.cons, 5 + k, N, g);
+    double rk;
+    if (substep == 1) {
+      rk = cq;
+      d.rkcons[(size_t)(5 + k) * N + g] = cq;
+    } else {
+      rk = ld(d.rkcons, 5 + k, N, g);
+    }
+    cp[k] = (1.0 - RK) * cq + RK * rk;
+  }
+  if (stop <= 1) return;
+  {
+    const int gl = j == 0 ? A.cell_off + A.np - 1 : g - 1;
+    for (int k = 0; k < np; ++k) {
+      if (j == 0) {
+        cp[k] -= ld(d.fphi, 8 + k, N, g);
+        cp[k] += ld(d.fphi, 8 + k, N, gl);
+      } else {
+        cp[k] += ld(d.fphi, 8 + k, N, gl);
+        cp[k] -= ld(d.fphi, 8 + k, N, g);
+      }
+    }
+  }
+  if (stop == 2) return;
+  for_cell_rface_ranges(d, A, a, g, d.par[A.inst].NR, [&](int s, int e, int asR) {
+    for (int n = s; n < e; ++n)
+      for (int k = 0; k < np; ++k) {
+        if (asR) cp[k] += ld(d.frf, 8 + k, NS, n);
+        else cp[k] -= ld(d.frf, 8 + k, NS, n);
+      }
+  });
+}
+
 // cell_update_phi + cell_update_dphi (src/Cell/cell_misc.c:59-96): the new
 // phi edge tn of cell g, its RK copy rk and the new width.
 __device__ __forceinline__ double mesh_advance(const DevPtrs &d, const Annulus &A, int a, int g, int substep,

@@ -108,6 +108,8 @@ class Sim:
         self._h = h
         self.num_annuli = lib.dgpu_sim_num_annuli(h)
         self.num_cells = lib.dgpu_sim_num_cells(h)
+        # NUM_Q: the five hydro variables and the passive scalars (NUM_N)
+        self.num_q = 5 + int(self.param("NUM_N"))
 
     def grid(self):
         N_p = np.zeros(self.num_annuli, np.int32)
@@ -125,7 +127,7 @@ class Sim:
     def initial_state(self) -> dict:
         """Host-computed initial state (what Context.init_state uploads)."""
         n = self.num_cells
-        out = {"prim": np.zeros((n, 5)), "tiph": np.zeros(n), "dphi": np.zeros(n),
+        out = {"prim": np.zeros((n, self.num_q)), "tiph": np.zeros(n), "dphi": np.zeros(n),
                "gm": np.zeros((2, 6))}
         rc = load().dgpu_sim_initial_state(self._h, _dptr(out["prim"]), _dptr(out["tiph"]),
                                           _dptr(out["dphi"]), _dptr(out["gm"]))
@@ -175,23 +177,23 @@ class Context:
         tiph = np.ascontiguousarray(tiph, np.float64)
         dphi = np.ascontiguousarray(dphi, np.float64)
         n = self.sims[inst].num_cells
-        assert prim.shape == (n, 5) and tiph.shape == (n,) and dphi.shape == (n,)
+        assert prim.shape == (n, self.sims[inst].num_q) and tiph.shape == (n,) and dphi.shape == (n,)
         self._ck(load().dgpu_set_state(self._h, inst, _dptr(prim), _dptr(tiph), _dptr(dphi)))
         self._ck(load().dgpu_synchronize(self._h))
 
     def get_state(self, inst: int = 0) -> dict:
-        n = self.sims[inst].num_cells
-        prim = np.zeros((n, 5))
-        cons = np.zeros((n, 5))
+        n, nq = self.sims[inst].num_cells, self.sims[inst].num_q
+        prim = np.zeros((n, nq))
+        cons = np.zeros((n, nq))
         tiph = np.zeros(n)
         dphi = np.zeros(n)
         self._ck(load().dgpu_get_state(self._h, inst, _dptr(prim), _dptr(cons), _dptr(tiph), _dptr(dphi)))
         return {"prim": prim, "cons": cons, "tiph": tiph, "dphi": dphi}
 
     def stage_data(self, inst: int = 0) -> dict:
-        n = self.sims[inst].num_cells
-        out = {"grad": np.zeros((n, 5)), "gradp": np.zeros((n, 5)), "wiph": np.zeros(n),
-               "RKcons": np.zeros((n, 5)), "RKtiph": np.zeros(n)}
+        n, nq = self.sims[inst].num_cells, self.sims[inst].num_q
+        out = {"grad": np.zeros((n, nq)), "gradp": np.zeros((n, nq)), "wiph": np.zeros(n),
+               "RKcons": np.zeros((n, nq)), "RKtiph": np.zeros(n)}
         self._ck(load().dgpu_get_stage_data(self._h, inst, _dptr(out["grad"]), _dptr(out["gradp"]),
                                             _dptr(out["wiph"]), _dptr(out["RKcons"]),
                                             _dptr(out["RKtiph"])))

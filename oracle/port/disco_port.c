@@ -411,6 +411,7 @@ static void prim2cons(const Port *p, const double *prim, double *cons, double r,
   cons[LLL] = r * rho * vp * dV;
   cons[SZZ] = rho * vz * dV;
   cons[TAU] = (.5 * rho * v2 + rhoe) * dV;
+  for (int q = 5; q < p->NQ; ++q) cons[q] = prim[q] * cons[DDD]; /* passive scalars */
 }
 static void cons2prim(const Port *p, const double *cons, double *prim, double r, double dV) {
   double CS_FLOOR = p->Cs_Floor, CS_CAP = p->Cs_Cap, RHO_FLOOR = p->Rho_Floor, VEL_CAP = p->Vel_Cap;
@@ -437,6 +438,7 @@ static void cons2prim(const Port *p, const double *cons, double *prim, double r,
     vz = vz * VEL_CAP / v_magnitude;
   }
   prim[RHO] = rho; prim[PPP] = Pp; prim[URR] = vr; prim[UPP] = vp / r; prim[UZZ] = vz;
+  for (int q = 5; q < p->NQ; ++q) prim[q] = cons[q] / cons[DDD]; /* passive scalars */
 }
 
 void port_calc_cons(Port *p) {
@@ -447,10 +449,10 @@ void port_calc_cons(Port *p) {
     for (j = 0; j < p->N_p[i]; ++j) {
       int g = p->off[i] + j;
       double dV = .5 * (rp * rp - rm * rm) * p->dphi[g] * dz;
-      double pr[5], c[5];
-      for (q = 0; q < 5; ++q) pr[q] = p->prim[q][g];
+      double pr[PORT_MAXQ], c[PORT_MAXQ];
+      for (q = 0; q < p->NQ; ++q) pr[q] = p->prim[q][g];
       prim2cons(p, pr, c, r, dV);
-      for (q = 0; q < 5; ++q) p->cons[q][g] = c[q];
+      for (q = 0; q < p->NQ; ++q) p->cons[q][g] = c[q];
     }
   }
 }
@@ -463,10 +465,10 @@ static void calc_prim(Port *p) {
     for (j = 0; j < p->N_p[i]; ++j) {
       int g = p->off[i] + j;
       double dV = .5 * (rp * rp - rm * rm) * p->dphi[g] * dz;
-      double c[5], pr[5];
-      for (q = 0; q < 5; ++q) c[q] = p->cons[q][g];
+      double c[PORT_MAXQ], pr[PORT_MAXQ];
+      for (q = 0; q < p->NQ; ++q) c[q] = p->cons[q][g];
       cons2prim(p, c, pr, r, dV);
-      for (q = 0; q < 5; ++q) p->prim[q][g] = pr[q];
+      for (q = 0; q < p->NQ; ++q) p->prim[q][g] = pr[q];
     }
   }
 }
@@ -475,12 +477,13 @@ static void calc_prim(Port *p) {
 int port_setup(Port *p) {
   int i, j, q;
   long idx = 0;
-  if (p->NumZ != 1 || p->NUM_C != 5 || p->NUM_N != 0) {
-    fprintf(stderr, "port: only 2-D, NUM_Q = 5 disks are restated\n");
+  if (p->NumZ != 1 || p->NUM_C != 5 || p->NUM_N < 0 || 5 + p->NUM_N > PORT_MAXQ) {
+    fprintf(stderr, "port: only 2-D disks with NUM_C = 5 and NUM_Q <= %d are restated\n", PORT_MAXQ);
     return 1;
   }
+  p->NQ = 5 + p->NUM_N;
   set_grid(p);
-  for (q = 0; q < 5; ++q) {
+  for (q = 0; q < p->NQ; ++q) {
     p->prim[q] = calloc((size_t)p->N, sizeof(double));
     p->cons[q] = calloc((size_t)p->N, sizeof(double));
     p->rkcons[q] = calloc((size_t)p->N, sizeof(double));
@@ -554,6 +557,10 @@ int port_setup(Port *p) {
       int g = p->off[i] + j;
       if (st == 0) continue; /* vortex leaves r >= R at cell_create's zeros */
       for (q = 0; q < 5; ++q) p->prim[q][g] = prof[q];
+      /* cell_init_vortex's dye: 1 where cos(phi) >= 0 (cell_init_vortex.c:64-68);
+         the other families leave passive scalars at zero */
+      if (p->InitialDataType == VORTEX && p->NQ > 5)
+        p->prim[5][g] = cos(p->tiph[g] - .5 * p->dphi[g]) < 0.0 ? 0.0 : 1.0;
       if (p->InitialDataType >= GRESHO) {
         double f = 1. + p->IC_Noise * noise_u(p->IC_Seed, idx);
         p->prim[RHO][g] = prof[RHO] * f;
@@ -577,7 +584,7 @@ int port_setup(Port *p) {
 
 void port_free(Port *p) {
   int q;
-  for (q = 0; q < 5; ++q) {
+  for (q = 0; q < p->NQ; ++q) {
     free(p->prim[q]); free(p->cons[q]); free(p->rkcons[q]); free(p->grad[q]); free(p->gradp[q]);
   }
   free(p->tiph); free(p->rktiph); free(p->dphi); free(p->wiph); free(p->nri);
@@ -741,7 +748,7 @@ static void plm_p(Port *p) {
     for (j = 0; j < n; ++j) {
       int c = a + j, cL = a + (j == 0 ? n - 1 : j - 1), cR = a + (j == n - 1 ? 0 : j + 1);
       double dpL = .5 * (p->dphi[c] + p->dphi[cL]), dpR = .5 * (p->dphi[c] + p->dphi[cR]);
-      for (q = 0; q < 5; ++q) {
+      for (q = 0; q < p->NQ; ++q) {
         double sL = (p->prim[q][c] - p->prim[q][cL]) / dpL;
         double sR = (p->prim[q][cR] - p->prim[q][c]) / dpR;
         double sM = (p->prim[q][cR] - p->prim[q][cL]) / (dpL + dpR);
@@ -770,12 +777,12 @@ static void face_dps(const Port *p, int n, double *dpL, double *dpR) {
 static void plm_rz(Port *p) {
   double dz = p->zf[1] - p->zf[0];
   int n, q, i, j;
-  for (q = 0; q < 5; ++q) memset(p->grad[q], 0, sizeof(double) * (size_t)p->N);
+  for (q = 0; q < p->NQ; ++q) memset(p->grad[q], 0, sizeof(double) * (size_t)p->N);
   for (n = 0; n < p->nf; ++n) {
     int cL = p->fL[n], cR = p->fR[n];
     double dpL, dpR;
     face_dps(p, n, &dpL, &dpR);
-    for (q = 0; q < 5; ++q) {
+    for (q = 0; q < p->NQ; ++q) {
       double WL = p->prim[q][cL] + dpL * p->gradp[q][cL];
       double WR = p->prim[q][cR] - dpR * p->gradp[q][cR];
       double S = (WR - WL) / (p->fdr[n] + p->fdl[n]);
@@ -791,14 +798,14 @@ static void plm_rz(Port *p) {
       if (i == 0) dAtot = dz * rp * dp;
       else if (i == p->NR - 1) dAtot = dz * rm * dp;
       else dAtot = dz * (rp + rm) * dp;
-      for (q = 0; q < 5; ++q) p->grad[q][g] /= dAtot;
+      for (q = 0; q < p->NQ; ++q) p->grad[q][g] /= dAtot;
     }
   }
   for (n = 0; n < p->nf; ++n) {
     int cL = p->fL[n], cR = p->fR[n];
     double dpL, dpR;
     face_dps(p, n, &dpL, &dpR);
-    for (q = 0; q < 5; ++q) {
+    for (q = 0; q < p->NQ; ++q) {
       double WL = p->prim[q][cL] + dpL * p->gradp[q][cL];
       double WR = p->prim[q][cR] - dpR * p->gradp[q][cR];
       double S = (WR - WL) / (p->fdr[n] + p->fdl[n]);
@@ -815,7 +822,8 @@ static void plm_rz(Port *p) {
 typedef struct {
   int cL, cR, n[3];
   double r, r_cell_L, r_cell_R, dA, cm;
-  double primL[5], primR[5], UL[5], UR[5], Ustar[5], FL[5], FR[5], Fstar[5], F[5], Fvisc[5];
+  double primL[PORT_MAXQ], primR[PORT_MAXQ], UL[PORT_MAXQ], UR[PORT_MAXQ], Ustar[PORT_MAXQ], FL[PORT_MAXQ],
+      FR[PORT_MAXQ], Fstar[PORT_MAXQ], F[PORT_MAXQ], Fvisc[PORT_MAXQ];
   double Sl, Sr, Ss;
   int state;
 } Rm;
@@ -836,6 +844,7 @@ static void set_flux(const Port *p, Rm *R, int side) {
   F[LLL] = r * (rho * vp * vn + Pp * R->n[1]);
   F[SZZ] = rho * vz * vn + Pp * R->n[2];
   F[TAU] = (.5 * rho * v2 + rhoe + Pp) * vn;
+  for (int q = 5; q < p->NQ; ++q) F[q] = prim[q] * F[DDD]; /* passive scalars */
 }
 static void star_hllc(const Port *p, Rm *R) {
   double r = R->r, G = p->Adiabatic_Index;
@@ -864,7 +873,8 @@ static void star_hllc(const Port *p, Rm *R) {
     R->Ustar[DDD] = Dstar; R->Ustar[SRR] = Msr; R->Ustar[LLL] = r * Msp; R->Ustar[SZZ] = Msz;
     R->Ustar[TAU] = Estar;
   }
-  for (q = 0; q < 5; ++q) R->Fstar[q] = Fk[q] + Sk * (R->Ustar[q] - Uk[q]);
+  for (q = 5; q < p->NQ; ++q) R->Ustar[q] = prim[q] * R->Ustar[DDD];
+  for (q = 0; q < p->NQ; ++q) R->Fstar[q] = Fk[q] + Sk * (R->Ustar[q] - Uk[q]);
 }
 
 static void visc_flux(const Port *p, Rm *R) {
@@ -944,18 +954,18 @@ static void add_flux(Port *p, Rm *R, double dt) {
   if (R->state == LEFT) {
     set_flux(p, R, LEFT);
     prim2cons(p, R->primL, R->UL, R->r, 1.0);
-    for (q = 0; q < 5; ++q) R->F[q] = R->FL[q] - w * R->UL[q];
+    for (q = 0; q < p->NQ; ++q) R->F[q] = R->FL[q] - w * R->UL[q];
   } else if (R->state == RIGHT) {
     set_flux(p, R, RIGHT);
     prim2cons(p, R->primR, R->UR, R->r, 1.0);
-    for (q = 0; q < 5; ++q) R->F[q] = R->FR[q] - w * R->UR[q];
+    for (q = 0; q < p->NQ; ++q) R->F[q] = R->FR[q] - w * R->UR[q];
   } else {
     if (p->RiemannSolver == HLL) {
       set_flux(p, R, LEFT);
       set_flux(p, R, RIGHT);
       prim2cons(p, R->primL, R->UL, R->r, 1.0);
       prim2cons(p, R->primR, R->UR, R->r, 1.0);
-      for (q = 0; q < 5; ++q) {
+      for (q = 0; q < p->NQ; ++q) {
         R->Ustar[q] = (R->Sr * R->UR[q] - R->Sl * R->UL[q] + R->FL[q] - R->FR[q]) / (R->Sr - R->Sl);
         R->Fstar[q] = (R->Sr * R->FL[q] - R->Sl * R->FR[q] - R->Sr * R->Sl * (R->UL[q] - R->UR[q])) / (R->Sr - R->Sl);
       }
@@ -968,10 +978,10 @@ static void add_flux(Port *p, Rm *R, double dt) {
       prim2cons(p, R->primR, R->UR, R->r, 1.0);
       star_hllc(p, R);
     }
-    for (q = 0; q < 5; ++q) R->F[q] = R->Fstar[q] - w * R->Ustar[q];
+    for (q = 0; q < p->NQ; ++q) R->F[q] = R->Fstar[q] - w * R->Ustar[q];
   }
   if (p->Explicit_Viscosity > 0.0) visc_flux(p, R);
-  for (q = 0; q < 5; ++q) {
+  for (q = 0; q < p->NQ; ++q) {
     p->cons[q][R->cL] += -dt * R->dA * R->F[q];
     p->cons[q][R->cR] += dt * R->dA * R->F[q];
   }
@@ -1002,7 +1012,7 @@ static void phi_fluxes(Port *p, double dt) {
       R.cm = p->tiph[R.cL];
       R.r_cell_L = r;
       R.r_cell_R = r;
-      for (q = 0; q < 5; ++q) {
+      for (q = 0; q < p->NQ; ++q) {
         R.primL[q] = p->prim[q][R.cL] + 0.5 * p->gradp[q][R.cL] * p->dphi[R.cL];
         R.primR[q] = p->prim[q][R.cR] - 0.5 * p->gradp[q][R.cR] * p->dphi[R.cR];
       }
@@ -1034,7 +1044,7 @@ static void r_fluxes(Port *p, double dt) {
     R.cm = p->fcm[n];
     R.r_cell_L = R.r - p->fdl[n];
     R.r_cell_R = R.r + p->fdr[n];
-    for (q = 0; q < 5; ++q) {
+    for (q = 0; q < p->NQ; ++q) {
       R.primL[q] = p->prim[q][R.cL] + p->grad[q][R.cL] * p->fdl[n] + p->gradp[q][R.cL] * dpL;
       R.primR[q] = p->prim[q][R.cR] - p->grad[q][R.cR] * p->fdr[n] - p->gradp[q][R.cR] * dpR;
     }
@@ -1242,15 +1252,15 @@ static void outflow_pair(Port *p, int i, int outer) {
   const int dst = outer ? i + 1 : i;
   const double dz = p->zf[1] - p->zf[0];
   for (n = p->nri[i]; n < p->nri[i + 1]; ++n)
-    for (q = 0; q < 5; ++q) p->prim[q][outer ? p->fR[n] : p->fL[n]] = 0.0;
+    for (q = 0; q < p->NQ; ++q) p->prim[q][outer ? p->fR[n] : p->fL[n]] = 0.0;
   for (n = p->nri[i]; n < p->nri[i + 1]; ++n) {
     const int to = outer ? p->fR[n] : p->fL[n], from = outer ? p->fL[n] : p->fR[n];
-    for (q = 0; q < 5; ++q) p->prim[q][to] += p->prim[q][from] * p->fdA[n];
+    for (q = 0; q < p->NQ; ++q) p->prim[q][to] += p->prim[q][from] * p->fdA[n];
   }
   for (j = 0; j < p->N_p[dst]; ++j) {
     const int g = p->off[dst] + j;
     const double dA = dz * FP(p, i) * p->dphi[g];
-    for (q = 0; q < 5; ++q) p->prim[q][g] /= dA;
+    for (q = 0; q < p->NQ; ++q) p->prim[q][g] /= dA;
   }
 }
 
@@ -1267,8 +1277,13 @@ static void boundary_and_damp(Port *p, double dt) {
       double prof[5];
       if (!((p->NoInnerBC != 1 && i < p->ng_min) || i > p->NR - p->ng_max - 1)) continue;
       if (single_init(p, i, prof) != 1) continue;
-      for (j = 0; j < p->N_p[i]; ++j)
-        for (q = 0; q < 5; ++q) p->prim[q][p->off[i] + j] = prof[q];
+      for (j = 0; j < p->N_p[i]; ++j) {
+        int g = p->off[i] + j;
+        for (q = 0; q < 5; ++q) p->prim[q][g] = prof[q];
+        /* cell_single_init_vortex's dye at the cell's current phi */
+        if (p->InitialDataType == VORTEX && p->NQ > 5)
+          p->prim[5][g] = cos(p->tiph[g] - .5 * p->dphi[g]) < 0.0 ? 0.0 : 1.0;
+      }
     }
   }
   /* cell_bc_damp (cell_misc.c:98-132) */
@@ -1304,7 +1319,7 @@ void port_substep(Port *p, double fac, int stop) {
   }
   set_w(p);
   for (g = 0; g < p->N; ++g)
-    for (q = 0; q < 5; ++q) p->cons[q][g] = (1.0 - p->RK) * p->cons[q][g] + p->RK * p->rkcons[q][g];
+    for (q = 0; q < p->NQ; ++q) p->cons[q][g] = (1.0 - p->RK) * p->cons[q][g] + p->RK * p->rkcons[q][g];
   if (stop == 0) return;
   plm_p(p);
   plm_rz(p);
@@ -1333,7 +1348,7 @@ void port_prologue(Port *p) {
   set_w(p);
   set_dt(p);
   for (g = 0; g < p->N; ++g) {
-    for (q = 0; q < 5; ++q) p->rkcons[q][g] = p->cons[q][g];
+    for (q = 0; q < p->NQ; ++q) p->rkcons[q][g] = p->cons[q][g];
     p->rktiph[g] = p->tiph[g];
   }
   for (k = 0; k < 2; ++k) {

@@ -5,11 +5,13 @@
  * and operation order as the reference, so with the same libm and
  * -ffp-contract=off it reproduces the reference bit for bit.
  *
- * Scope: 2-D (NumZ = 1), single process, fixed radial boundaries, NUM_Q = 5,
- * the initial data types VORTEX, SSTEST, GRESHO, KEPLER_RING, CIRCUMBINARY.
+ * Scope: 2-D (NumZ = 1), single process, fixed or outflow radial boundaries,
+ * NUM_C = 5 with up to PORT_MAXQ - 5 passive scalars, every initial-data type.
  */
 #ifndef DISCO_PORT_H
 #define DISCO_PORT_H
+
+#define PORT_MAXQ 8 /* NUM_Q = NUM_C + NUM_N at most */
 
 typedef struct {
   /* parfile keys (src/Sim/sim_readpar.c:55-106) + the initial-data keys */
@@ -37,13 +39,13 @@ typedef struct {
   int IC_Seed;
 
   /* grid */
-  int NR, N, ng_min, ng_max;
+  int NR, N, ng_min, ng_max, NQ;
   int *N_p, *off;        /* cells per annulus, first cell of each annulus */
   double *rf;            /* NR+1 radial faces: rf[i+1] = FacePos(i) */
   double zf[2];          /* the single z layer */
 
   /* cells (structure of arrays, (k,i,j) order) */
-  double *prim[5], *cons[5], *rkcons[5], *grad[5], *gradp[5];
+  double *prim[PORT_MAXQ], *cons[PORT_MAXQ], *rkcons[PORT_MAXQ], *grad[PORT_MAXQ], *gradp[PORT_MAXQ];
   double *tiph, *rktiph, *dphi, *wiph;
 
   /* GravMass */

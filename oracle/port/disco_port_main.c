@@ -28,7 +28,7 @@ static void rd(FILE *f, void *p, size_t sz, size_t n) {
 
 static void dump_state(const char *path, const Port *p, int ext) {
   FILE *f = fopen(path, "wb");
-  int hdr[5] = {p->NR, 1, 5, p->N, ext}, i, n, q;
+  int hdr[5] = {p->NR, 1, p->NQ, p->N, ext}, i, n, q;
   double td[2] = {p->t, p->dt}, g[12];
   if (!f) exit(2);
   wr(f, "DSTATE1", 1, 8);
@@ -41,15 +41,15 @@ static void dump_state(const char *path, const Port *p, int ext) {
   wr(f, g, sizeof(double), 12);
   wr(f, p->N_p, sizeof(int), (size_t)p->NR);
   wr(f, p->rf, sizeof(double), (size_t)p->NR + 1);
-  for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) wr(f, &p->prim[q][n], sizeof(double), 1);
-  for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) wr(f, &p->cons[q][n], sizeof(double), 1);
+  for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) wr(f, &p->prim[q][n], sizeof(double), 1);
+  for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) wr(f, &p->cons[q][n], sizeof(double), 1);
   wr(f, p->tiph, sizeof(double), (size_t)p->N);
   wr(f, p->dphi, sizeof(double), (size_t)p->N);
   if (ext) {
-    for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) wr(f, &p->grad[q][n], sizeof(double), 1);
-    for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) wr(f, &p->gradp[q][n], sizeof(double), 1);
+    for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) wr(f, &p->grad[q][n], sizeof(double), 1);
+    for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) wr(f, &p->gradp[q][n], sizeof(double), 1);
     wr(f, p->wiph, sizeof(double), (size_t)p->N);
-    for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) wr(f, &p->rkcons[q][n], sizeof(double), 1);
+    for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) wr(f, &p->rkcons[q][n], sizeof(double), 1);
     wr(f, p->rktiph, sizeof(double), (size_t)p->N);
   }
   fclose(f);
@@ -63,16 +63,16 @@ static void load_state(const char *path, Port *p) {
   if (!f) exit(2);
   rd(f, magic, 1, 8);
   rd(f, hdr, sizeof(int), 5);
-  if (memcmp(magic, "DSTATE1", 8) != 0 || hdr[0] != p->NR || hdr[2] != 5 || hdr[3] != p->N) {
+  if (memcmp(magic, "DSTATE1", 8) != 0 || hdr[0] != p->NR || hdr[2] != p->NQ || hdr[3] != p->N) {
     fprintf(stderr, "state file %s does not match the parfile grid\n", path);
     exit(2);
   }
   rd(f, skip, sizeof(double), 14);
-  buf = malloc(sizeof(double) * ((size_t)p->NR + 1 + (size_t)p->N * 5));
+  buf = malloc(sizeof(double) * ((size_t)p->NR + 1 + (size_t)p->N * p->NQ));
   rd(f, buf, sizeof(int), (size_t)p->NR);
   rd(f, buf, sizeof(double), (size_t)p->NR + 1);
-  for (n = 0; n < p->N; ++n) for (q = 0; q < 5; ++q) rd(f, &p->prim[q][n], sizeof(double), 1);
-  rd(f, buf, sizeof(double), (size_t)p->N * 5);
+  for (n = 0; n < p->N; ++n) for (q = 0; q < p->NQ; ++q) rd(f, &p->prim[q][n], sizeof(double), 1);
+  rd(f, buf, sizeof(double), (size_t)p->N * p->NQ);
   rd(f, p->tiph, sizeof(double), (size_t)p->N);
   rd(f, p->dphi, sizeof(double), (size_t)p->N);
   free(buf);

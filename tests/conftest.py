@@ -15,7 +15,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ("gresho16", "kepler24", "cbd32", "kepler24out", "cbd32out", "kepler12noin", "kepler1out",
-         "shear12", "sstest32", "vortex16", "torus16", "milos16", "raddom16", "middle16")
+         "shear12", "sstest32", "vortex16", "torus16", "milos16", "raddom16", "middle16",
+         "vortex16dye", "vortex16dyeout")
 
 # Cases whose result moves further than the default bars under last-ulp
 # differences of the transcendentals: (max relative after 1 and 5 steps, L1

@@ -50,6 +50,10 @@ CASES = {
     "milos16": configs.milos_macfadyen(num_r=16),
     "raddom16": configs.rad_dom(num_r=16),
     "middle16": configs.middle(num_r=16),
+    # a passive scalar (NUM_N = 1): the vortex's dye, HLLC with the fixed
+    # boundary that resets it by phi, and HLL with the outflow boundary
+    "vortex16dye": configs.vortex_test(num_r=16, R_Min=0.1, NUM_N=1),
+    "vortex16dyeout": configs.vortex_test(num_r=16, R_Min=0.1, NUM_N=1, BoundTypeR=1, RiemannSolver=1),
 }
 STEPS = (1, 5, 100)
 PHASES = (0, 1, 2, 3, 4, 5, 6, 7)

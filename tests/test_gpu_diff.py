@@ -157,6 +157,7 @@ def test_adjoint_independent_of_checkpoint_spacing(base):
 @pytest.mark.parametrize("par,msg", [
     (configs.gresho(num_r=16), "C_RIGID"),
     (configs.kepler_ring(num_r=16, BoundTypeR=1), "outflow"),
+    (configs.kepler_ring(num_r=16, NUM_N=1), "passive"),
 ])
 def test_differentiation_refuses_unsupported(par, msg):
     s = lib.Sim(par)

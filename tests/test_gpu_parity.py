@@ -3,8 +3,9 @@
 Expected values are the reference's own outputs (tests/golden, made from the
 unmodified reference sources by make_golden.py).  Bars:
   - face list (integer topology + geometry): bit-exact, always;
-  - Gresho vortex, shear layer, isentropic vortex (no transcendental on the
-    device path): bit-exact, all phases and 100 steps;
+  - Gresho vortex, shear layer, isentropic vortex with and without its dye
+    (no transcendental on the device path): bit-exact, all phases and
+    100 steps;
   - the other disks (device pow/sin/cos/exp differ from the host libm in the
     last ulp): L1 relative difference <= 1e-10 after 100 steps in rho, S_r,
     L and E, and max relative <= 1e-12 per substep phase and after 1 and 5
@@ -22,7 +23,7 @@ from disco2_b200 import lib
 pytestmark = pytest.mark.gpu
 
 # no device transcendental reaches these disks' results: bit-exact
-EXACT = {"gresho16", "shear12", "vortex16"}
+EXACT = {"gresho16", "shear12", "vortex16", "vortex16dye", "vortex16dyeout"}
 L1_TOL = 1e-10      # after 100 RK2 steps (rho, S_r, L, tau)
 STAGE_TOL = 1e-12   # one substep phase, per array (max relative)
 STEP_TOL = 1e-12    # 1 and 5 steps

@@ -67,7 +67,8 @@ def test_optional_initial_data_keys_default():
 
 @pytest.mark.parametrize("over,msg", [
     ({"NumZ": 4}, "NumZ"),
-    ({"NUM_N": 1}, "NUM_N"),
+    ({"NUM_N": 4}, "NUM_N"),
+    ({"NUM_N": 1, "DAMP_TIME": 1.0}, "passive scalars in a damping zone"),
     ({"w_numeric_type": 1}, "w_numeric_type"),
     ({"RiemannSolver": 7}, "RiemannSolver"),
     ({"InitialDataType": 0}, "single-cell"),
