@@ -154,7 +154,7 @@ __device__ T block_excl_scan(T v, T *sh, T &total) {
 // cell_plm_p (src/Cell/cell_plm.c:116-161) and, for the first cell of each disk,
 // gravMass_copy at the start of a step (GravMass_misc.c:20-28) and
 // gravMass_clean_pi (GravMass_misc.c:9-17).  Runs concurrently with k_merge.
-template <typename T>
+template <typename T, bool PS = false>
 __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
         pr = ldq<T>(d.prim, tp.prim, q, N, gr);
       stq<T>(d.gradp, tp.gradp, q, N, g, plm_p_slope(pl, pc, pr, dpL, dpR, P.plm));
     }
-    for (int q = 5; q < 5 + P.num_n; ++q)
+    for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q)
       d.gradp[(size_t)q * N + g] = plm_p_slope(ld(d.prim, q, N, gl), ld(d.prim, q, N, g), ld(d.prim, q, N, gr), dpL, dpR, P.plm);
   }
   if (g == P.cell_base) {
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
 // cell_plm_rz (src/Cell/cell_plm.c:31-53) and the wrapped dpL, dpR that
 // cell_plm_rz, riemann_setup_rz (Riemann_setup.c:18-25) and riemann_visc_flux
 // (Riemann_routines.c:220-228) all form the same way.
-template <typename T>
+template <typename T, bool PS = false>
 __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= d.n_slots) return;
@@ -436,14 +436,14 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
     T WR = ldqr<T>(d.prim, tp.prim, q, N, cR) - dpR * ldqr<T>(d.gradp, tp.gradp, q, N, cR);
     stq<T>(d.fS, tp.fS, q, NS, slot, (WR - WL) / den);
   }
-  for (int q = 5; q < 5 + d.par[A.inst].num_n; ++q) {
+  for (int q = 5; q < 5 + (PS ? d.par[A.inst].num_n : 0); ++q) {
     const double WL = ldr(d.prim, q, N, cL) + dpL * ldr(d.gradp, q, N, cL);
     const double WR = ldr(d.prim, q, N, cR) - dpR * ldr(d.gradp, q, N, cR);
     d.fS[(size_t)q * NS + slot] = (WR - WL) / den;
   }
 }
 
-template <typename T, int MB = DGPU_MINB_PLM>
+template <typename T, int MB = DGPU_MINB_PLM, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells, NS = d.n_slots;
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
       }
     });
     // passive scalars: the same face-weighted slope and limiter
-    for (int q = 5; q < 5 + P.num_n; ++q) {
+    for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q) {
       double gs = 0.0;
       for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
         double dA = F.r * F.dphi * F.dperp;
@@ -595,7 +595,7 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
 // phi faces: thread per cell j, face (j, j+1) (riemann_setup_p, Riemann_setup.c:46-80)
-template <typename T, int MB = DGPU_MINB_FLUX>
+template <typename T, int MB = DGPU_MINB_FLUX, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   const double w = d.w_ann[a];
   T F[5];
   double qL[DGPU_MAX_PASSIVE], qR[DGPU_MAX_PASSIVE], Fq[DGPU_MAX_PASSIVE];
-  const int np = P.num_n;
+  const int np = PS ? P.num_n : 0;
   for (int s = 0; s < np; ++s) {
     qL[s] = ld(d.prim, 5 + s, N, cL) + 0.5 * ld(d.gradp, 5 + s, N, cL) * dpL;
     qR[s] = ld(d.prim, 5 + s, N, cR) - 0.5 * ld(d.gradp, 5 + s, N, cR) * dpR;
@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
 }
 
 // r faces: thread per face slot (riemann_setup_rz, Riemann_setup.c:11-44)
-template <typename T, int MB = DGPU_MINB_FLUXR>
+template <typename T, int MB = DGPU_MINB_FLUXR, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
   }
   T F[5];
   double qL[DGPU_MAX_PASSIVE], qR[DGPU_MAX_PASSIVE], Fq[DGPU_MAX_PASSIVE];
-  const int np = P.num_n;
+  const int np = PS ? P.num_n : 0;
   for (int s = 0; s < np; ++s) {
     qL[s] = ld(d.prim, 5 + s, N, cL) + ld(d.grad, 5 + s, N, cL) * deltaL + ld(d.gradp, 5 + s, N, cL) * dpL;
     qR[s] = ld(d.prim, 5 + s, N, cR) - ld(d.grad, 5 + s, N, cR) * deltaR - ld(d.gradp, 5 + s, N, cR) * dpR;
@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
 // so this kernel runs concurrently with k_flux.  Its first n_ann threads also
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
-template <typename T, int MB = DGPU_MINB_SOURCE>
+template <typename T, int MB = DGPU_MINB_SOURCE, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
   __shared__ double sh_md[2][BLK / 32];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -897,7 +897,7 @@ __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int s
 // rec (the adjoint's segment replay, else NULL): the conserved sum before
 // cons2prim and the new width of each cell go to slot 2 * (*rec_idx) +
 // substep - 1 of rec ([slot][6][n_cells]).
-template <typename T, int MB = DGPU_MINB_UPDATE>
+template <typename T, int MB = DGPU_MINB_UPDATE, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
                                                                   int tail, double *rec, const int *rec_idx) {
   __shared__ bool last;
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     const double dt = fac * S.dt;
     T c[5];
     double cp[DGPU_MAX_PASSIVE], pp[DGPU_MAX_PASSIVE];
-    const int np = P.num_n;
+    const int np = PS ? P.num_n : 0;
     if (np > 0) passive_sum(d, A, a, g, substep, stop, np, cp);
     if (!update_sum(d, tp, A, a, g, substep, stop, dt, true, c)) {
 #pragma unroll
@@ -1050,7 +1050,7 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
 }
 
 // cell_calc_cons over all cells (set-up and state upload)
-template <typename T>
+template <typename T, bool PS = false>
 __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = d.n_cells;
@@ -1065,7 +1065,7 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   prim2cons(p, c, r, dV, P.gamma);
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
-  for (int q = 5; q < 5 + P.num_n; ++q) d.cons[(size_t)q * N + g] = ld(d.prim, q, N, g) * val(c[D_DDD]);
+  for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q) d.cons[(size_t)q * N + g] = ld(d.prim, q, N, g) * val(c[D_DDD]);
 }
 
 // One pass of cell_boundary_outflow_r (src/Cell/cell_boundary.c:14-139) over
@@ -1227,20 +1227,25 @@ int dgk_update_blocks(int n_cells) { return (n_cells + BLK - 1) / BLK; }
 int dgk_block_size(void) { return BLK; }
 
 // t == NULL: the forward kernels; otherwise their tangent instances.
+// Contexts with passive scalars take the instances that carry them (PS).
 #define DGK_LAUNCH(kern, grid, smem, stream, ...)                                                  \
   do {                                                                                            \
     static const TanPtrs none_ = {};                                                              \
     if (t) kern<Dual><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, *t, __VA_ARGS__);       \
+    else if (d->n_pass > 0)                                                                       \
+      kern<double, true><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, none_, __VA_ARGS__); \
     else kern<double><<<(grid), BLK, (smem), (cudaStream_t)(stream)>>>(*d, none_, __VA_ARGS__);    \
   } while (0)
 // The same for the kernels the autotuner sizes: the forward instance with
 // d->tune[which] resident blocks per SM (0: the built-in choice).
-#define DGK_LAUNCH_TUNED(kern, which, grid, stream, ...)                                  \
+#define DGK_LAUNCH_TUNED(kern, which, mbdef, grid, stream, ...)                           \
   do {                                                                                   \
     static const TanPtrs none_ = {};                                                     \
     cudaStream_t s_ = (cudaStream_t)(stream);                                            \
     if (t) {                                                                             \
       kern<Dual><<<(grid), BLK, 0, s_>>>(*d, *t, __VA_ARGS__);                            \
+    } else if (d->n_pass > 0) {                                                          \
+      kern<double, mbdef, true><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__);          \
     } else {                                                                             \
       switch (d->tune[which]) {                                                          \
         case 2: kern<double, 2><<<(grid), BLK, 0, s_>>>(*d, none_, __VA_ARGS__); break;   \
@@ -1264,30 +1269,31 @@ int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream) {
   if (d->n_slots <= 0) return 0;
   static const TanPtrs none = {};
   if (t) k_rslope<Dual><<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, *t);
+  else if (d->n_pass > 0) k_rslope<double, true><<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   else k_rslope<double><<<(d->n_slots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   return (int)cudaGetLastError();
 }
 int dgk_plm_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
-  DGK_LAUNCH_TUNED(k_plm_r, DGPU_TUNE_PLM, (d->n_cells + BLK - 1) / BLK, stream, substep);
+  DGK_LAUNCH_TUNED(k_plm_r, DGPU_TUNE_PLM, DGPU_MINB_PLM, (d->n_cells + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
-  DGK_LAUNCH_TUNED(k_flux_phi, DGPU_TUNE_FLUXPHI, (d->n_cells + BLK - 1) / BLK, stream, substep);
+  DGK_LAUNCH_TUNED(k_flux_phi, DGPU_TUNE_FLUXPHI, DGPU_MINB_FLUX, (d->n_cells + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_flux_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   if (d->n_slots <= 0) return 0;
-  DGK_LAUNCH_TUNED(k_flux_r, DGPU_TUNE_FLUXR, (d->n_slots + BLK - 1) / BLK, stream, substep);
+  DGK_LAUNCH_TUNED(k_flux_r, DGPU_TUNE_FLUXR, DGPU_MINB_FLUXR, (d->n_slots + BLK - 1) / BLK, stream, substep);
   return (int)cudaGetLastError();
 }
 int dgk_source(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   int n = d->n_cells > d->n_ann ? d->n_cells : d->n_ann;
-  DGK_LAUNCH_TUNED(k_source, DGPU_TUNE_SOURCE, (n + BLK - 1) / BLK, stream, substep, 1);
+  DGK_LAUNCH_TUNED(k_source, DGPU_TUNE_SOURCE, DGPU_MINB_SOURCE, (n + BLK - 1) / BLK, stream, substep, 1);
   return (int)cudaGetLastError();
 }
 int dgk_update(const DevPtrs *d, const TanPtrs *t, int substep, int stop, void *stream) {
   int tail = stop >= 7 ? 2 : (stop >= 5 ? 1 : 0);
-  DGK_LAUNCH_TUNED(k_update, DGPU_TUNE_UPDATE, dgk_update_blocks(d->n_cells), stream, substep, stop, tail,
+  DGK_LAUNCH_TUNED(k_update, DGPU_TUNE_UPDATE, DGPU_MINB_UPDATE, dgk_update_blocks(d->n_cells), stream, substep, stop, tail,
                    (double *)NULL, (const int *)NULL);
   return (int)cudaGetLastError();
 }
@@ -1305,8 +1311,12 @@ int dgk_ann_consts(const DevPtrs *d, int substep, void *stream) {
 int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
   int tail = stop >= 5 ? 1 : 0;
   static const TanPtrs none = {};
-  k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop, tail,
-                                                                                      nullptr, nullptr);
+  if (d->n_pass > 0)
+    k_update<double, DGPU_MINB_UPDATE, true><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(
+        *d, none, substep, stop, tail, nullptr, nullptr);
+  else
+    k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop,
+                                                                                        tail, nullptr, nullptr);
   return (int)cudaGetLastError();
 }
 int dgk_outflow(const DevPtrs *d, int stop, void *stream) {
@@ -1317,6 +1327,7 @@ int dgk_outflow(const DevPtrs *d, int stop, void *stream) {
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream) {
   static const TanPtrs none = {};
   if (t) k_calc_cons<Dual><<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, *t);
+  else if (d->n_pass > 0) k_calc_cons<double, true><<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   else k_calc_cons<double><<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, none);
   return (int)cudaGetLastError();
 }
