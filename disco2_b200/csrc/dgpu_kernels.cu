@@ -980,7 +980,8 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     }
   }
   if (tail == 0) return;
-  __threadfence();
+  // the last block reads nothing the other blocks write (mdot_part comes from
+  // k_source), so no fence is needed before the count
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(&d.counters[1], 1u) == gridDim.x - 1;
   __syncthreads();
