@@ -521,7 +521,8 @@ def main():
                               "achieved_gbs": value / world * STEP_ALG_BYTES / 1e9,
                               "frac": value / world * STEP_ALG_BYTES / 1e9 / peak},
             "kernel_ms": per_kernel,
-            "gpu_launches": 2 * len(KERNELS) * args.steps,
+            # the eight kernels of each substep, and k_dt after the CFL minimum
+            "gpu_launches": (2 * len(KERNELS) + 1) * args.steps,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": ke, "how": "dgpu_set_state from pinned host prim/tiph/dphi, "
                                         "dgpu_step_rk2(1), dgpu_get_state to pinned host, per step"},

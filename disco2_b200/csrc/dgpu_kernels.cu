@@ -572,23 +572,19 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
   } else if (inst >= 0 && key != ~0ull) {
     atomicMin(&d.ist[inst].dtkey, key);
   }
+}
 
-  // last block: dt = min, clipped to Time_Max (timestep_set_dt, timestep_set.c:16-21)
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&d.counters[0], 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
+// dt of each disk once k_plm_r has formed the CFL minimum: the minimum,
+// clipped to Time_Max (timestep_set_dt, timestep_set.c:16-21).  A kernel of
+// its own, so that no block of k_plm_r has to wait for its stores to land
+// before a last block is elected.
+__global__ void k_dt(DevPtrs d) {
   for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
     InstState &S = d.ist[k];
-    unsigned long long kk = atomicOr(&S.dtkey, 0ull);
-    double dt = __longlong_as_double((long long)kk);
+    double dt = __longlong_as_double((long long)S.dtkey);
     if (S.t + dt > d.par[k].t_max) dt = d.par[k].t_max - S.t;
     S.dt = dt;
   }
-  if (threadIdx.x == 0) d.counters[0] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1276,6 +1272,7 @@ int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream) {
 }
 int dgk_plm_r(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
   DGK_LAUNCH_TUNED(k_plm_r, DGPU_TUNE_PLM, DGPU_MINB_PLM, (d->n_cells + BLK - 1) / BLK, stream, substep);
+  if (substep == 1) k_dt<<<1, BLK, 0, (cudaStream_t)stream>>>(*d);
   return (int)cudaGetLastError();
 }
 int dgk_flux_phi(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) {
