@@ -380,14 +380,16 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     return fail(NULL, DGPU_ERR_NOMEM, "device allocation failed");
   }
   {
-    /* k_face stages the phi edges and widths of its annulus pair in shared memory */
+    /* k_merge stages the phi edges and widths of its annulus pair, and
+     * builds the pair's runs, in shared memory */
     int a, mx = 0;
     for (a = 0; a < c->n_ann; ++a) {
       const Annulus *A = &c->h_ann[a];
-      int m = A->np + (A->face_cap > 0 ? c->h_ann[a + 1].np : 0);
+      int m = 2 * (int)sizeof(double) * (A->np + (A->face_cap > 0 ? c->h_ann[a + 1].np : 0)) +
+              (int)sizeof(int) * A->run_cap;
       if (m > mx) mx = m;
     }
-    c->d.smem_face = (int)(2 * sizeof(double) * (size_t)mx) <= 48 * 1024 ? (int)(2 * sizeof(double) * (size_t)mx) : 0;
+    c->d.smem_face = mx <= 48 * 1024 ? mx : 0;
   }
   c->d.n_inst = n;
   c->d.n_ann = c->n_ann;

@@ -61,6 +61,7 @@ struct FaceCtx {
   int *fL, *fR;
   double *fdphi, *fcm;
   int *runs;
+  int *sruns;   // copy of runs the rr pass reads (shared memory when staged)
   int *fstart;  // fstart of the inner annulus cells (indexed by j)
   int cap, rcap;
   int *err;
@@ -83,7 +84,7 @@ __device__ void face_cell(const FaceCtx &c, int j, int &jp, int &n, int &s) {
         c.fdphi[n] = dphi;
         c.fcm[n] = tp - .5 * dphi;
       }
-      if (mark && s < c.rcap) c.runs[s] = n;
+      if (mark && s < c.rcap) c.runs[s] = c.sruns[s] = n;
     }
     mark = false;
     ++n;
@@ -205,11 +206,13 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
 // build_jloop (src/Face/face_create_destroy.c:22-193) as a checked parallel
 // merge, and cell_set_w (src/Cell/cell_set_w.c:12-102) of annulus i.
 __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int substep) {
-  __shared__ int sh_i[BLK];
+  __shared__ int sh_i[BLK / 32];
   __shared__ int sh_j[BLK];
-  __shared__ double sh_v[BLK];
-  __shared__ int sh_flag;
-  extern __shared__ double sm[];  // staged phi edges and widths of the pair
+  __shared__ double sh_v[BLK / 32];
+  __shared__ unsigned long long sh_u[BLK / 32];
+  __shared__ int sh_flag, sh_nf, sh_T;
+  // staged phi edges and widths of the pair, then the runs
+  extern __shared__ double sm[];
   const int a = blockIdx.x;
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -222,7 +225,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
   if (A.i < P.NR - 1) {
     const int npo = d.ann[a + 1].np;
     const int offo = d.ann[a + 1].cell_off;
-    const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo);
+    const int rcap = A.run_cap;
+    const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo) + (int)sizeof(int) * rcap;
     const double *tin = traw + off, *din = d.dphi + off;
     const double *tout = traw + offo, *dout = d.dphi + offo;
     if (staged) {
@@ -253,18 +257,19 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
     c.fdphi = d.fdphi + A.face_base;
     c.fcm = d.fcm + A.face_base;
     c.runs = d.runs + A.run_base;
+    c.sruns = staged ? reinterpret_cast<int *>(sm + 2 * (np + npo)) : c.runs;
     c.fstart = d.fstart + off;
     c.cap = A.face_cap;
-    c.rcap = A.run_cap;
+    c.rcap = rcap;
     c.err = d.err;
     c.offL = off;
     c.offR = offo;
     const double p0 = c.tin[np - 1];
 
     // jpmin: first outer cell with the smallest wrap(tiph - p0), start (PHIMAX, 0)
+    double bv = PHIMAX;
+    int bi = 0;
     {
-      double bv = PHIMAX;
-      int bi = 0;
       for (int jp = tid; jp < c.Nout; jp += nt) {
         double dp = wrap_pos(c.tout[jp] - p0, d.err);
         if (dp < bv || (dp == bv && jp < bi)) {
@@ -272,23 +277,35 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
           bi = jp;
         }
       }
-      sh_v[tid] = bv;
-      sh_i[tid] = bi;
-      __syncthreads();
-      for (int o = nt / 2; o > 0; o >>= 1) {
-        if (tid < o) {
-          double v2 = sh_v[tid + o];
-          int i2 = sh_i[tid + o];
-          if (v2 < sh_v[tid] || (v2 == sh_v[tid] && i2 < sh_i[tid])) {
-            sh_v[tid] = v2;
-            sh_i[tid] = i2;
-          }
+      // the (value, index) minimum is the same in any order of combination:
+      // per warp by shuffles, then over the warps
+      const unsigned full = 0xffffffffu;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_down_sync(full, bv, o);
+        int i2 = __shfl_down_sync(full, bi, o);
+        if (v2 < bv || (v2 == bv && i2 < bi)) {
+          bv = v2;
+          bi = i2;
         }
-        __syncthreads();
+      }
+      if ((tid & 31) == 0) {
+        sh_v[tid >> 5] = bv;
+        sh_i[tid >> 5] = bi;
+      }
+      __syncthreads();
+      bv = sh_v[0];
+      bi = sh_i[0];
+      for (int w = 1; w < (nt >> 5); ++w) {
+        const double v2 = sh_v[w];
+        const int i2 = sh_i[w];
+        if (v2 < bv || (v2 == bv && i2 < bi)) {
+          bv = v2;
+          bi = i2;
+        }
       }
     }
-    const int jpmin = sh_i[0];
-    __syncthreads();
+    const int jpmin = bi;
 
     // contiguous chunk of inner cells per thread; speculative start outer cell
     const int chunk = (np + nt - 1) / nt;
@@ -325,26 +342,34 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
     const bool sequential = sh_flag != 0;
 
     if (!sequential) {
-      int ntot, stot;
-      int fo = block_excl_scan<int>(cnt, sh_i, ntot);
-      int so = block_excl_scan<int>(steps, sh_j, stot);
+      // one scan of (faces, advances) packed in a 64-bit word: the advances
+      // of a pair stay far below 2^32, so no carry reaches the face count
+      unsigned long long tot;
+      const unsigned long long pre =
+          block_excl_scan<unsigned long long>(((unsigned long long)cnt << 32) | (unsigned)steps, sh_u, tot);
+      const int fo = (int)(pre >> 32), so = (int)(pre & 0xffffffffu);
+      const int ntot = (int)(tot >> 32), stot = (int)(tot & 0xffffffffu);
       if (ntot > c.cap || stot + 2 > c.rcap) {
         if (tid == 0) {
           set_err(d.err, DGPU_EF_FACE_OVERFLOW);
           d.pair_nf[a] = 0;
           d.pair_T[a] = 0;
+          sh_nf = 0;
+          sh_T = 0;
         }
       } else {
         int n = fo, s = so;
         jp = jp_start;
         for (int j = j0; j < j1; ++j) face_cell<true>(c, j, jp, n, s);
         if (tid == 0) {
-          c.runs[0] = 0;
-          c.runs[stot + 1] = ntot;
+          c.runs[0] = c.sruns[0] = 0;
+          c.runs[stot + 1] = c.sruns[stot + 1] = ntot;
           d.pair_nf[a] = ntot;
           d.pair_jpmin[a] = jpmin;
           d.pair_T[a] = stot;
           d.pair_seq[a] = 0;
+          sh_nf = ntot;
+          sh_T = stot;
         }
       }
     } else if (tid == 0) {
@@ -356,27 +381,31 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
         set_err(d.err, DGPU_EF_FACE_OVERFLOW);
         d.pair_nf[a] = 0;
         d.pair_T[a] = 0;
+        sh_nf = 0;
+        sh_T = 0;
       } else {
-        c.runs[0] = 0;
-        c.runs[s + 1] = n;
+        c.runs[0] = c.sruns[0] = 0;
+        c.runs[s + 1] = c.sruns[s + 1] = n;
         d.pair_nf[a] = n;
         d.pair_jpmin[a] = jpmin;
         d.pair_T[a] = s;
         d.pair_seq[a] = 1;
+        sh_nf = n;
+        sh_T = s;
       }
     }
     __syncthreads();
     // per outer cell, the face ranges of its runs s = jp - jpmin (mod Nout) and
     // s + Nout (the cell at the wrap point); z = INT_MIN flags a third run
     {
-      const int nf = d.pair_nf[a], T = d.pair_T[a];
+      const int nf = sh_nf, T = sh_T;
       for (int jq = tid; jq < npo; jq += nt) {
         int4 rr = make_int4(0, 0, 0, 0);
         if (nf > 0) {
           int s0 = jq - jpmin;
           if (s0 < 0) s0 += npo;
-          if (s0 <= T) rr.x = c.runs[s0], rr.y = c.runs[s0 + 1];
-          if (s0 + npo <= T) rr.z = c.runs[s0 + npo], rr.w = c.runs[s0 + npo + 1];
+          if (s0 <= T) rr.x = c.sruns[s0], rr.y = c.sruns[s0 + 1];
+          if (s0 + npo <= T) rr.z = c.sruns[s0 + npo], rr.w = c.sruns[s0 + npo + 1];
           if (s0 + 2 * npo <= T) rr.z = INT_MIN;
         }
         reinterpret_cast<int4 *>(d.rr)[offo + jq] = rr;
@@ -1459,7 +1488,7 @@ __device__ FaceCtx noalloc_ctx(const NoallocScratch *S, int i, const double *tip
   c.Nout = S->np[i + 1];
   c.fL = c.fR = nullptr;
   c.fdphi = c.fcm = nullptr;
-  c.runs = c.fstart = nullptr;
+  c.runs = c.sruns = c.fstart = nullptr;
   c.cap = c.rcap = 0;
   c.err = err;
   c.offL = c.offR = 0;
