@@ -60,3 +60,35 @@ def test_full_size_steps_match_the_oracle(name, impl):
         d = float(np.abs(got[k] - getattr(want, k)).max())
         assert (d == 0.0) if exact else (d <= max(tol, 1e-12) * 2 * np.pi), (k, d)
     assert abs(t - want.t) <= (0.0 if exact else max(tol, 1e-12) * abs(want.t))
+
+
+def test_wide_annuli_merge_from_global_memory(impl):
+    """Annuli of about 1,500 cells: the pair's phi edges and runs no longer
+    fit the merge's 48 KB of shared memory, so it reads them from global
+    memory. The face lists of the initial state and of the state three steps
+    later, and that state, must be the reference's bit for bit (a Gresho
+    vortex, no device transcendental). The reference dumps the face list of
+    the state it starts from, so the later list comes from loading the later
+    state into it."""
+    p = configs.gresho(num_r=8, R_Min=0.3, R_Max=0.31)
+    sim = lib.Sim(p)
+    N_p, _ = sim.grid()
+    need = max(16 * (int(N_p[i]) + int(N_p[i + 1])) + 4 * (int(N_p[i + 1]) + 8) for i in range(len(N_p) - 1))
+    assert need > 48 * 1024
+    with tempfile.TemporaryDirectory() as td:
+        par = configs.write_parfile(p, os.path.join(td, "wide.par"))
+        _, f0, _ = oracle.run(par, 0, impl=impl, faces=True)
+        want, _, _ = oracle.run(par, STEPS, impl=impl)
+        _, f3, _ = oracle.run(par, 0, impl=impl, load=want, faces=True)
+    ctx = lib.Context(sim)
+    ctx.init_state(0)
+    got0 = ctx.face_list(0)
+    ctx.step(STEPS)
+    got = ctx.get_state(0)
+    got3 = ctx.face_list(0)
+    ctx.close()
+    for f, wf in ((got0, f0), (got3, f3)):
+        for k in ("nri", "L", "R", "r", "dphi", "dA", "deltaL", "deltaR", "cm"):
+            assert np.array_equal(f[k], getattr(wf, k)), k
+    for k in ("prim", "cons", "tiph", "dphi"):
+        assert np.array_equal(got[k], getattr(want, k)), k
