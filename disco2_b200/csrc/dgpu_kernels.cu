@@ -31,7 +31,7 @@
 // (measured on B200, circumbinary disk: these kernels are latency-bound, so
 // occupancy beats the extra spills)
 #ifndef DGPU_MINB_FACE
-#define DGPU_MINB_FACE 4
+#define DGPU_MINB_FACE 6
 #endif
 #ifndef DGPU_MINB_PLM
 #define DGPU_MINB_PLM 4
