@@ -941,6 +941,9 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     pf_planes(d.src, 6, N, g);
     pf(d.tiphw + g);
     pf((substep == 1 ? d.tiph0 : d.tiph1) + g);
+    // and its r-face run ranges and first face, which k_merge just wrote
+    pf(d.rr + 4 * (size_t)g);
+    pf(d.fstart + g);
     const int a = d.cell_ann[g];
     const Annulus &A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
