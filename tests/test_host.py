@@ -5,8 +5,13 @@ The grid and the initial state must equal the reference's bit for bit
 and the initial data, src/main.c:74-119); the fixtures hold the reference's
 own values.
 """
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
+import torch
 
 from conftest import CASES, golden
 from disco2_b200 import configs, lib
@@ -91,3 +96,25 @@ def test_sweep_generator_is_deterministic():
     assert all(128 <= d["NumR"] <= 512 for d in a)
     cells = sum(lib.Sim(d).num_cells for d in a)
     assert 3e6 < cells < 2e7
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    # a fresh process, so no library is cached yet
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from disco2_b200 import lib\n"
+            "try:\n"
+            "    lib.load(%r)\n"
+            "except ImportError as e:\n"
+            "    print('refused:', e)\n" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                          str(tmp_path / "libdisco_gpu.so")))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "refused:" in r.stdout and "missing" in r.stdout
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="needs a host without a CUDA device")
+def test_no_device_is_an_error_not_a_host_fallback():
+    # a supported disk: creation reaches the device and fails there
+    sim = lib.Sim(configs.gresho(num_r=16))
+    with pytest.raises(lib.DiscoError, match="CUDA"):
+        lib.Context(sim)
