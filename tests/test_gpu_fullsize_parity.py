@@ -92,3 +92,33 @@ def test_wide_annuli_merge_from_global_memory(impl):
             assert np.array_equal(f[k], getattr(wf, k)), k
     for k in ("prim", "cons", "tiph", "dphi"):
         assert np.array_equal(got[k], getattr(want, k)), k
+
+
+def test_sweep_disks_in_one_context_match_the_oracle(impl):
+    """The two smallest disks of the 48-disk circumbinary sweep (unequal-mass
+    binaries, q = 0.62 and 0.017, with their own alpha, h/r, N_r and outer
+    radius), advanced together in one context, against the reference run on
+    each disk alone: three RK2 steps, max relative 1e-12 per array."""
+    sweep = configs.circumbinary_sweep(48, seed=3)
+    sims_all = [lib.Sim(p) for p in sweep]
+    pick = sorted(range(len(sweep)), key=lambda k: sims_all[k].num_cells)[:2]
+    assert all(sweep[k]["MassRatio"] < 0.99 for k in pick)
+    sims = [sims_all[k] for k in pick]
+    ctx = lib.Context(sims)
+    for i in range(len(sims)):
+        ctx.init_state(i)
+    ctx.step(STEPS)
+    tol = 1e-12
+    with tempfile.TemporaryDirectory() as td:
+        for i, k in enumerate(pick):
+            par = configs.write_parfile(sweep[k], os.path.join(td, f"sweep{k}.par"))
+            want, _, _ = oracle.run(par, STEPS, impl=impl)
+            got = ctx.get_state(i)
+            t, _ = ctx.time(i)
+            for key in ("prim", "cons"):
+                assert max_rel(got[key], getattr(want, key)) <= tol, (k, key, max_rel(got[key], getattr(want, key)))
+            for key in ("tiph", "dphi"):
+                d = float(np.abs(got[key] - getattr(want, key)).max())
+                assert d <= tol * 2 * np.pi, (k, key, d)
+            assert abs(t - want.t) <= tol * abs(want.t), (k, t, want.t)
+    ctx.close()
