@@ -3,8 +3,8 @@ reference build where it was compiled, else the C restatement) on the same
 full-size disks, three RK2 steps from the same initial state.
 
 Bars as in test_gpu_parity.py: bit-exact where no device transcendental
-reaches the result (Gresho vortex, shear layer), max relative 1e-12 per
-array otherwise; the Shakura-Sunyaev test problem carries last-ulp
+reaches the result (Gresho vortex, shear layer, isentropic vortex), max
+relative 1e-12 per array otherwise; the Shakura-Sunyaev test problem carries last-ulp
 differences further (its bar is CASE_TOL's).
 """
 import os
@@ -27,6 +27,12 @@ DISKS = {
     "circumbinary_400": (configs.circumbinary(), False, 1e-12),
     "shear_128": (configs.shear_test(), True, 0.0),
     "sstest_128": (configs.sstest(), False, CASE_TOL["sstest32"][0]),
+    # the reference's other initial-data families at their parfiles' sizes
+    "vortex_67": (configs.vortex_test(), True, 0.0),
+    "torus_83": (configs.torus_2d(), False, 1e-12),
+    "milos_131": (configs.milos_macfadyen(), False, 1e-12),
+    "raddom_131": (configs.rad_dom(), False, 1e-12),
+    "middle_131": (configs.middle(), False, 1e-12),
 }
 
 
