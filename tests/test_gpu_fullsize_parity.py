@@ -29,6 +29,9 @@ DISKS = {
     "sstest_128": (configs.sstest(), False, CASE_TOL["sstest32"][0]),
     # the reference's other initial-data families at their parfiles' sizes
     "vortex_67": (configs.vortex_test(), True, 0.0),
+    # its passive scalar (the dye), with the fixed and the outflow boundary
+    "vortex_67_dye": (configs.vortex_test(NUM_N=1), True, 0.0),
+    "vortex_67_dye_outflow": (configs.vortex_test(NUM_N=1, BoundTypeR=1, RiemannSolver=1), True, 0.0),
     "torus_83": (configs.torus_2d(), False, 1e-12),
     "milos_131": (configs.milos_macfadyen(), False, 1e-12),
     "raddom_131": (configs.rad_dom(), False, 1e-12),
