@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import CASE_TOL, max_rel
+from conftest import CASE_TOL, l1_rel, max_rel
 from disco2_b200 import configs, lib
 
 pytestmark = pytest.mark.gpu
@@ -131,3 +131,24 @@ def test_sweep_disks_in_one_context_match_the_oracle(impl):
                 assert d <= tol * 2 * np.pi, (k, key, d)
             assert abs(t - want.t) <= tol * abs(want.t), (k, t, want.t)
     ctx.close()
+
+
+def test_circumbinary_full_size_100_steps_l1(impl):
+    """The headline correctness bar on the headline disk: the 258,078-cell
+    circumbinary disk after 100 RK2 steps, against the reference run on the
+    host from the same initial state. rho (D), momenta (S_r, L) and energy
+    (tau) agree to L1-relative 1e-10; t to 1e-12 relative."""
+    p = configs.circumbinary()
+    with tempfile.TemporaryDirectory() as td:
+        par = configs.write_parfile(p, os.path.join(td, "cbd400.par"))
+        want, _, _ = oracle.run(par, 100, impl=impl)
+    sim = lib.Sim(p)
+    ctx = lib.Context(sim)
+    ctx.init_state(0)
+    ctx.step(100)
+    got = ctx.get_state(0)
+    t, _ = ctx.time(0)
+    ctx.close()
+    for q in (0, 2, 3, 1):
+        assert l1_rel(got["cons"][:, q], want.cons[:, q]) <= 1e-10, (q, l1_rel(got["cons"][:, q], want.cons[:, q]))
+    assert abs(t - want.t) <= 1e-12 * abs(want.t)
