@@ -1,21 +1,32 @@
 // sm_100a kernels of the moving-mesh finite-volume step.
 //
-// One RK substep is four launches:
-//   k_face    per annulus : cell_clean_pi, cell_plm_p, cell_set_w, GravMass
-//                           copy/clean_pi, and the r-face list of the annulus
-//                           pair (i, i+1) (build_jloop) as a checked parallel
-//                           merge of the two sorted phi-edge lists
-//   k_plm_r   per cell    : cell_plm_rz (face-weighted slope + limiter) and,
-//                           in substep 1, the CFL minimum (cell_mindt)
-//   k_flux    per face    : riemann_setup_p/_rz + riemann_AddFlux (HLL/HLLC in
-//                           the moving frame + viscous flux), stored as the
-//                           per-face increment dt*dA*F
-//   k_update  per cell    : gathers the face increments in the reference's
-//                           accumulation order, then cell_add_src,
-//                           cell_add_visc_src, cell_add_split_fictitious,
-//                           cell_update_phi/_dphi, cell_calc_prim, the fixed
-//                           radial boundary, cell_bc_damp and cell_calc_cons;
-//                           its last block advances the GravMass state.
+// One RK substep is eight launches in a CUDA graph:
+//   k_merge    per annulus pair : the r-face list of pair (i, i+1) (face_create
+//                                 / build_jloop) as a checked parallel merge of
+//                                 the two sorted phi-edge lists, and
+//                                 cell_set_w
+//   k_cellprep per cell         : cell_clean_pi, cell_plm_p, GravMass copy /
+//                                 clean_pi
+//   k_rslope   per r face       : the face slope S and the wrapped offsets of
+//                                 cell_plm_rz / riemann_setup_rz
+//   k_plm_r    per cell         : cell_plm_rz (face-weighted slope + limiter)
+//                                 and, in substep 1, the CFL minimum
+//                                 (cell_mindt); k_dt then forms dt
+//                                 (timestep_set_dt)
+//   k_source   per cell         : the increments of cell_add_src and
+//                                 cell_add_visc_src; per-annulus constants
+//   k_flux_phi per phi face     : riemann_setup_p + riemann_AddFlux
+//   k_flux_r   per r face       : riemann_setup_rz + riemann_AddFlux; both
+//                                 flux kernels store dt*dA*F per face
+//   k_update   per cell         : gathers the increments in the reference's
+//                                 accumulation order, cell_add_split_fictitious,
+//                                 cell_update_phi/_dphi, cell_calc_prim, the
+//                                 fixed radial boundary, cell_bc_damp and
+//                                 cell_calc_cons; its last block advances the
+//                                 GravMass state
+// and, for disks with the outflow radial boundary, k_outflow per disk
+// (cell_boundary_outflow_r).  k_merge runs beside k_cellprep on a second
+// stream, and k_source then k_flux_phi beside k_flux_r.
 //
 // Built with -fmad=false: every expression keeps the reference's operation
 // order and rounding (double '/' and sqrt are IEEE-rounded on the GPU), so
