@@ -865,7 +865,7 @@ int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, dou
   if (rc) return rc;
   s = c->sims[inst];
   p = &c->h_par[inst];
-  /* build the list of the current state: one k_face pass (substep-1 buffers) */
+  /* build the list of the current state: one k_merge pass (substep-1 buffers) */
   CKK(dgk_merge(&c->d, 1, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
   nf = (int *)malloc(sizeof(int) * (size_t)s->NR);

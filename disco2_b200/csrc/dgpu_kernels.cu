@@ -785,7 +785,7 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
 // the reference's order: src[0..4] = S_r (pressure/centrifugal), S_r (gravity
 // + frame), L, S_z, tau; src[5] = viscous heating; src[6+p] = sink mass of mass
 // p.  They read only the substep's primitives, slopes and GravMass positions,
-// so this kernel runs concurrently with k_flux.  Its first n_ann threads also
+// so this kernel runs concurrently with k_flux_r.  Its first n_ann threads also
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
 template <typename T, int MB = DGPU_MINB_SOURCE, bool PS = false>
@@ -1425,7 +1425,7 @@ __global__ void k_noalloc_setup(NoallocScratch *S, int NR) {
   S->fill_ok = 0;
 }
 
-// Chunk start, count and verification of one pair; the same decisions as k_face.
+// Chunk start, count and verification of one pair; the same decisions as k_merge.
 struct PairPlan {
   int jpmin, jp_start, j0, j1, cnt, sequential;
 };
