@@ -43,6 +43,7 @@ class DiskRun(torch.autograd.Function):
         ctx.close()
         fctx.save_for_backward(prim0)
         fctx.args = (params, qv, av, nsteps, window_start)
+        fctx.devs = (getattr(q, "device", torch.device("cpu")), getattr(alpha, "device", torch.device("cpu")))
         return torch.as_tensor(J, dtype=torch.float64)
 
     @staticmethod
@@ -53,6 +54,8 @@ class DiskRun(torch.autograd.Function):
         g = ctx.adjoint(nsteps, window_start, ckpt_every=CKPT_EVERY,
                         weights=gJ.detach().cpu().numpy().astype(np.float64))
         ctx.close()
+        dev_q, dev_a = fctx.devs
         return (torch.as_tensor(g["dprim"], dtype=torch.float64).to(prim0.device),
-                torch.tensor(g["dq"], dtype=torch.float64), torch.tensor(g["dalpha"], dtype=torch.float64),
+                torch.tensor(g["dq"], dtype=torch.float64, device=dev_q),
+                torch.tensor(g["dalpha"], dtype=torch.float64, device=dev_a),
                 None, None, None)

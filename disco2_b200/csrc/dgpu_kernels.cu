@@ -1641,9 +1641,10 @@ __global__ void __launch_bounds__(BLK) k_noalloc_fill(NoallocScratch *S, const d
 
 }  // namespace
 
-// Device address of the scratch array, looked up once per device (on the first
-// call made with that device current).
-static void *g_noalloc_ptr[64];
+// The device address of the scratch array is looked up on every call, in the
+// calling thread's current context, so it stays valid after a device reset or
+// from another context on the same device.  Every pointer argument must be
+// memory of that current device.
 
 extern "C" __attribute__((visibility("default"))) int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double *dphi, int cap,
                                       int *nri, int *L, int *R, double *fdphi, double *fdA, double *fcm,
@@ -1655,13 +1656,10 @@ extern "C" __attribute__((visibility("default"))) int dgpu_face_list_noalloc(con
   const int NR = sim->NR;
   if (NR > NOALLOC_MAXA || NR < 3) return DGPU_ERR_ARG;  // more annuli than the static scratch holds
   if (sim->NumZ != 1) return DGPU_ERR_UNSUPPORTED;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DGPU_ERR_CUDA;
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DGPU_ERR_CUDA;
-    g_noalloc_ptr[dev] = p;
-  }
-  NoallocScratch *S = (NoallocScratch *)g_noalloc_ptr[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return DGPU_ERR_CUDA;
+  void *sp = nullptr;
+  if (cudaGetSymbolAddress(&sp, g_noalloc_scratch) != cudaSuccess || !sp) return DGPU_ERR_CUDA;
+  NoallocScratch *S = (NoallocScratch *)sp;
   const double dperp = dsim_zface(sim, 0) - dsim_zface(sim, -1);
   if (cudaMemcpyAsync(S->np, sim->N_p, sizeof(int) * (size_t)NR, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(S->rface, sim->r_faces, sizeof(double) * (size_t)(NR + 1), cudaMemcpyHostToDevice, st) !=

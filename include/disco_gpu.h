@@ -161,11 +161,11 @@ int dgpu_face_list(dgpu_ctx *ctx, int inst, int cap, int *nri, int *L, int *R, d
  * the library keeps until the process exits, sized for at most
  * DGPU_NOALLOC_MAX_ANNULI annuli (any number of cells); larger grids return
  * DGPU_ERR_ARG, as does a face count above cap (*nf then holds the count).
- * The first call on a device looks up that array's device address (with the
- * caller's current device), so make the first call before any stream capture.
- * Every call reuses the same array, so calls that overlap on the GPU (other
- * streams or threads) race; serialise them.  Synchronous: returns after the
- * list is complete. */
+ * Every call looks up that array's device address in the calling thread's
+ * current device and context; every pointer argument must be memory of that
+ * device.  Every call reuses the same array, so calls that overlap on the GPU
+ * (other streams or threads) race; serialise them.  Synchronous: returns after
+ * the list is complete. */
 #define DGPU_NOALLOC_MAX_ANNULI 4096
 #define DGPU_NOALLOC_SCRATCH_BYTES (128 * 1024)
 int dgpu_face_list_noalloc(const dgpu_sim *sim, const double *tiph, const double *dphi, int cap,

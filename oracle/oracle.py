@@ -22,7 +22,8 @@ PORT_LIB = os.path.join(HERE, "_build", "libdisco_port.so")
 # the restatement built with every libm result in the step moved by one ulp
 # (the sensitivity of a case to last-ulp differences; tests only)
 PORT_ULP_BIN = os.path.join(HERE, "_build", "disco_port_ulp")
-REFSRC = "/root/reference/src"
+# the reference tree where it is mounted (override with DISCO_REFSRC)
+REFSRC = os.environ.get("DISCO_REFSRC", "/root/reference/src")
 
 
 def build(ref: bool | None = None, port: bool = True) -> None:

@@ -55,6 +55,7 @@ def test_noalloc_face_list_matches_context_entry_point_twice(make, steps):
            "dA": torch.empty(cap, dtype=torch.float64, device=dev),
            "cm": torch.empty(cap, dtype=torch.float64, device=dev)}
     torch.cuda.synchronize()
+    free_after = []
     for call in range(2):
         for k, v in out.items():
             v.fill_(-7 if v.dtype == torch.int32 else float("nan"))
@@ -62,11 +63,14 @@ def test_noalloc_face_list_matches_context_entry_point_twice(make, steps):
         nf = C.c_int(-1)
         rc = _call(L, sim, tiph, dphi, cap, out, nf)
         assert rc == 0, (call, rc)
+        # device memory in use does not grow from one call to the next
+        free_after.append(torch.cuda.mem_get_info(0)[0])
         assert nf.value == nf_want
         got = {k: v.cpu().numpy() for k, v in out.items()}
         assert np.array_equal(got["nri"], want["nri"]), call
         for k in ("L", "R", "dphi", "dA", "cm"):
             assert np.array_equal(got[k][:nf_want], want[k]), (call, k)
+    assert free_after[1] == free_after[0], free_after
 
 
 def test_noalloc_rejects_sizes_beyond_its_limits():
