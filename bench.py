@@ -34,21 +34,17 @@ UNIT = "zone-updates/s"
 PEAKS_FILE = os.path.join(HERE, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
-# Compulsory DRAM bytes per unit for each kernel as designed (each array
-# element touched once): per cell and per r-face of one substep.
-KERNELS = ["cellprep", "merge", "rslope", "plm_r", "source", "flux_phi", "flux_r", "update"]
-ALG_BYTES = {
-    # name: (bytes per cell, bytes per r-face)
-    "cellprep": (8 + 8 + 40 + 8 + 40, 0),
-    "merge": (8 + 8 + 4 + 4, 24),
-    "rslope": (40 + 40 + 8 + 8, 24 + 40 + 16),
-    "plm_r": (8 + 4 + 40, 24 + 40),
-    "source": (40 + 8 + 8 + 16 + 64, 0),
-    "flux_phi": (40 + 40 + 40 + 8 + 8 + 64, 0),
-    "flux_r": (0, 8 + 16 + 16 + 64 + 2 * (40 + 40 + 40 + 8)),
-    "update": (40 + 40 + 40 + 8 + 8 + 8 + 8 + 64 + 64 + 8 + 40 + 40 + 8 + 8 + 8, 64),
-}
-STEP_ALG_BYTES = 240  # per zone-update: 5 conserved + 1 phi edge, read/written across 2 stages
+# Algorithmic DRAM bytes per zone-update (one interior cell advanced by one RK2
+# step): 5 conserved values and 1 phi edge, FP64, read and written across the
+# two stages -- stage 1 reads U^n (48 B) and writes U^1 (48 B), stage 2 reads
+# U^1 and U^n and writes U^(n+1) (144 B).  Everything else (prims, slopes,
+# faces, w, dt) is recomputable within the step.
+STEP_ALG_BYTES = 240
+# The kernel that reads and writes the state carries those bytes: per interior
+# cell, (substep 1, substep 2).  No other kernel of the step has a share.
+STATE_SHARE = {"update": (96, 144), "sweep": (96, 144)}
+PROFILE_SUMMARY = {"sweep": "profiles/sweep_circumbinary.md", "prep": "profiles/sweep_circumbinary.md",
+                   "update": "profiles/step_kernels_circumbinary.md"}
 
 
 def workload_params(name: str):
@@ -67,22 +63,25 @@ def workload_params(name: str):
 
 
 def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of a kernel from the committed ncu summary (one
-    --set full capture of the same workload), or None."""
+    """DRAM bytes per launch of a kernel (dram__bytes_read.sum +
+    dram__bytes_write.sum) as recorded in the committed ncu summary of the
+    same workload, and that file's name; (None, None) when there is none."""
     import re
-    path = os.path.join(HERE, "profiles", "step_kernels_circumbinary.md")
+    rel = PROFILE_SUMMARY.get(kernel)
+    if rel is None:
+        return None, None
     try:
-        text = open(path).read()
+        text = open(os.path.join(HERE, rel)).read()
     except OSError:
-        return None
+        return None, None
     m = re.search(r"dram_bytes_per_launch:([^`\n]*)", text)
     if not m:
-        return None
+        return None, None
     for tok in m.group(1).split():
         k, _, v = tok.partition("=")
         if k == "k_" + kernel:
-            return float(v)
-    return None
+            return float(v), rel
+    return None, None
 
 
 def load_peaks():
@@ -202,6 +201,23 @@ def interior_cells(sim) -> int:
     return int(N_p[ngmin:len(N_p) - ngmax].sum())
 
 
+def reference_grid(par_text: str):
+    """The state header of a workload from the reference build's own set-up (a
+    0-step run dumps N_p and the cell count), so the reference arm never loads
+    this package's library."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle  # noqa: E402  (reference arm only)
+    exe = oracle.REF_BIN if oracle.have_ref() else oracle.PORT_BIN
+    with tempfile.TemporaryDirectory() as td:
+        par = os.path.join(td, "w.par")
+        with open(par, "w") as f:
+            f.write(par_text)
+        out = os.path.join(td, "o.bin")
+        subprocess.run([exe, "run", par, "0", out], capture_output=True, check=True)
+        st = oracle.read_state(out)
+    return st
+
+
 def run_reference(args, rank, world):
     """The reference build on every host core at once. Without MPI it is
     single-threaded, so each core runs its own copy of the disk; the value is
@@ -211,9 +227,14 @@ def run_reference(args, rank, world):
     from concurrent.futures import ThreadPoolExecutor
     from disco2_b200 import configs
     p, desc = workload_params(args.workload)
-    from disco2_b200 import lib
-    sim = lib.Sim(p)
-    nin = interior_cells(sim)
+    text = configs.parfile_text(p)
+    try:
+        st = reference_grid(text)
+    except Exception as e:  # no oracle binary could be built or run
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build did not run: {e}"}))
+        return
+    ng = int(p["ng"])
+    nin = int(st.N_p[1:st.NR - ng].sum())
     # the reference needs ~2 s per step here: time a bounded sample of the K steps
     steps = max(1, min(args.steps, args.ref_max_steps))
     warm = max(0, min(args.warmup, 3))
@@ -221,7 +242,6 @@ def run_reference(args, rank, world):
         cores = len(os.sched_getaffinity(0))
     except AttributeError:
         cores = os.cpu_count() or 1
-    text = configs.parfile_text(p)
     with ThreadPoolExecutor(max_workers=cores) as ex:
         res = list(ex.map(lambda _: cpu_baseline_run(text, steps, warm), range(cores)))
     if any(r is None for r in res):
@@ -234,8 +254,8 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sum(walls) / len(walls) / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": desc, "cells": sim.num_cells,
-                                        "interior_cells": nin, "annuli": sim.num_annuli,
+        "data": "synthetic", "config": {"workload": desc, "cells": int(st.N),
+                                        "interior_cells": nin, "annuli": int(st.NR),
                                         "parallelism": f"{cores} independent copies, one per host core"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{steps} of the {args.steps} requested RK2 steps of the same "
@@ -370,6 +390,8 @@ def main():
                     help="steps per launch-shape candidate for the autotuner (0: built-in shapes)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=500)
+    ap.add_argument("--eight", action="store_true",
+                    help="time the eight-kernel substep instead of the fused one")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -405,6 +427,8 @@ def main():
     nin = interior_cells(sim)
     stream = torch.cuda.Stream()
     ctx = lib.Context(sim, device=local, stream=stream.cuda_stream)
+    if args.eight:
+        ctx.set_fused(False)
     ctx.init_state(0)
     L = lib.load()
     # launch shapes of the heavy kernels timed on this disk (state restored)
@@ -446,27 +470,29 @@ def main():
     value = nin * args.steps * world / (ms / 1e3)
 
     # per-kernel device times (same steps launched kernel by kernel, L2 flushed between steps)
-    kern = [0.0] * (2 * len(KERNELS))
+    kern = {}
     nprof = max(3, min(args.steps, 50))
     for k in range(nprof):
         with torch.cuda.stream(stream):
             flush.zero_()
         torch.cuda.synchronize()
-        km = ctx.step_timed(1)
-        kern = [a + b for a, b in zip(kern, km)]
-    per_kernel = {}
-    nk = len(KERNELS)
-    for i, nm in enumerate(KERNELS):
-        per_kernel[nm] = (kern[i] + kern[nk + i]) / (2 * nprof)  # ms per launch
+        for nm, (t1, t2) in ctx.step_timed(1).items():
+            a, b = kern.get(nm, (0.0, 0.0))
+            kern[nm] = (a + t1, b + t2)
+    kern = {nm: (a / nprof, b / nprof) for nm, (a, b) in kern.items()}  # ms per launch, substep 1 / 2
+    per_kernel = {nm: (a + b) / 2 for nm, (a, b) in kern.items()}
     dom = max(per_kernel, key=per_kernel.get)
-    # units: cells and r-faces of one substep
     fl = ctx.face_list(0)
     nfaces = int(len(fl["L"]))
     ncell = sim.num_cells
-    bpc, bpf = ALG_BYTES[dom]
-    alg_bytes = bpc * ncell + bpf * nfaces
     peak, peak_kind = load_peaks()
-    achieved = alg_bytes / (per_kernel[dom] * 1e-3) / 1e9
+    # the dominant kernel's share of the algorithmic bytes, over its two launches of a step
+    s1, s2 = STATE_SHARE.get(dom, (0, 0))
+    alg_bytes_step = (s1 + s2) * nin
+    achieved = alg_bytes_step / ((kern[dom][0] + kern[dom][1]) * 1e-3) / 1e9
+    traffic, traffic_src = profiled_traffic(dom) if args.workload == "circumbinary" else (None, None)
+    fused = ctx.fused
+    launches_per_step = 2 * len(ctx.kernels) + (0 if fused else 1)  # + k_dt after the CFL minimum
 
     # end to end through the C ABI: host (pinned) state in, one step, host state out
     n = sim.num_cells
@@ -526,16 +552,21 @@ def main():
                        "blocks_per_sm": tuned},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": profiled_traffic(dom) if args.workload == "circumbinary" else None,
-                         "alg_bytes_per_launch": alg_bytes,
+                         "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes_step / 2,
+                         "alg_bytes": f"{s1} B (substep 1) and {s2} B (substep 2) per interior cell: "
+                                      "the conserved state and phi edge the kernel reads and writes",
                          "ms_per_launch": per_kernel[dom],
-                         "traffic_source": "profiles/step_kernels_circumbinary.md (ncu dram__bytes_read+write, one launch)"},
+                         "traffic_source": (f"copied from {traffic_src} (ncu dram__bytes_read.sum + "
+                                            "dram__bytes_write.sum, one launch of the same workload); "
+                                            "not measured in this run") if traffic_src else None},
             "step_roofline": {"alg_bytes_per_zone_update": STEP_ALG_BYTES,
                               "achieved_gbs": value / world * STEP_ALG_BYTES / 1e9,
                               "frac": value / world * STEP_ALG_BYTES / 1e9 / peak},
-            "kernel_ms": per_kernel,
-            # the eight kernels of each substep, and k_dt after the CFL minimum
-            "gpu_launches": (2 * len(KERNELS) + 1) * args.steps,
+            "kernel_ms": {nm: {"substep1": a, "substep2": b} for nm, (a, b) in kern.items()},
+            "step_kernels": "fused: k_prep + k_sweep per substep" if fused else
+                            "eight kernels per substep (+ k_dt)",
+            "gpu_launches": launches_per_step * args.steps,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": ke, "how": "dgpu_set_state from pinned host prim/tiph/dphi, "
                                         "dgpu_step_rk2(1), dgpu_get_state to pinned host, per step"},

@@ -202,7 +202,8 @@ void dgpu_destroy(dgpu_ctx *c) {
                   c->d.rkcons, c->d.grad, c->d.gradp, c->d.tiph0, c->d.tiph1, c->d.tiphw, c->d.rktiph,
                   c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.rr, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
-                  c->d.mdot_part, c->d.counters, c->d.err, c->d.obuf, c->d_stage, c->d_torque};
+                  c->d.mdot_part, c->d.counters, c->d.err, c->d.obuf, c->d_stage, c->d_torque,
+                  c->d.cfl_ann, c->d.sweep_flag};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
       if (ps[k]) cudaFree(ps[k]);
   }
@@ -368,6 +369,8 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.runs = (int *)dmalloc(sizeof(int) * (size_t)(c->n_runs ? c->n_runs : 1), &ok);
     c->d.mdot_part = (double *)dmalloc(sizeof(double) * 2 * (size_t)c->n_upd_blocks, &ok);
     c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
+    c->d.cfl_ann = (unsigned long long *)dmalloc(sizeof(unsigned long long) * A, &ok);
+    c->d.sweep_flag = (int *)dmalloc(sizeof(int) * A, &ok);
     c->d.err = (int *)dmalloc(sizeof(int), &ok);
     if (n_ob > 0) c->d.obuf = (double *)dmalloc(sizeof(double) * NQ * (size_t)n_ob, &ok);
     c->d_stage = (double *)dmalloc(sizeof(double) * NQ * (size_t)maxcells, &ok);
@@ -391,6 +394,12 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     }
     c->d.smem_face = mx <= 48 * 1024 ? mx : 0;
   }
+  /* the fused substep covers the forward step of disks without passive
+   * scalars, outflow radial boundary or sink */
+  c->fused_ok = c->n_pass == 0 && c->n_ob == 0;
+  for (k = 0; k < n; ++k)
+    if (c->h_par[k].rho_sink_on == 1) c->fused_ok = 0;
+  c->fused = c->fused_ok;
   c->d.n_inst = n;
   c->d.n_ann = c->n_ann;
   c->d.n_cells = c->n_cells;
@@ -441,6 +450,8 @@ int dctx_read_err(struct dgpu_ctx *c) {
     return fail(c, DGPU_ERR_NUMERIC, "a phi wrap loop did not terminate (non-finite phi edge; flags 0x%x)", e);
   if (e & DGPU_EF_NONFINITE)
     return fail(c, DGPU_ERR_NUMERIC, "non-finite state: a non-ghost cell's CFL time step is NaN (flags 0x%x)", e);
+  if (e & DGPU_EF_SWEEP_WAIT)
+    return fail(c, DGPU_ERR_CUDA, "a k_sweep block gave up waiting for the previous annulus (flags 0x%x)", e);
   if (e & DGPU_EF_VISC_VZ)
     return fail(c, DGPU_ERR_NUMERIC, "viscosity with nonzero v_z (the reference exits here, Riemann_routines.c:271-274)");
   return DGPU_OK;
@@ -670,6 +681,14 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double
 
 int dctx_launch_step(struct dgpu_ctx *c) {
   int sub;
+  if (c->fused) {
+    /* per substep: k_prep (face list, phi slopes, CFL minima), then k_sweep */
+    for (sub = 1; sub <= 2; ++sub) {
+      CKK(dgk_prep(&c->d, sub, c->stream));
+      CKK(dgk_sweep(&c->d, sub, c->stream));
+    }
+    return DGPU_OK;
+  }
   for (sub = 1; sub <= 2; ++sub) {
     /* k_merge (per annulus pair) alongside k_cellprep (per cell) */
     CK(cudaEventRecord(c->fork[0], c->stream));
@@ -719,12 +738,48 @@ int dgpu_step_rk2(dgpu_ctx *c, int nsteps) {
   return DGPU_OK;
 }
 
+int dgpu_set_fused(dgpu_ctx *c, int fused) {
+  if (!c || fused < 0 || fused > 1) return DGPU_ERR_ARG;
+  if (fused && !c->fused_ok)
+    return fail(c, DGPU_ERR_UNSUPPORTED, "the fused substep needs disks without passive scalars, outflow radial "
+                                         "boundary or sink");
+  if (fused != c->fused && c->have_graph) {
+    cudaSetDevice(c->device);
+    cudaGraphExecDestroy(c->graph);
+    c->have_graph = 0;
+  }
+  c->fused = fused;
+  return DGPU_OK;
+}
+
+int dgpu_fused(const dgpu_ctx *c) { return c ? c->fused : DGPU_ERR_ARG; }
+
 int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
   cudaEvent_t ev[DGPU_STEP_KERNELS + 1];
   int k, s, sub, rc = DGPU_OK;
   if (!c || nsteps < 0 || !kernel_ms) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
   for (k = 0; k <= DGPU_STEP_KERNELS; ++k) CK(cudaEventCreate(&ev[k]));
+  if (c->fused) {
+    /* kernel_ms[0], [1]: k_prep, k_sweep of substep 1; [8], [9]: of substep 2 */
+    for (s = 0; s < nsteps; ++s) {
+      for (sub = 1; sub <= 2; ++sub) {
+        CK(cudaEventRecord(ev[0], c->stream));
+        CKK(dgk_prep(&c->d, sub, c->stream));
+        CK(cudaEventRecord(ev[1], c->stream));
+        CKK(dgk_sweep(&c->d, sub, c->stream));
+        CK(cudaEventRecord(ev[2], c->stream));
+        CK(cudaEventSynchronize(ev[2]));
+        for (k = 0; k < 2; ++k) {
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+          kernel_ms[8 * (sub - 1) + k] += (double)ms;
+        }
+      }
+    }
+    for (k = 0; k <= DGPU_STEP_KERNELS; ++k) cudaEventDestroy(ev[k]);
+    return dctx_read_err(c);
+  }
   for (s = 0; s < nsteps && rc == DGPU_OK; ++s) {
     int e = 0;
     CK(cudaEventRecord(ev[e++], c->stream));
@@ -766,22 +821,23 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
 #define TUNE_NCAND 4
 static const int tune_cand[TUNE_NCAND] = {2, 3, 4, 5};
 /* kernel_ms slot of each tuned kernel in substep 1 (substep 2 is +8) */
-static const int tune_slot[DGPU_TUNE_N] = {3, 5, 6, 4, 7};
+static const int tune_slot[DGPU_TUNE_N] = {3, 5, 6, 4, 7, 1};
 
 int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
   double *buf = NULL, ms[DGPU_STEP_KERNELS];
   InstState *ist = NULL;
   int k, v, rc = DGPU_OK;
-  static const int order[DGPU_TUNE_N] = {DGPU_TUNE_UPDATE, DGPU_TUNE_FLUXR, DGPU_TUNE_FLUXPHI, DGPU_TUNE_SOURCE,
-                                         DGPU_TUNE_PLM};
+  static const int order[DGPU_TUNE_N - 1] = {DGPU_TUNE_UPDATE, DGPU_TUNE_FLUXR, DGPU_TUNE_FLUXPHI, DGPU_TUNE_SOURCE,
+                                             DGPU_TUNE_PLM};
+  static const int order_fused[1] = {DGPU_TUNE_SWEEP};
   if (!c || steps < 0) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
   if (steps == 0) {
     /* apply the given choice */
     if (!choice) return fail(c, DGPU_ERR_ARG, "steps == 0 needs a choice to apply");
     for (k = 0; k < DGPU_TUNE_N; ++k) {
-      if (choice[k] != 0 && (choice[k] < 2 || choice[k] > 5))
-        return fail(c, DGPU_ERR_ARG, "blocks per SM must be 0 or 2..5, got %d", choice[k]);
+      if (choice[k] != 0 && (choice[k] < 2 || choice[k] > (k == DGPU_TUNE_SWEEP ? 4 : 5)))
+        return fail(c, DGPU_ERR_ARG, "blocks per SM must be 0 or 2..5 (sweep 2..4), got %d", choice[k]);
     }
     for (k = 0; k < DGPU_TUNE_N; ++k) c->d.tune[k] = choice[k];
   } else {
@@ -793,11 +849,15 @@ int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
       return fail(c, DGPU_ERR_NOMEM, "autotune: device allocation failed");
     }
     if (dgk_snap(&c->d, buf, ist, 1, c->stream)) rc = fail(c, DGPU_ERR_CUDA, "autotune: state save failed");
-    for (k = 0; k < DGPU_TUNE_N && rc == DGPU_OK; ++k) {
-      const int kk = order[k];
+    /* the fused step tunes k_sweep (2..4 blocks per SM), the other the five
+     * heavy kernels */
+    const int nk = c->fused ? 1 : DGPU_TUNE_N - 1;
+    for (k = 0; k < nk && rc == DGPU_OK; ++k) {
+      const int kk = c->fused ? order_fused[k] : order[k];
+      const int ncand = kk == DGPU_TUNE_SWEEP ? TUNE_NCAND - 1 : TUNE_NCAND;
       double best = 1e300;
       int bestv = c->d.tune[kk];
-      for (v = 0; v < TUNE_NCAND && rc == DGPU_OK; ++v) {
+      for (v = 0; v < ncand && rc == DGPU_OK; ++v) {
         double t;
         c->d.tune[kk] = tune_cand[v];
         if (dgk_snap(&c->d, buf, ist, 0, c->stream)) {

@@ -35,6 +35,8 @@ struct dgpu_ctx {
   double *d_torque;   /* partial sums + result */
   cudaGraphExec_t graph;
   int have_graph;
+  int fused_ok;       /* every disk can take the fused substep (k_prep + k_sweep) */
+  int fused;          /* the step uses it */
   struct dgpu_diff *diff;
   double *d_diag;     /* diagnostics buffers (allocated on first use) */
   size_t diag_cap;    /* their size in doubles */

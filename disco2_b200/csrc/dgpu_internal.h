@@ -38,6 +38,7 @@ enum { DR_HLLC, DR_HLL };
 #define DGPU_EF_VISC_VZ 4
 #define DGPU_EF_RUN_OVERFLOW 8
 #define DGPU_EF_NONFINITE 16   /* a non-ghost cell's CFL step is not a number (its state holds a NaN) */
+#define DGPU_EF_SWEEP_WAIT 32  /* a k_sweep block gave up waiting for the block of the previous annulus */
 
 /* annulus kind bits */
 #define DGPU_AK_CFL 1        /* non-ghost: enters the CFL minimum (cell_mindt.c:38-42) */
@@ -121,7 +122,8 @@ typedef struct {
 #define DGPU_TUNE_FLUXR 2
 #define DGPU_TUNE_SOURCE 3
 #define DGPU_TUNE_UPDATE 4
-#define DGPU_TUNE_N 5
+#define DGPU_TUNE_SWEEP 5
+#define DGPU_TUNE_N 6
 
 /* Device pointers and sizes handed to every kernel. */
 typedef struct {
@@ -160,6 +162,9 @@ typedef struct {
                              grad and gradp hold 5 + n_pass planes, fS 5 + n_pass, fphi and frf
                              8 + n_pass (the passive increments after the viscous ones) */
   int tune[DGPU_TUNE_N];  /* host-side launch choice of the tuned kernels: resident blocks per SM (0: built-in) */
+  /* the fused substep (k_prep, k_sweep) */
+  unsigned long long *cfl_ann; /* [n_ann] CFL minimum of each annulus (bit pattern; ~0: none) */
+  int *sweep_flag;             /* [n_ann] last k_sweep phase done for each annulus */
 } DevPtrs;
 
 /* Forward-mode tangent: d/de of the state and of the substep intermediates
@@ -222,6 +227,11 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
 /* the outflow radial boundary, its damping and cell_calc_cons on the annuli
  * it rewrites (one block per disk); after k_update, for stop >= 6 */
 int dgk_outflow(const DevPtrs *d, int stop, void *stream);
+/* the fused substep: k_prep (face list, phi slopes, CFL minima) then k_sweep
+ * (the wavefront over the annuli); forward, no passive scalar, no outflow
+ * boundary, no sink */
+int dgk_prep(const DevPtrs *d, int substep, void *stream);
+int dgk_sweep(const DevPtrs *d, int substep, void *stream);
 /* k_update recording the conserved sum and new widths into rec (adjoint replay) */
 int dgk_update_rec(const DevPtrs *d, int substep, double *rec, const int *rec_idx, void *stream);
 /* the per-annulus constants of k_source only (ann_c) */

@@ -59,6 +59,12 @@
 #ifndef DGPU_MINB_UPDATE
 #define DGPU_MINB_UPDATE 4
 #endif
+#ifndef DGPU_MINB_PREP
+#define DGPU_MINB_PREP 4
+#endif
+#ifndef DGPU_MINB_SWEEP
+#define DGPU_MINB_SWEEP 3
+#endif
 
 namespace {
 
@@ -162,15 +168,11 @@ __device__ T block_excl_scan(T v, T *sh, T &total) {
   return pre + x - v;
 }
 
-// Per cell, once per substep: cell_clean_pi (src/Cell/cell_misc.c:12-26),
-// cell_plm_p (src/Cell/cell_plm.c:116-161) and, for the first cell of each disk,
-// gravMass_copy at the start of a step (GravMass_misc.c:20-28) and
-// gravMass_clean_pi (GravMass_misc.c:9-17).  Runs concurrently with k_merge.
-template <typename T, bool PS = false>
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, TanPtrs tp, int substep) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+// Per cell, once per substep: cell_clean_pi of the phi edge
+// (src/Cell/cell_misc.c:12-26) and cell_plm_p (src/Cell/cell_plm.c:116-161).
+template <typename T, bool PS>
+__device__ __forceinline__ void cellprep_cell(const DevPtrs &d, const TanPtrs &tp, int g, int substep) {
   const int N = d.n_cells;
-  if (g >= N) return;
   const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
   pf_planes(d.prim, 5, N, g);
   pf(d.dphi + g);
@@ -180,21 +182,31 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
   const DiskParams &P = d.par[A.inst];
   const int np = A.np, off = A.cell_off, j = g - off;
   d.tiphw[g] = wrap_pos(traw[g], d.err);
-  {
-    const int gl = off + (j == 0 ? np - 1 : j - 1);
-    const int gr = off + (j == np - 1 ? 0 : j + 1);
-    const double dc = d.dphi[g];
-    const double dpL = .5 * (dc + d.dphi[gl]);
-    const double dpR = .5 * (dc + d.dphi[gr]);
+  const int gl = off + (j == 0 ? np - 1 : j - 1);
+  const int gr = off + (j == np - 1 ? 0 : j + 1);
+  const double dc = d.dphi[g];
+  const double dpL = .5 * (dc + d.dphi[gl]);
+  const double dpR = .5 * (dc + d.dphi[gr]);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      T pc = ldq<T>(d.prim, tp.prim, q, N, g), pl = ldq<T>(d.prim, tp.prim, q, N, gl),
-        pr = ldq<T>(d.prim, tp.prim, q, N, gr);
-      stq<T>(d.gradp, tp.gradp, q, N, g, plm_p_slope(pl, pc, pr, dpL, dpR, P.plm));
-    }
-    for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q)
-      d.gradp[(size_t)q * N + g] = plm_p_slope(ld(d.prim, q, N, gl), ld(d.prim, q, N, g), ld(d.prim, q, N, gr), dpL, dpR, P.plm);
+  for (int q = 0; q < 5; ++q) {
+    T pc = ldq<T>(d.prim, tp.prim, q, N, g), pl = ldq<T>(d.prim, tp.prim, q, N, gl),
+      pr = ldq<T>(d.prim, tp.prim, q, N, gr);
+    stq<T>(d.gradp, tp.gradp, q, N, g, plm_p_slope(pl, pc, pr, dpL, dpR, P.plm));
   }
+  for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q)
+    d.gradp[(size_t)q * N + g] = plm_p_slope(ld(d.prim, q, N, gl), ld(d.prim, q, N, g), ld(d.prim, q, N, gr), dpL, dpR, P.plm);
+}
+
+// cellprep_cell for every cell and, for the first cell of each disk,
+// gravMass_copy at the start of a step (GravMass_misc.c:20-28) and
+// gravMass_clean_pi (GravMass_misc.c:9-17).  Runs concurrently with k_merge.
+template <typename T, bool PS = false>
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, TanPtrs tp, int substep) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.n_cells) return;
+  cellprep_cell<T, PS>(d, tp, g, substep);
+  const Annulus &A = d.ann[d.cell_ann[g]];
+  const DiskParams &P = d.par[A.inst];
   if (g == P.cell_base) {
     InstState &S = d.ist[A.inst];
     if (substep == 1) {
@@ -213,10 +225,10 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
   }
 }
 
-// Per annulus pair (i, i+1) of a disk: the r-face list of face_create/
-// build_jloop (src/Face/face_create_destroy.c:22-193) as a checked parallel
-// merge, and cell_set_w (src/Cell/cell_set_w.c:12-102) of annulus i.
-__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int substep) {
+// Per annulus pair (i, i+1) of a disk, one block: the r-face list of
+// face_create/build_jloop (src/Face/face_create_destroy.c:22-193) as a checked
+// parallel merge, and cell_set_w (src/Cell/cell_set_w.c:12-102) of annulus i.
+__device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep) {
   __shared__ int sh_i[BLK / 32];
   __shared__ int sh_j[BLK];
   __shared__ double sh_v[BLK / 32];
@@ -224,7 +236,6 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
   __shared__ int sh_flag, sh_nf, sh_T;
   // staged phi edges and widths of the pair, then the runs
   extern __shared__ double sm[];
-  const int a = blockIdx.x;
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
   const double *traw = substep == 1 ? d.tiph0 : d.tiph1;
@@ -439,6 +450,10 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
   }
 }
 
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int substep) {
+  merge_pair(d, blockIdx.x, substep);
+}
+
 // ---------------------------------------------------------------------------
 // cell_plm_rz (src/Cell/cell_plm.c:13-114) per cell + CFL (cell_mindt.c:32-100)
 // ---------------------------------------------------------------------------
@@ -446,10 +461,8 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int su
 // cell_plm_rz (src/Cell/cell_plm.c:31-53) and the wrapped dpL, dpR that
 // cell_plm_rz, riemann_setup_rz (Riemann_setup.c:18-25) and riemann_visc_flux
 // (Riemann_routines.c:220-228) all form the same way.
-template <typename T, bool PS = false>
-__global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
-  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= d.n_slots) return;
+template <typename T, bool PS>
+__device__ __forceinline__ void rslope_face(const DevPtrs &d, const TanPtrs &tp, int slot) {
   const int cL = rd(d.fL + slot);
   if (cL < 0) return;  // slot past the face list of its pair
   const int cR = rd(d.fR + slot);
@@ -483,10 +496,125 @@ __global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
   }
 }
 
+template <typename T, bool PS = false>
+__global__ void __launch_bounds__(BLK) k_rslope(DevPtrs d, TanPtrs tp) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= d.n_slots) return;
+  rslope_face<T, PS>(d, tp, slot);
+}
+
+// cell_plm_rz's r slope of cell g (src/Cell/cell_plm.c:56-114): the
+// face-area-weighted mean of the face slopes S, then the theta limiter against
+// each face's S in face order.
+template <typename T, bool PS>
+__device__ __forceinline__ void plm_r_grad(const DevPtrs &d, const TanPtrs &tp, int g) {
+  const int N = d.n_cells, NS = d.n_slots;
+  pf(d.rr + 4 * (size_t)g);
+  pf(d.fstart + g);
+  pf(d.dphi + g);
+  const int a = d.cell_ann[g];
+  const Annulus A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  T gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+    double dA = F.r * F.dphi * F.dperp;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gq[q] += ldq<T>(d.fS, tp.fS, q, NS, slot) * dA;
+  });
+  double dAtot;
+  {
+    double dz = P.dz, dp = d.dphi[g];
+    if (A.i == 0) dAtot = dz * A.rp * dp;
+    else if (A.i == P.NR - 1) dAtot = dz * A.rm * dp;
+    else dAtot = dz * (A.rp + A.rm) * dp;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gq[q] /= dAtot;
+  }
+  for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      T Sq = ldq<T>(d.fS, tp.fS, q, NS, slot);
+      if (Sq * gq[q] < 0.0) gq[q] = 0.0;
+      else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
+    }
+  });
+  // passive scalars: the same face-weighted slope and limiter
+  for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q) {
+    double gs = 0.0;
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+      double dA = F.r * F.dphi * F.dperp;
+      gs += ld(d.fS, q, NS, slot) * dA;
+    });
+    gs /= dAtot;
+    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
+      const double Sq = ld(d.fS, q, NS, slot);
+      if (Sq * gs < 0.0) gs = 0.0;
+      else if (fabs(P.plm * Sq) < fabs(gs)) gs = P.plm * Sq;
+    });
+    d.grad[(size_t)q * N + g] = gs;
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) stq<T>(d.grad, tp.grad, q, N, g, gq[q]);
+}
+
+// The CFL step of non-ghost cell g (cell_mindt, src/Cell/cell_mindt.c:10-100)
+// as the bit pattern of the positive double (~0: no candidate, also for a NaN,
+// which is reported).  rkx/rky/rkM: the step-start GravMass positions and
+// masses (the viscous limit's nu); wa = wiph of the annulus.
+__device__ __forceinline__ unsigned long long cfl_key(const DevPtrs &d, const Annulus &A, const DiskParams &P,
+                                                      int g, double wa, const double *rkx, const double *rky,
+                                                      const double *rkM) {
+  const int N = d.n_cells;
+  const double *traw = d.tiph0;
+  double w = .5 * (wa + wa);
+  double dr = A.rp - A.rm;
+  double r = .5 * (A.rp + A.rm);
+  double dx = dr;
+  double rdphi = .5 * (A.rp + A.rm) * d.dphi[g];
+  if (rdphi < dr) dx = rdphi;
+  if (dx > P.dz) dx = P.dz;
+  double Pp = ld(d.prim, D_PPP, N, g), rho = ld(d.prim, D_RHO, N, g);
+  double vp = ld(d.prim, D_UPP, N, g) * r - w;
+  double vr = ld(d.prim, D_URR, N, g), vz = ld(d.prim, D_UZZ, N, g);
+  double cs = sqrt(P.gamma * Pp / rho);
+  double cf2 = cs * cs;
+  double maxv = sqrt(cf2) + sqrt(vr * vr + vp * vp + vz * vz);
+  double dt = P.cfl * dx / maxv;
+  if (P.has_visc) {
+    double nu;
+    if (P.visc_const == 1) {
+      nu = P.visc;
+    } else {
+      double tc = traw[g] - 0.5 * d.dphi[g];
+      if (P.init_type == DI_SHEAR) {
+        nu = P.visc * P.gamma * Pp / rho * dpow(fabs(r * cos(tc)), 2.0);
+        if (r * cos(tc) > 20.) nu = 0.000000001;
+      } else {
+        double sc, cc;
+        sincos(tc, &sc, &cc);
+        const double x = r * cc, y = r * sc;
+        double d0 = gm_dist_xy(x, y, rkx[0], rky[0]);
+        double d1 = gm_dist_xy(x, y, rkx[1], rky[1]);
+        double eps = P.g_eps;
+        nu = P.visc * Pp / rho /
+             sqrt(dpow(d0 * d0 + eps * eps, -1.5) * rkM[0] + dpow(d1 * d1 + eps * eps, -1.5) * rkM[1]);
+      }
+    }
+    double dt_visc = .25 * dx * dx / nu;
+    dt = dt / (1. + dt / dt_visc);
+  }
+  unsigned long long key = (unsigned long long)__double_as_longlong(dt);
+  if (__longlong_as_double((long long)key) < 0.0 || dt != dt) key = ~0ull;
+  // the reference's minimum skips such a cell too (cell_mindt.c); here it
+  // is also reported
+  if (dt != dt) set_err(d.err, DGPU_EF_NONFINITE);
+  return key;
+}
+
 template <typename T, int MB = DGPU_MINB_PLM, bool PS = false>
 __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int substep) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int N = d.n_cells, NS = d.n_slots;
+  const int N = d.n_cells;
   unsigned long long key = ~0ull;
   int inst = -1;
   if (g < d.n_inst) {
@@ -500,100 +628,14 @@ __global__ void __launch_bounds__(BLK, MB) k_plm_r(DevPtrs d, TanPtrs tp, int su
     }
   }
   if (g < N) {
-    pf(d.rr + 4 * (size_t)g);
-    pf(d.fstart + g);
-    pf(d.dphi + g);
+    plm_r_grad<T, PS>(d, tp, g);
     const int a = d.cell_ann[g];
-    const Annulus A = d.ann[a];
-    const DiskParams &P = d.par[A.inst];
+    const Annulus &A = d.ann[a];
     inst = A.inst;
-    T gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
-      double dA = F.r * F.dphi * F.dperp;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) gq[q] += ldq<T>(d.fS, tp.fS, q, NS, slot) * dA;
-    });
-    double dAtot;
-    {
-      double dz = P.dz, dp = d.dphi[g];
-      if (A.i == 0) dAtot = dz * A.rp * dp;
-      else if (A.i == P.NR - 1) dAtot = dz * A.rm * dp;
-      else dAtot = dz * (A.rp + A.rm) * dp;
-#pragma unroll
-      for (int q = 0; q < 5; ++q) gq[q] /= dAtot;
-    }
-    for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        T Sq = ldq<T>(d.fS, tp.fS, q, NS, slot);
-        if (Sq * gq[q] < 0.0) gq[q] = 0.0;
-        else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
-      }
-    });
-    // passive scalars: the same face-weighted slope and limiter
-    for (int q = 5; q < 5 + (PS ? P.num_n : 0); ++q) {
-      double gs = 0.0;
-      for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
-        double dA = F.r * F.dphi * F.dperp;
-        gs += ld(d.fS, q, NS, slot) * dA;
-      });
-      gs /= dAtot;
-      for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int slot, int) {
-        const double Sq = ld(d.fS, q, NS, slot);
-        if (Sq * gs < 0.0) gs = 0.0;
-        else if (fabs(P.plm * Sq) < fabs(gs)) gs = P.plm * Sq;
-      });
-      d.grad[(size_t)q * N + g] = gs;
-    }
-#pragma unroll
-    for (int q = 0; q < 5; ++q) stq<T>(d.grad, tp.grad, q, N, g, gq[q]);
-
     // CFL candidate (cell_mindt), substep 1 only, non-ghost annuli
     if (substep == 1 && (A.kind & DGPU_AK_CFL)) {
       const InstState &S = d.ist[A.inst];
-      const double *traw = d.tiph0;
-      double w = .5 * (d.w_ann[a] + d.w_ann[a]);
-      double dr = A.rp - A.rm;
-      double r = .5 * (A.rp + A.rm);
-      double dx = dr;
-      double rdphi = .5 * (A.rp + A.rm) * d.dphi[g];
-      if (rdphi < dr) dx = rdphi;
-      if (dx > P.dz) dx = P.dz;
-      double Pp = ld(d.prim, D_PPP, N, g), rho = ld(d.prim, D_RHO, N, g);
-      double vp = ld(d.prim, D_UPP, N, g) * r - w;
-      double vr = ld(d.prim, D_URR, N, g), vz = ld(d.prim, D_UZZ, N, g);
-      double cs = sqrt(P.gamma * Pp / rho);
-      double cf2 = cs * cs;
-      double maxv = sqrt(cf2) + sqrt(vr * vr + vp * vp + vz * vz);
-      double dt = P.cfl * dx / maxv;
-      if (P.has_visc) {
-        double nu;
-        if (P.visc_const == 1) {
-          nu = P.visc;
-        } else {
-          double tc = traw[g] - 0.5 * d.dphi[g];
-          if (P.init_type == DI_SHEAR) {
-            nu = P.visc * P.gamma * Pp / rho * dpow(fabs(r * cos(tc)), 2.0);
-            if (r * cos(tc) > 20.) nu = 0.000000001;
-          } else {
-            double sc, cc;
-            sincos(tc, &sc, &cc);
-            const double x = r * cc, y = r * sc;
-            double d0 = gm_dist_xy(x, y, S.rkx[0], S.rky[0]);
-            double d1 = gm_dist_xy(x, y, S.rkx[1], S.rky[1]);
-            double eps = P.g_eps;
-            nu = P.visc * Pp / rho /
-                 sqrt(dpow(d0 * d0 + eps * eps, -1.5) * S.grk_M[0] + dpow(d1 * d1 + eps * eps, -1.5) * S.grk_M[1]);
-          }
-        }
-        double dt_visc = .25 * dx * dx / nu;
-        dt = dt / (1. + dt / dt_visc);
-      }
-      key = (unsigned long long)__double_as_longlong(dt);
-      if (__longlong_as_double((long long)key) < 0.0 || dt != dt) key = ~0ull;
-      // the reference's minimum skips such a cell too (cell_mindt.c); here it
-      // is also reported
-      if (dt != dt) set_err(d.err, DGPU_EF_NONFINITE);
+      key = cfl_key(d, A, d.par[A.inst], g, d.w_ann[a], S.rkx, S.rky, S.grk_M);
     }
   }
   if (substep != 1) return;
@@ -631,13 +673,12 @@ __global__ void k_dt(DevPtrs d) {
 // Face increments: one thread per phi face (at its left cell) and per r-face slot
 // ---------------------------------------------------------------------------
 // phi faces: thread per cell j, face (j, j+1) (riemann_setup_p, Riemann_setup.c:46-80)
-template <typename T, int MB = DGPU_MINB_FLUX, bool PS = false>
-__global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// S: the disk's state with this substep's GravMass positions; dt: the
+// substep's fac * dt.
+template <typename T, bool PS>
+__device__ __forceinline__ void flux_phi_cell(const DevPtrs &d, const TanPtrs &tp, int g, const InstState &S,
+                                              double dt) {
   const int N = d.n_cells;
-  const double fac = substep == 1 ? 1.0 : 0.5;
-  if (t >= N) return;
-  const int g = t;
   // the cell's own planes (its right neighbour's share the lines) ahead of
   // the annulus lookups
   pf_planes(d.prim, 5, N, g);
@@ -648,7 +689,6 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   const int a = d.cell_ann[g];
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
-  const InstState &S = d.ist[A.inst];
   const int j = g - A.cell_off;
   const int cL = g, cR = (j == A.np - 1) ? A.cell_off : g + 1;
   const double dpL = d.dphi[cL], dpR = d.dphi[cR];
@@ -671,7 +711,6 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
     qR[s] = ld(d.prim, 5 + s, N, cR) - 0.5 * ld(d.gradp, 5 + s, N, cR) * dpR;
   }
   riemann_flux(pL, pR, r, 1, w, P.gamma, P.riemann, F, np, qL, qR, Fq);
-  const double dt = fac * S.dt;
   const double k = dt * dA;
 #pragma unroll
   for (int q = 0; q < 5; ++q) stq<T>(d.fphi, tp.fphi, q, N, g, k * F[q]);
@@ -703,21 +742,25 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int
   }
 }
 
+template <typename T, int MB = DGPU_MINB_FLUX, bool PS = false>
+__global__ void __launch_bounds__(BLK, MB) k_flux_phi(DevPtrs d, TanPtrs tp, int substep) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= d.n_cells) return;
+  const InstState &S = d.ist[d.ann[d.cell_ann[g]].inst];
+  flux_phi_cell<T, PS>(d, tp, g, S, (substep == 1 ? 1.0 : 0.5) * S.dt);
+}
+
 // r faces: thread per face slot (riemann_setup_rz, Riemann_setup.c:11-44)
-template <typename T, int MB = DGPU_MINB_FLUXR, bool PS = false>
-__global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+template <typename T, bool PS>
+__device__ __forceinline__ void flux_r_face(const DevPtrs &d, const TanPtrs &tp, int slot, const InstState &S,
+                                            double dt) {
   const int N = d.n_cells;
-  const double fac = substep == 1 ? 1.0 : 0.5;
-  const int slot = t;
-  if (slot >= d.n_slots) return;
   const int cL = d.fL[slot];
   if (cL < 0) return;  // slot past the face list of its pair
   const int cR = d.fR[slot];
   const int a = d.slot_ann[slot];
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
-  const InstState &S = d.ist[A.inst];
   const double fdphi = d.fdphi[slot], cm = d.fcm[slot];
   const double deltaL = A.f_dl, deltaR = A.f_dr;
   const double dpL = d.fdp[slot];
@@ -742,7 +785,6 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
     qR[s] = ld(d.prim, 5 + s, N, cR) - ld(d.grad, 5 + s, N, cR) * deltaR - ld(d.gradp, 5 + s, N, cR) * dpR;
   }
   riemann_flux(pL, pR, r, 0, 0.0, P.gamma, P.riemann, F, np, qL, qR, Fq);
-  const double dt = fac * S.dt;
   const double k = dt * dA;
   const int NS = d.n_slots;
 #pragma unroll
@@ -776,6 +818,15 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
   }
 }
 
+template <typename T, int MB = DGPU_MINB_FLUXR, bool PS = false>
+__global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int substep) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= d.n_slots) return;
+  if (d.fL[slot] < 0) return;  // slot past the face list of its pair
+  const InstState &S = d.ist[d.ann[d.slot_ann[slot]].inst];
+  flux_r_face<T, PS>(d, tp, slot, S, (substep == 1 ? 1.0 : 0.5) * S.dt);
+}
+
 // ---------------------------------------------------------------------------
 // Per-cell update: flux gather + sources + mesh motion + prim/cons + BC + damping
 // ---------------------------------------------------------------------------
@@ -788,42 +839,39 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
 // so this kernel runs concurrently with k_flux_r.  Its first n_ann threads also
 // form the per-annulus constants of the substep (epicyclic rotation of
 // cell_add_split_fictitious.c:26-38, relaxation factor of cell_misc.c:121).
-template <typename T, int MB = DGPU_MINB_SOURCE, bool PS = false>
-__global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
-  __shared__ double sh_md[2][BLK / 32];
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int N = d.n_cells;
-  const double fac = substep == 1 ? 1.0 : 0.5;
-  if (t < d.n_ann) {
-    // per-annulus constants of this substep for k_update: the epicyclic rotation
-    // of cell_add_split_fictitious (cell_add_split_fictitious.c:26-38) and the
-    // relaxation factor of cell_bc_damp (cell_misc.c:121), identical for every
-    // cell of the annulus
-    const Annulus &A = d.ann[t];
-    const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const double dt = fac * S.dt;
-    const double r = 0.5 * (A.rm + A.rp);
-    const double a_sep = S.gr[0] + S.gr[1];
-    const double rom = frame_rom(P, A.rom, r, a_sep);
-    const double Omega = rom / r;
-    const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
-    const double kappa2 = 2. * Omega / r * dr_r2Om;
-    double kappa = 0.0, ck = 1.0, sk = 0.0;
-    if (kappa2 > 0.) {
-      kappa = sqrt(kappa2);
-      ck = cos(kappa * dt);
-      sk = sin(kappa * dt);
-    }
-    const int NA = d.n_ann;
-    d.ann_c[t] = kappa;
-    d.ann_c[NA + t] = ck;
-    d.ann_c[2 * NA + t] = sk;
-    d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
+// Per-annulus constants of the substep for the update of annulus t: the
+// epicyclic rotation of cell_add_split_fictitious
+// (cell_add_split_fictitious.c:26-38) and the relaxation factor of
+// cell_bc_damp (cell_misc.c:121), identical for every cell of the annulus.
+__device__ __forceinline__ void ann_consts(const DevPtrs &d, int t, const InstState &S, double dt) {
+  const Annulus &A = d.ann[t];
+  const DiskParams &P = d.par[A.inst];
+  const double r = 0.5 * (A.rm + A.rp);
+  const double a_sep = S.gr[0] + S.gr[1];
+  const double rom = frame_rom(P, A.rom, r, a_sep);
+  const double Omega = rom / r;
+  const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
+  const double kappa2 = 2. * Omega / r * dr_r2Om;
+  double kappa = 0.0, ck = 1.0, sk = 0.0;
+  if (kappa2 > 0.) {
+    kappa = sqrt(kappa2);
+    ck = cos(kappa * dt);
+    sk = sin(kappa * dt);
   }
-  double md0 = 0.0, md1 = 0.0;
-  if (t < N && cells) {
-    const int g = t;
+  const int NA = d.n_ann;
+  d.ann_c[t] = kappa;
+  d.ann_c[NA + t] = ck;
+  d.ann_c[2 * NA + t] = sk;
+  d.ann_c[3 * NA + t] = (A.kind & DGPU_AK_DAMP) ? (1. - exp(-A.damp_rate * dt)) : 0.0;
+}
+
+// The source increments of cell g (see k_source); the sink masses of the
+// cells counted in Mdot are added to md0 / md1.
+template <typename T, bool PS>
+__device__ __forceinline__ void source_cell_k(const DevPtrs &d, const TanPtrs &tp, int g, const InstState &S,
+                                              double dt, double &md0, double &md1) {
+  const int N = d.n_cells;
+  {
     pf_planes(d.prim, 5, N, g);
     pf(d.grad + (size_t)D_UPP * N + g);
     pf(d.gradp + (size_t)D_URR * N + g);
@@ -832,8 +880,6 @@ __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int s
     const int a = d.cell_ann[g];
     const Annulus &A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const double dt = fac * S.dt;
     const double a_sep = S.gr[0] + S.gr[1];
     const double dphi = d.dphi[g];
     const double rm = A.rm, rp = A.rp;
@@ -907,6 +953,23 @@ __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int s
       }
     }
   }
+}
+
+template <typename T, int MB = DGPU_MINB_SOURCE, bool PS = false>
+__global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int substep, int cells) {
+  __shared__ double sh_md[2][BLK / 32];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  if (t < d.n_ann) {
+    const InstState &S = d.ist[d.ann[t].inst];
+    ann_consts(d, t, S, fac * S.dt);
+  }
+  double md0 = 0.0, md1 = 0.0;
+  if (t < N && cells) {
+    const InstState &S = d.ist[d.ann[d.cell_ann[t]].inst];
+    source_cell_k<T, PS>(d, tp, t, S, fac * S.dt, md0, md1);
+  }
   // deterministic per-block Mdot partial sums (reduced in block order by k_update)
   const unsigned full = 0xffffffffu;
 #pragma unroll
@@ -930,18 +993,19 @@ __global__ void __launch_bounds__(BLK, MB) k_source(DevPtrs d, TanPtrs tp, int s
   }
 }
 
-// rec (the adjoint's segment replay, else NULL): the conserved sum before
-// cons2prim and the new width of each cell go to slot 2 * (*rec_idx) +
-// substep - 1 of rec ([slot][6][n_cells]).
-template <typename T, int MB = DGPU_MINB_UPDATE, bool PS = false>
-__global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
-                                                                  int tail, double *rec, const int *rec_idx) {
-  __shared__ bool last;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+// The update of cell g after its face and source increments are in place:
+// the conserved sum in the reference's order (update_sum),
+// cell_update_phi/_dphi, cell_calc_prim, the fixed radial boundary,
+// cell_bc_damp and cell_calc_cons.  dt: the substep's fac * dt.  XC: the
+// increments were written by other blocks of the running kernel (plain loads,
+// not the read-only path).  rec (the adjoint's segment replay, else NULL): the
+// conserved sum before cons2prim and the new width of each cell go to slot
+// 2 * (*rec_idx) + substep - 1 of rec ([slot][6][n_cells]).
+template <typename T, bool PS, bool XC = false>
+__device__ __forceinline__ void update_cell(const DevPtrs &d, const TanPtrs &tp, int g, int substep, int stop,
+                                            double dt, double *rec, const int *rec_idx) {
   const int N = d.n_cells;
-  const double RK = substep == 1 ? 0.0 : 0.5;
-  const double fac = substep == 1 ? 1.0 : 0.5;
-  if (g < N) {
+  {
     // the cell's own planes, before the annulus lookups they do not depend on
     pf_planes(d.cons, 5, N, g);
     if (substep == 2) {
@@ -958,13 +1022,11 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
     const int a = d.cell_ann[g];
     const Annulus &A = d.ann[a];
     const DiskParams &P = d.par[A.inst];
-    const InstState &S = d.ist[A.inst];
-    const double dt = fac * S.dt;
     T c[5];
     double cp[DGPU_MAX_PASSIVE], pp[DGPU_MAX_PASSIVE];
     const int np = PS ? P.num_n : 0;
     if (np > 0) passive_sum(d, A, a, g, substep, stop, np, cp);
-    if (!update_sum(d, tp, A, a, g, substep, stop, dt, true, c)) {
+    if (!update_sum<T, !XC>(d, tp, A, a, g, substep, stop, dt, true, c)) {
 #pragma unroll
       for (int q = 0; q < 5; ++q) stq<T>(d.cons, tp.cons, q, N, g, c[q]);
       for (int k = 0; k < np; ++k) d.cons[(size_t)(5 + k) * N + g] = cp[k];
@@ -1018,6 +1080,69 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
       }
     }
   }
+}
+
+// GravMass after the substep for disk k: gravMass_update_RK
+// (GravMass_misc.c:66-77), then gravMass_move(t, fac*dt) (GravMass_misc.c:31-64);
+// after substep 2 also t += dt and Macc += Mdot*dt (timestep_algorithm.c:27-39).
+// S.gphi holds the substep's wrapped phases (gravMass_clean_pi) and S.mdot
+// the substep's sink rates.
+__device__ __forceinline__ void gm_tail(const DevPtrs &d, InstState &S, const DiskParams &P, int substep,
+                                        int tail) {
+  const double RK = substep == 1 ? 0.0 : 0.5;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  for (int p = 0; p < 2; ++p) {
+    S.grk_phi[p] = adjust_toward(S.gphi[p], S.grk_phi[p], M_PI, 2. * M_PI, d.err);
+    S.gr[p] = (1.0 - RK) * S.gr[p] + RK * S.grk_r[p];
+    S.gphi[p] = (1.0 - RK) * S.gphi[p] + RK * S.grk_phi[p];
+    S.gM[p] = (1.0 - RK) * S.gM[p] + RK * S.grk_M[p];
+    S.gom[p] = (1.0 - RK) * S.gom[p] + RK * S.grk_om[p];
+  }
+  if (tail >= 2) {
+    double t = S.t, dtm = fac * S.dt;
+    double m0 = S.gM[0], m1 = S.gM[1];
+    double M = m0 + m1;
+    double a_0 = 1.0, tau_0 = P.orb_tscale, T0 = P.orb_t0;
+    double asep, omega;
+    if ((t - T0) / tau_0 < 1.) {
+      asep = a_0 * pow((1.0 - (t - T0) / tau_0), 0.25);
+      omega = pow(asep / M, -1.5);
+    } else {
+      asep = 0.0;
+      omega = 0.0;
+    }
+    double r0, r1;
+    if (M < 1.e-12) {
+      r0 = 0.0;
+      r1 = 0.0;
+    } else {
+      r0 = m1 / M * asep;
+      r1 = m0 / M * asep;
+    }
+    S.gphi[0] += omega * dtm;
+    S.gphi[1] += omega * dtm;
+    S.gr[0] = r0;
+    S.gr[1] = r1;
+    S.gom[0] = omega;
+    S.gom[1] = omega;
+    if (substep == 2) {
+      S.t += S.dt;
+      for (int p = 0; p < 2; ++p) S.macc[p] = S.macc[p] + S.mdot[p] * S.dt;
+    }
+  }
+}
+
+template <typename T, int MB = DGPU_MINB_UPDATE, bool PS = false>
+__global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int substep, int stop,
+                                                                  int tail, double *rec, const int *rec_idx) {
+  __shared__ bool last;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  if (g < N) {
+    const InstState &S = d.ist[d.ann[d.cell_ann[g]].inst];
+    update_cell<T, PS>(d, tp, g, substep, stop, fac * S.dt, rec, rec_idx);
+  }
   if (tail == 0) return;
   // the last block reads nothing the other blocks write (mdot_part comes from
   // k_source), so no fence is needed before the count
@@ -1026,9 +1151,6 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // GravMass after the substep: gravMass_update_RK (GravMass_misc.c:66-77),
-  // then gravMass_move(t, fac*dt) (GravMass_misc.c:31-64); after substep 2
-  // also t += dt and Macc += Mdot*dt (timestep_algorithm.c:27-39).
   for (int k = threadIdx.x; k < d.n_inst; k += blockDim.x) {
     InstState &S = d.ist[k];
     const DiskParams &P = d.par[k];
@@ -1046,47 +1168,232 @@ __global__ void __launch_bounds__(BLK, MB) k_update(DevPtrs d, TanPtrs tp, int s
       S.mdot[0] = s0;
       S.mdot[1] = s1;
     }
-    for (int p = 0; p < 2; ++p) {
-      S.grk_phi[p] = adjust_toward(S.gphi[p], S.grk_phi[p], M_PI, 2. * M_PI, d.err);
-      S.gr[p] = (1.0 - RK) * S.gr[p] + RK * S.grk_r[p];
-      S.gphi[p] = (1.0 - RK) * S.gphi[p] + RK * S.grk_phi[p];
-      S.gM[p] = (1.0 - RK) * S.gM[p] + RK * S.grk_M[p];
-      S.gom[p] = (1.0 - RK) * S.gom[p] + RK * S.grk_om[p];
+    gm_tail(d, S, P, substep, tail);
+  }
+  if (threadIdx.x == 0) d.counters[1] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// The fused substep: k_prep then k_sweep
+// ---------------------------------------------------------------------------
+// k_prep: one block per annulus a of every disk.  The face list of pair
+// (a, a+1) and cell_set_w (merge_pair), cell_clean_pi and cell_plm_p of the
+// annulus's cells and, in substep 1, gravMass_copy and the annulus's CFL
+// minimum (cell_mindt, src/Cell/cell_mindt.c:10-100), from which every block of
+// k_sweep forms the disk's dt (timestep_set_dt).  It also clears the sweep's
+// progress flags and work counters.
+template <int MB>
+__global__ void __launch_bounds__(BLK, MB) k_prep(DevPtrs d, int substep) {
+  __shared__ unsigned long long sh_k[BLK / 32];
+  __shared__ double sh_rk[6];
+  const int a = blockIdx.x;
+  const TanPtrs tp = {};
+  merge_pair(d, a, substep);
+  __syncthreads();  // w_ann[a] (one lane) before the CFL
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  for (int j = threadIdx.x; j < A.np; j += BLK) cellprep_cell<double, false>(d, tp, A.cell_off + j, substep);
+  if (threadIdx.x == 0) {
+    d.sweep_flag[a] = 0;
+    if (a == 0) {
+      d.counters[3] = 0;
+      d.counters[4] = 0;
     }
-    if (tail >= 2) {
-      double t = S.t, dtm = fac * S.dt;
-      double m0 = S.gM[0], m1 = S.gM[1];
-      double M = m0 + m1;
-      double a_0 = 1.0, tau_0 = P.orb_tscale, T0 = P.orb_t0;
-      double asep, omega;
-      if ((t - T0) / tau_0 < 1.) {
-        asep = a_0 * pow((1.0 - (t - T0) / tau_0), 0.25);
-        omega = pow(asep / M, -1.5);
-      } else {
-        asep = 0.0;
-        omega = 0.0;
-      }
-      double r0, r1;
-      if (M < 1.e-12) {
-        r0 = 0.0;
-        r1 = 0.0;
-      } else {
-        r0 = m1 / M * asep;
-        r1 = m0 / M * asep;
-      }
-      S.gphi[0] += omega * dtm;
-      S.gphi[1] += omega * dtm;
-      S.gr[0] = r0;
-      S.gr[1] = r1;
-      S.gom[0] = omega;
-      S.gom[1] = omega;
-      if (substep == 2) {
-        S.t += S.dt;
-        for (int p = 0; p < 2; ++p) S.macc[p] = S.macc[p] + S.mdot[p] * S.dt;
+  }
+  if (substep != 1) return;
+  if (threadIdx.x == 0) {
+    InstState &S = d.ist[A.inst];
+    // gravMass_dist of the step-start positions, for the CFL's viscosity
+    for (int p = 0; p < 2; ++p) {
+      sh_rk[p] = S.gr[p] * cos(S.gphi[p]);
+      sh_rk[2 + p] = S.gr[p] * sin(S.gphi[p]);
+      sh_rk[4 + p] = S.gM[p];
+    }
+    if (A.i == 0) {
+      // gravMass_copy (GravMass_misc.c:20-28); no block of this kernel reads
+      // these copies
+      for (int p = 0; p < 2; ++p) {
+        S.grk_r[p] = S.gr[p];
+        S.grk_phi[p] = S.gphi[p];
+        S.grk_M[p] = S.gM[p];
+        S.grk_om[p] = S.gom[p];
       }
     }
   }
-  if (threadIdx.x == 0) d.counters[1] = 0;
+  __syncthreads();
+  unsigned long long key = ~0ull;
+  if (A.kind & DGPU_AK_CFL) {
+    const double wa = d.w_ann[a];
+    for (int j = threadIdx.x; j < A.np; j += BLK) {
+      const unsigned long long k = cfl_key(d, A, P, A.cell_off + j, wa, sh_rk, sh_rk + 2, sh_rk + 4);
+      key = k < key ? k : key;
+    }
+  }
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long k2 = __shfl_down_sync(full, key, o);
+    key = k2 < key ? k2 : key;
+  }
+  if ((threadIdx.x & 31) == 0) sh_k[threadIdx.x >> 5] = key;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < BLK / 32; ++w) key = sh_k[w] < key ? sh_k[w] : key;
+    d.cfl_ann[a] = key;
+  }
+}
+
+// dt of a disk from k_prep's per-annulus CFL minima: the minimum (1e100 when
+// no cell has a candidate), clipped to Time_Max (timestep_set_dt,
+// src/TimeStep/timestep_set.c:16-21).  The same value as k_plm_r + k_dt form.
+__device__ __forceinline__ double sweep_dt(const DevPtrs &d, const DiskParams &P, double t) {
+  unsigned long long key = (unsigned long long)__double_as_longlong(1.e100);
+  for (int k = P.ann_base; k < P.ann_base + P.NR; ++k) {
+    const unsigned long long v = d.cfl_ann[k];
+    key = v < key ? v : key;
+  }
+  double dt = __longlong_as_double((long long)key);
+  if (t + dt > P.t_max) dt = P.t_max - t;
+  return dt;
+}
+
+// Progress flags of k_sweep: after a __syncthreads, thread 0 publishes that
+// this block's phase v of annulus a is done (its stores ordered before the
+// flag), or waits until the block of annulus a has published v (the block's
+// later loads ordered after the flag).  A wait gives up after
+// DGPU_SWEEP_SPIN_LIMIT polls, reports DGPU_EF_SWEEP_WAIT and returns.
+#define DGPU_SWEEP_SPIN_LIMIT (1 << 18)
+__device__ __forceinline__ void sweep_publish(const DevPtrs &d, int a, int v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(d.sweep_flag + a), "r"(v) : "memory");
+  }
+}
+__device__ __forceinline__ void sweep_wait(const DevPtrs &d, int a, int v) {
+  if (threadIdx.x == 0) {
+    int it = 0, f;
+    for (;;) {
+      asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(f) : "l"(d.sweep_flag + a) : "memory");
+      if (f >= v) break;
+      if (++it > DGPU_SWEEP_SPIN_LIMIT) {
+        set_err(d.err, DGPU_EF_SWEEP_WAIT);
+        break;
+      }
+      __nanosleep(100);
+    }
+  }
+  __syncthreads();
+}
+
+// The update of annulus b's cells (update_cell) once its increments are in
+// place, with the annulus's constants of the substep.
+__device__ __forceinline__ void sweep_update(const DevPtrs &d, const TanPtrs &tp, int b, int substep,
+                                             const InstState &S, double dt) {
+  const Annulus &B = d.ann[b];
+  if (threadIdx.x == 0) ann_consts(d, b, S, dt);
+  __syncthreads();
+  for (int j = threadIdx.x; j < B.np; j += BLK)
+    update_cell<double, false, true>(d, tp, B.cell_off + j, substep, 7, dt, nullptr, nullptr);
+}
+
+// k_sweep: the rest of the substep as one wavefront over the annuli.  Each
+// block takes the next annulus a in order (a work counter, so every earlier
+// annulus is held by a block that is already running) and does, waiting only
+// on the block of annulus a-1 of the same disk:
+//   1. the face slopes S and offsets of the faces of pair (a, a+1) (k_rslope);
+//   2. the r slopes of annulus a (cell_plm_rz) -- needs 1. of a-1;
+//   3. the fluxes of the faces of pair (a-1, a) (riemann_setup_rz +
+//      riemann_AddFlux) -- needs 2. of a-1 -- and the phi faces and source
+//      increments of annulus a;
+//   4. the update of annulus a-1 (and of a itself when it is the disk's last),
+//      whose increments are then all in place -- needs 3. of a-1.
+// A block never waits for a later annulus, so the wavefront always advances.
+// The last block to finish advances the GravMass state (gm_tail).  The
+// increments pass between neighbouring annuli through L2 instead of HBM round
+// trips between eight kernels, and phases of different annuli overlap on the
+// SMs.
+template <int MB>
+__global__ void __launch_bounds__(BLK, MB) k_sweep(DevPtrs d, int substep) {
+  __shared__ int s_a;
+  __shared__ InstState s_S;
+  __shared__ bool s_last;
+  const TanPtrs tp = {};
+  if (threadIdx.x == 0) s_a = (int)atomicAdd(&d.counters[3], 1u);
+  __syncthreads();
+  const int a = s_a;
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  if (threadIdx.x == 0) {
+    // the disk's state with the substep's GravMass positions (gravMass_clean_pi,
+    // then gravMass_dist's r cos(phi), r sin(phi)) and, in substep 1, its dt
+    s_S = d.ist[A.inst];
+    for (int p = 0; p < 2; ++p) {
+      const double ph = wrap_pos(s_S.gphi[p], d.err);
+      s_S.gphi[p] = ph;
+      s_S.gc[p] = cos(ph);
+      s_S.gs[p] = sin(ph);
+      s_S.gx[p] = s_S.gr[p] * s_S.gc[p];
+      s_S.gy[p] = s_S.gr[p] * s_S.gs[p];
+    }
+    if (substep == 1) s_S.dt = sweep_dt(d, P, s_S.t);
+  }
+  __syncthreads();
+  const double dt = (substep == 1 ? 1.0 : 0.5) * s_S.dt;
+  // 1. face slopes of pair (a, a+1)
+  if (A.i < P.NR - 1) {
+    const int nf = d.pair_nf[a];
+    for (int n = threadIdx.x; n < nf; n += BLK) rslope_face<double, false>(d, tp, A.face_base + n);
+  }
+  sweep_publish(d, a, 1);
+  // 2. r slopes of annulus a
+  if (A.i > 0) sweep_wait(d, a - 1, 1);
+  for (int j = threadIdx.x; j < A.np; j += BLK) plm_r_grad<double, false>(d, tp, A.cell_off + j);
+  sweep_publish(d, a, 2);
+  // 3. fluxes of pair (a-1, a); phi faces and sources of annulus a
+  if (A.i > 0) {
+    sweep_wait(d, a - 1, 2);
+    const Annulus &Q = d.ann[a - 1];
+    const int nf = d.pair_nf[a - 1];
+    for (int n = threadIdx.x; n < nf; n += BLK) flux_r_face<double, false>(d, tp, Q.face_base + n, s_S, dt);
+  }
+  {
+    double md0 = 0.0, md1 = 0.0;
+    for (int j = threadIdx.x; j < A.np; j += BLK) {
+      const int g = A.cell_off + j;
+      flux_phi_cell<double, false>(d, tp, g, s_S, dt);
+      source_cell_k<double, false>(d, tp, g, s_S, dt, md0, md1);
+    }
+  }
+  sweep_publish(d, a, 3);
+  // 4. update of annulus a-1, then of the disk's last annulus
+  if (A.i > 0) {
+    sweep_wait(d, a - 1, 3);
+    sweep_update(d, tp, a - 1, substep, s_S, dt);
+  }
+  if (A.i == P.NR - 1) {
+    __syncthreads();
+    sweep_update(d, tp, a, substep, s_S, dt);
+  }
+  // the last block: the GravMass of every disk.  It reads nothing that
+  // another block of this kernel writes.
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&d.counters[4], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  for (int k = threadIdx.x; k < d.n_inst; k += BLK) {
+    InstState &S = d.ist[k];
+    const DiskParams &Pk = d.par[k];
+    if (substep == 1) S.dt = sweep_dt(d, Pk, S.t);
+    for (int p = 0; p < 2; ++p) S.gphi[p] = wrap_pos(S.gphi[p], d.err);
+    S.mdot[0] = 0.0;  // no sink on this path
+    S.mdot[1] = 0.0;
+    gm_tail(d, S, Pk, substep, 2);
+  }
+  if (threadIdx.x == 0) {
+    d.counters[3] = 0;
+    d.counters[4] = 0;
+  }
 }
 
 // cell_calc_cons over all cells (set-up and state upload)
@@ -1358,6 +1665,19 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
   else
     k_update<double><<<dgk_update_blocks(d->n_cells), BLK, 0, (cudaStream_t)stream>>>(*d, none, substep, stop,
                                                                                         tail, nullptr, nullptr);
+  return (int)cudaGetLastError();
+}
+int dgk_prep(const DevPtrs *d, int substep, void *stream) {
+  k_prep<DGPU_MINB_PREP><<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_sweep(const DevPtrs *d, int substep, void *stream) {
+  cudaStream_t s_ = (cudaStream_t)stream;
+  switch (d->tune[DGPU_TUNE_SWEEP]) {
+    case 2: k_sweep<2><<<d->n_ann, BLK, 0, s_>>>(*d, substep); break;
+    case 4: k_sweep<4><<<d->n_ann, BLK, 0, s_>>>(*d, substep); break;
+    default: k_sweep<DGPU_MINB_SWEEP><<<d->n_ann, BLK, 0, s_>>>(*d, substep);
+  }
   return (int)cudaGetLastError();
 }
 int dgk_outflow(const DevPtrs *d, int stop, void *stream) {

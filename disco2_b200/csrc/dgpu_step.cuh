@@ -44,12 +44,22 @@ __device__ __forceinline__ double new_tiph(double tw, double &rk, double RK, dou
   return t;
 }
 
+// A face or source increment: through the read-only path (NC) when an earlier
+// kernel wrote it, by a plain load when another block of the running kernel
+// did.
+template <typename T, bool NC>
+__device__ __forceinline__ T ldinc(const double *v, const double *dv, int q, int n, int g) {
+  if constexpr (NC) return ldqr<T>(v, dv, q, n, g);
+  else return ldq<T>(v, dv, q, n, g);
+}
+
 // The conserved sum of a cell before cons2prim: cell_adjust_RK_cons, the phi
 // and r face increments in the reference's order, cell_add_src, cooling,
 // cell_add_visc_src and cell_add_split_fictitious (the forward stops after
 // `stop` like the stage-parity path; returns false when it stopped early).
-// Writes rkcons in substep 1 when `write_rk`.
-template <typename T>
+// Writes rkcons in substep 1 when `write_rk`.  NC: the increments and the
+// annulus constants come from earlier kernels (see ldinc).
+template <typename T, bool NC = true>
 __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, const Annulus &A, int a, int g,
                                            int substep, int stop, double dt, bool write_rk, T *c) {
   const int N = d.n_cells;
@@ -78,20 +88,20 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     const double r = .5 * (A.rp + A.rm);
     auto addL = [&](int f) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) c[q] -= ldqr<T>(d.fphi, tp.fphi, q, N, f);
+      for (int q = 0; q < 5; ++q) c[q] -= ldinc<T, NC>(d.fphi, tp.fphi, q, N, f);
       if (P.has_visc) {
-        c[D_SRR] -= ldqr<T>(d.fphi, tp.fphi, 5, N, f) / r;
-        c[D_LLL] -= ldqr<T>(d.fphi, tp.fphi, 6, N, f);
-        c[D_TAU] -= ldqr<T>(d.fphi, tp.fphi, 7, N, f);
+        c[D_SRR] -= ldinc<T, NC>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] -= ldinc<T, NC>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] -= ldinc<T, NC>(d.fphi, tp.fphi, 7, N, f);
       }
     };
     auto addR = [&](int f) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) c[q] += ldqr<T>(d.fphi, tp.fphi, q, N, f);
+      for (int q = 0; q < 5; ++q) c[q] += ldinc<T, NC>(d.fphi, tp.fphi, q, N, f);
       if (P.has_visc) {
-        c[D_SRR] += ldqr<T>(d.fphi, tp.fphi, 5, N, f) / r;
-        c[D_LLL] += ldqr<T>(d.fphi, tp.fphi, 6, N, f);
-        c[D_TAU] += ldqr<T>(d.fphi, tp.fphi, 7, N, f);
+        c[D_SRR] += ldinc<T, NC>(d.fphi, tp.fphi, 5, N, f) / r;
+        c[D_LLL] += ldinc<T, NC>(d.fphi, tp.fphi, 6, N, f);
+        c[D_TAU] += ldinc<T, NC>(d.fphi, tp.fphi, 7, N, f);
       }
     };
     if (j == 0) {
@@ -136,8 +146,8 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           if (q < 5 || visc) {
-            u[q] = ldqr<T>(d.frf, tp.frf, q, NS, n);
-            v[q] = ldqr<T>(d.frf, tp.frf, q, NS, n + 1);
+            u[q] = ldinc<T, NC>(d.frf, tp.frf, q, NS, n);
+            v[q] = ldinc<T, NC>(d.frf, tp.frf, q, NS, n + 1);
           }
         }
         apply(u);
@@ -147,7 +157,7 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
         T u[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q)
-          if (q < 5 || visc) u[q] = ldqr<T>(d.frf, tp.frf, q, NS, n);
+          if (q < 5 || visc) u[q] = ldinc<T, NC>(d.frf, tp.frf, q, NS, n);
         apply(u);
       }
     });
@@ -155,13 +165,13 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
   if (stop == 3) return false;
   // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
   // increments come from k_source; added here in the reference's order
-  c[D_SRR] += ldqr<T>(d.src, tp.src, 0, N, g);
-  c[D_SRR] += ldqr<T>(d.src, tp.src, 1, N, g);
-  c[D_LLL] += ldqr<T>(d.src, tp.src, 2, N, g);
-  c[D_SZZ] += ldqr<T>(d.src, tp.src, 3, N, g);
-  c[D_TAU] += ldqr<T>(d.src, tp.src, 4, N, g);
+  c[D_SRR] += ldinc<T, NC>(d.src, tp.src, 0, N, g);
+  c[D_SRR] += ldinc<T, NC>(d.src, tp.src, 1, N, g);
+  c[D_LLL] += ldinc<T, NC>(d.src, tp.src, 2, N, g);
+  c[D_SZZ] += ldinc<T, NC>(d.src, tp.src, 3, N, g);
+  c[D_TAU] += ldinc<T, NC>(d.src, tp.src, 4, N, g);
   if (P.rho_sink_on == 1) {
-    for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldqr<T>(d.src, tp.src, 6 + p, N, g);
+    for (int p = 0; p < P.num_sinks && p < 2; ++p) c[D_DDD] -= ldinc<T, NC>(d.src, tp.src, 6 + p, N, g);
   }
   const double rm = A.rm, rp = A.rp;
   const double r = .5 * (rp + rm);
@@ -182,7 +192,7 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
       c[D_TAU] -= cooling_term;
     }
   }
-  if (P.has_visc) c[D_TAU] += ldqr<T>(d.src, tp.src, 5, N, g);
+  if (P.has_visc) c[D_TAU] += ldinc<T, NC>(d.src, tp.src, 5, N, g);
   // cell_add_split_fictitious (src/Cell/cell_add_split_fictitious.c:11-44)
   {
     const double a_sep = S.gr[0] + S.gr[1];
@@ -190,8 +200,10 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     const double Omega = rom / r;
     const double dr_r2Om = 2. * rom + r * frame_rdrom(P, A.rdrom, r, a_sep);
     const int NA = d.n_ann;
-    const double kappa = rd(d.ann_c + a);  // sqrt(kappa2) when kappa2 > 0, else 0 (k_source)
-    if (kappa > 0.) split_rotate(c, rd(d.ann_c + NA + a), rd(d.ann_c + 2 * NA + a), dr_r2Om, kappa, Omega, r);
+    const double kappa = NC ? rd(d.ann_c + a) : d.ann_c[a];  // sqrt(kappa2) when kappa2 > 0, else 0
+    if (kappa > 0.)
+      split_rotate(c, NC ? rd(d.ann_c + NA + a) : d.ann_c[NA + a], NC ? rd(d.ann_c + 2 * NA + a) : d.ann_c[2 * NA + a],
+                   dr_r2Om, kappa, Omega, r);
   }
   return stop > 4;
 }

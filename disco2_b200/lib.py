@@ -46,6 +46,8 @@ SIGNATURES = {
     "dgpu_step_rk2": (_I, [_P, _I]),
     "dgpu_synchronize": (_I, [_P]),
     "dgpu_step_rk2_timed": (_I, [_P, _I, _dp]),
+    "dgpu_set_fused": (_I, [_P, _I]),
+    "dgpu_fused": (_I, [_P]),
     "dgpu_stage": (_I, [_P, _I]),
     "dgpu_get_stage_data": (_I, [_P, _I, _dp, _dp, _dp, _dp, _dp]),
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
@@ -222,13 +224,26 @@ class Context:
             self.synchronize()
 
     KERNELS = ("cellprep", "merge", "rslope", "plm_r", "source", "flux_phi", "flux_r", "update")
+    FUSED_KERNELS = ("prep", "sweep")
 
-    def step_timed(self, nsteps: int = 1) -> np.ndarray:
-        """Per-kernel device milliseconds summed over nsteps (KERNELS of substep 1,
-        then of substep 2)."""
-        ms = np.zeros(2 * len(self.KERNELS))
+    @property
+    def fused(self) -> bool:
+        """True when a substep is the two fused kernels (k_prep, k_sweep)."""
+        return bool(load().dgpu_fused(self._h))
+
+    def set_fused(self, on: bool):
+        self._ck(load().dgpu_set_fused(self._h, 1 if on else 0))
+
+    @property
+    def kernels(self) -> tuple:
+        return self.FUSED_KERNELS if self.fused else self.KERNELS
+
+    def step_timed(self, nsteps: int = 1) -> dict:
+        """Device milliseconds per launch of each kernel of the step, summed
+        over nsteps: {kernel: (substep 1, substep 2)}."""
+        ms = np.zeros(16)
         self._ck(load().dgpu_step_rk2_timed(self._h, nsteps, _dptr(ms)))
-        return ms
+        return {k: (ms[i], ms[8 + i]) for i, k in enumerate(self.kernels)}
 
     @property
     def handle(self):
@@ -274,13 +289,13 @@ class Context:
                                          _dptr(out["equat"]), _dptr(out["extra"])))
         return out
 
-    TUNED = ("plm_r", "flux_phi", "flux_r", "source", "update")
+    TUNED = ("plm_r", "flux_phi", "flux_r", "source", "update", "sweep")
 
     def autotune(self, steps: int = 3, choice=None) -> dict:
         """Time each launch shape of the heavy kernels on this context's disks
         and keep the fastest (steps == 0: apply `choice`); returns the blocks
         per SM chosen for each tuned kernel."""
-        ch = (C.c_int * 5)(*(choice if choice is not None else [0] * 5))
+        ch = (C.c_int * 6)(*(list(choice) + [0] * (6 - len(choice)) if choice is not None else [0] * 6))
         self._ck(load().dgpu_autotune(self._h, steps, ch))
         return dict(zip(self.TUNED, list(ch)))
 

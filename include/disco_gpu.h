@@ -108,23 +108,41 @@ int dgpu_set_time(dgpu_ctx *ctx, int inst, double t);
  * surface at the next dgpu_synchronize (or any dgpu_get_*). */
 int dgpu_step_rk2(dgpu_ctx *ctx, int nsteps);
 int dgpu_synchronize(dgpu_ctx *ctx);
+/* Which kernels make up a substep (no counterpart in the reference; the
+ * results are bitwise the same either way).  The fused substep is two
+ * launches: k_prep (one block per annulus: the face list, cell_clean_pi,
+ * cell_plm_p and, in substep 1, the CFL minimum) and k_sweep (one wavefront
+ * over the annuli: face slopes, r slopes, the r- and phi-face fluxes, the
+ * sources and the update).  The other form is eight kernels per substep
+ * (cellprep, merge, rslope, plm_r, source, flux_phi, flux_r, update).  A
+ * context uses the fused form when all its disks allow it (no passive scalar,
+ * no outflow radial boundary, no sink); dgpu_set_fused(ctx, 0) selects the
+ * eight kernels, dgpu_set_fused(ctx, 1) the fused form (DGPU_ERR_UNSUPPORTED
+ * where not allowed).  dgpu_fused returns 1 when the step uses the fused
+ * form.  The tangent, adjoint and stage runs always use the eight kernels. */
+int dgpu_set_fused(dgpu_ctx *ctx, int fused);
+int dgpu_fused(const dgpu_ctx *ctx);
 /* The same steps launched one kernel at a time with CUDA events between the
  * kernels on the context's stream (no graph); adds each kernel's device time in
- * milliseconds to kernel_ms[16] (cellprep, merge, rslope, plm_r, source,
- * flux_phi, flux_r, update of substep 1, then of substep 2).  Synchronous.
- * For measurement only: inside the step graph merge runs beside cellprep, and
- * source and flux_phi beside flux_r. */
+ * milliseconds to kernel_ms[16]: for the eight-kernel substep cellprep,
+ * merge, rslope, plm_r, source, flux_phi, flux_r, update of substep 1, then of
+ * substep 2; for the fused one k_prep, k_sweep of substep 1 in [0], [1] and of
+ * substep 2 in [8], [9].  Synchronous.  For measurement only: inside the step
+ * graph of the eight kernels merge runs beside cellprep, and source and
+ * flux_phi beside flux_r. */
 int dgpu_step_rk2_timed(dgpu_ctx *ctx, int nsteps, double *kernel_ms);
-/* Autotuner (no counterpart in the reference): chooses, for the five heavy
- * step kernels, how many blocks of 256 threads each SM should hold (2..5, the
- * register budget per thread), by timing every choice on this context's own
- * disks from its current state with dgpu_step_rk2_timed (1 warm-up + `steps`
- * steps per choice), one kernel after the other.  The state, t and the
- * GravMass are restored afterwards, and results are bitwise the same under
- * every choice.  choice[5] (may be NULL) receives the chosen values in the
- * order plm_r, flux_phi, flux_r, source, update; with steps == 0 the given
- * choice[5] is applied instead (0 = the built-in value).  The next
- * dgpu_step_rk2 captures a new step graph.  Synchronous. */
+/* Autotuner (no counterpart in the reference): chooses how many blocks of 256
+ * threads each SM should hold for the heavy step kernels (the register budget
+ * per thread), by timing every choice on this context's own disks from its
+ * current state with dgpu_step_rk2_timed (1 warm-up + `steps` steps per
+ * choice), one kernel after the other: for the eight-kernel substep plm_r,
+ * flux_phi, flux_r, source and update (2..5 each), for the fused one k_sweep
+ * (2..4).  The state, t and the GravMass are restored afterwards, and results
+ * are bitwise the same under every choice.  choice[6] (may be NULL) receives
+ * the chosen values in the order plm_r, flux_phi, flux_r, source, update,
+ * sweep; with steps == 0 the given choice[6] is applied instead (0 = the
+ * built-in value).  The next dgpu_step_rk2 captures a new step graph.
+ * Synchronous. */
 int dgpu_autotune(dgpu_ctx *ctx, int steps, int *choice);
 /* Stage parity: the prologue of timestep_rk2 and the first substep
  * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`

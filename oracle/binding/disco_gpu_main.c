@@ -1,0 +1,193 @@
+/*
+ * The reference's own main loop with timestep_rk2 handed to the B200 library:
+ * the binding that INTEGRATION.md describes, compiled from the reference's
+ * objects (oracle/Makefile, target `binding`) and linked against
+ * libdisco_gpu.so.
+ *
+ * Set-up is the reference's (src/main.c:56-123: MPIsetup, Sim from the
+ * parfile, GravMass, cell_create with its srand(666) phi offsets, clean_pi,
+ * syncs, initial data, calc_cons).  Then the state crosses to the GPU once
+ * (cell_pack -> dgpu_set_state, the GravMass and t), the loop of
+ * src/main.c:124-141 calls dgpu_step_rk2 in place of timestep_rk2, and the
+ * state comes back (dgpu_get_state -> cell_unpack, the GravMass, t and dt)
+ * into the reference's own structures, which are dumped in the oracle
+ * driver's state format.
+ *
+ *   disco_gpu_main <par> <nsteps> <out.bin> [--eight]
+ *
+ * --eight steps with the eight-kernel substep instead of the fused one.
+ * Test infrastructure: the parity test compares its dump with the reference
+ * build's own run of the same parfile (disco_ref run).
+ */
+#define CELL_PRIVATE_DEFS
+#define PLANET_PRIVATE_DEFS
+#define TIMESTEP_PRIVATE_DEFS
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "Headers/Cell.h"
+#include "Headers/GravMass.h"
+#include "Headers/MPIsetup.h"
+#include "Headers/Sim.h"
+#include "Headers/TimeStep.h"
+#include "Headers/header.h"
+#include "cell_pack.h"
+#include "disco_gpu.h"
+#include "ref_newic.h"
+
+int readvar(char *filename, char *varname, int vartype, void *ptr);
+
+static int die(const char *what, const char *msg) {
+  fprintf(stderr, "%s: %s\n", what, msg ? msg : "");
+  return 1;
+}
+
+static void wr(FILE *f, const void *p, size_t sz, size_t n) {
+  if (fwrite(p, sz, n, f) != n) {
+    fprintf(stderr, "write failed\n");
+    exit(2);
+  }
+}
+
+/* the reference's cells, GravMass and clock in the driver's DSTATE1 format */
+static int dump(const char *path, struct Sim *s, struct Cell ***cells, struct GravMass *gm, struct TimeStep *ts) {
+  FILE *f = fopen(path, "wb");
+  int NR = sim_N(s, R_DIR), NZ = sim_N(s, Z_DIR), NQ = sim_NUM_Q(s), N = cell_pack_count(s);
+  int hdr[5] = {NR, NZ, NQ, N, 0}, i, n, p;
+  double td[2] = {ts->t, ts->dt}, g[12];
+  struct Cell *c = cells[0][0];
+  if (!f) return die("cannot open", path);
+  wr(f, "DSTATE1", 1, 8);
+  wr(f, hdr, sizeof(int), 5);
+  wr(f, td, sizeof(double), 2);
+  for (p = 0; p < 2; ++p) {
+    g[6 * p + 0] = gm[p].r;
+    g[6 * p + 1] = gm[p].phi;
+    g[6 * p + 2] = gm[p].M;
+    g[6 * p + 3] = gm[p].omega;
+    g[6 * p + 4] = gm[p].Mdot;
+    g[6 * p + 5] = gm[p].Macc;
+  }
+  wr(f, g, sizeof(double), 12);
+  for (i = 0; i < NR; ++i) {
+    int np = sim_N_p(s, i);
+    wr(f, &np, sizeof(int), 1);
+  }
+  for (i = -1; i < NR; ++i) {
+    double rf = sim_FacePos(s, i, R_DIR);
+    wr(f, &rf, sizeof(double), 1);
+  }
+  for (n = 0; n < N; ++n) wr(f, c[n].prim, sizeof(double), NQ);
+  for (n = 0; n < N; ++n) wr(f, c[n].cons, sizeof(double), NQ);
+  for (n = 0; n < N; ++n) wr(f, &c[n].tiph, sizeof(double), 1);
+  for (n = 0; n < N; ++n) wr(f, &c[n].dphi, sizeof(double), 1);
+  fclose(f);
+  return 0;
+}
+
+int main(int argc, char **argv) {
+  char parbuf[1024];
+  int nsteps, step, p, eight = 0, N, NQ;
+  double g6[12], t, dt;
+  double *prim, *cons, *tiph, *dphi;
+  struct MPIsetup *mpi;
+  struct Sim *s;
+  struct GravMass *gm;
+  struct Cell ***cells;
+  struct TimeStep *ts;
+  dgpu_sim *gs = NULL;
+  dgpu_ctx *gctx = NULL;
+  if (argc < 4) {
+    fprintf(stderr, "usage: disco_gpu_main <parfile> <nsteps> <out.bin> [--eight]\n");
+    return 2;
+  }
+  strncpy(parbuf, argv[1], sizeof(parbuf) - 1);
+  parbuf[sizeof(parbuf) - 1] = 0;
+  nsteps = atoi(argv[2]);
+  if (argc > 4 && !strcmp(argv[4], "--eight")) eight = 1;
+  /* the reference prints read notices on stdout */
+  if (!freopen("/dev/null", "w", stdout)) return 2;
+
+  /* src/main.c:56-119 */
+  mpi = mpisetup_create(argc, argv);
+  mpisetup_setprocs(mpi, parbuf);
+  mpisetup_cart_create(mpi);
+  mpisetup_left_right(mpi);
+  s = sim_create(mpi);
+  if (sim_read_par_file(s, mpi, parbuf) != 0) return die("parfile read failed", parbuf);
+  readvar(parbuf, "IC_HoR", VAR_DOUB, &oracle_ic_hor);
+  readvar(parbuf, "IC_Noise", VAR_DOUB, &oracle_ic_noise);
+  readvar(parbuf, "IC_Seed", VAR_INT, &oracle_ic_seed);
+  sim_alloc_arr(s, mpi);
+  sim_set_rz(s, mpi);
+  sim_set_N_p(s);
+  sim_set_misc(s, mpi);
+  gm = gravMass_create(sim_NumGravMass(s));
+  cells = cell_create(s, mpi);
+  cell_clean_pi(cells, s);
+  cell_syncproc_r(cells, s, mpi);
+  cell_syncproc_z(cells, s, mpi);
+  ts = timestep_create(s);
+  (*gravMass_init_ptr(s))(gm, s);
+  (*cell_init_ptr(s))(cells, s, gm, mpi);
+  gravMass_clean_pi(gm, s);
+  cell_syncproc_r(cells, s, mpi);
+  cell_syncproc_z(cells, s, mpi);
+  cell_calc_cons(cells, s);
+
+  /* the state crosses to the GPU once */
+  N = cell_pack_count(s);
+  NQ = sim_NUM_Q(s);
+  prim = (double *)malloc(sizeof(double) * (size_t)N * (size_t)NQ);
+  cons = (double *)malloc(sizeof(double) * (size_t)N * (size_t)NQ);
+  tiph = (double *)malloc(sizeof(double) * (size_t)N);
+  dphi = (double *)malloc(sizeof(double) * (size_t)N);
+  if (!prim || !cons || !tiph || !dphi) return die("out of memory", NULL);
+  if (dgpu_sim_from_parfile(parbuf, &gs) != DGPU_OK) return die("dgpu_sim_from_parfile", dgpu_last_error(NULL));
+  if (dgpu_sim_num_cells(gs) != N) return die("grid", "the library's grid differs from the reference's");
+  if (dgpu_create((const dgpu_sim *const *)&gs, 1, 0, NULL, &gctx) != DGPU_OK)
+    return die("dgpu_create", dgpu_last_error(NULL));
+  if (eight && dgpu_set_fused(gctx, 0) != DGPU_OK) return die("dgpu_set_fused", dgpu_last_error(gctx));
+  cell_pack(cells, s, prim, tiph, dphi);
+  for (p = 0; p < 2; ++p) {
+    g6[6 * p + 0] = gm[p].r;
+    g6[6 * p + 1] = gm[p].phi;
+    g6[6 * p + 2] = gm[p].M;
+    g6[6 * p + 3] = gm[p].omega;
+    g6[6 * p + 4] = gm[p].Mdot;
+    g6[6 * p + 5] = gm[p].Macc;
+  }
+  if (dgpu_set_state(gctx, 0, prim, tiph, dphi) != DGPU_OK || dgpu_set_gravmass(gctx, 0, g6) != DGPU_OK ||
+      dgpu_set_time(gctx, 0, timestep_get_t(ts)) != DGPU_OK)
+    return die("state upload", dgpu_last_error(gctx));
+
+  /* src/main.c:124-141: timestep_rk2 becomes dgpu_step_rk2 */
+  for (step = 0; step < nsteps && timestep_get_t(ts) < sim_get_T_MAX(s); ++step) {
+    if (dgpu_step_rk2(gctx, 1) != DGPU_OK || dgpu_get_time(gctx, 0, &t, &dt) != DGPU_OK)
+      return die("dgpu_step_rk2", dgpu_last_error(gctx));
+    ts->t = t;
+    ts->dt = dt;
+  }
+
+  /* and back into the reference's structures */
+  if (dgpu_get_state(gctx, 0, prim, cons, tiph, dphi) != DGPU_OK || dgpu_get_gravmass(gctx, 0, g6) != DGPU_OK)
+    return die("state download", dgpu_last_error(gctx));
+  cell_unpack(cells, s, prim, cons, tiph, dphi);
+  for (p = 0; p < 2; ++p) {
+    gm[p].r = g6[6 * p + 0];
+    gm[p].phi = g6[6 * p + 1];
+    gm[p].M = g6[6 * p + 2];
+    gm[p].omega = g6[6 * p + 3];
+    gm[p].Mdot = g6[6 * p + 4];
+    gm[p].Macc = g6[6 * p + 5];
+  }
+  if (dump(argv[3], s, cells, gm, ts)) return 2;
+  dgpu_destroy(gctx);
+  dgpu_sim_destroy(gs);
+  free(prim);
+  free(cons);
+  free(tiph);
+  free(dphi);
+  return 0;
+}

@@ -22,6 +22,9 @@ PORT_LIB = os.path.join(HERE, "_build", "libdisco_port.so")
 # the restatement built with every libm result in the step moved by one ulp
 # (the sensitivity of a case to last-ulp differences; tests only)
 PORT_ULP_BIN = os.path.join(HERE, "_build", "disco_port_ulp")
+# the reference's main loop stepping through the B200 library (binding/)
+BINDING_BIN = os.path.join(HERE, "_ref", "disco_gpu_main")
+GPU_LIB = os.path.join(os.path.dirname(HERE), "disco2_b200", "_lib", "libdisco_gpu.so")
 # the reference tree where it is mounted (override with DISCO_REFSRC)
 REFSRC = os.environ.get("DISCO_REFSRC", "/root/reference/src")
 
@@ -33,6 +36,8 @@ def build(ref: bool | None = None, port: bool = True) -> None:
         ref = os.path.isdir(REFSRC)
     port = port and os.path.exists(os.path.join(HERE, "port", "disco_port.c"))
     targets = (["ref"] if ref else []) + (["port"] if port else [])
+    if ref and os.path.exists(GPU_LIB):
+        targets.append("binding")
     if targets:
         subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
 

@@ -7,6 +7,8 @@ import os
 import re
 import subprocess
 
+import pytest
+
 from conftest import ROOT
 from disco2_b200 import lib
 
@@ -43,3 +45,17 @@ def test_exports_are_exactly_the_declared_abi():
 
 def test_python_binding_covers_the_header():
     assert set(lib.SIGNATURES) == declared_symbols()
+
+
+def test_binding_links_the_library_abi():
+    """The compiled Disco2-side binding (oracle/binding) resolves its dgpu_*
+    calls against libdisco_gpu.so."""
+    import oracle
+    if not os.path.exists(oracle.BINDING_BIN):
+        pytest.skip("binding not built (needs the reference sources)")
+    out = subprocess.run(["nm", "-D", "--undefined-only", oracle.BINDING_BIN], capture_output=True,
+                         text=True, check=True).stdout
+    used = {ln.split()[-1] for ln in out.splitlines() if "dgpu_" in ln}
+    assert {"dgpu_create", "dgpu_set_state", "dgpu_step_rk2", "dgpu_get_state", "dgpu_set_fused"} <= used
+    ldd = subprocess.run(["ldd", oracle.BINDING_BIN], capture_output=True, text=True).stdout
+    assert "libdisco_gpu.so" in ldd and "not found" not in ldd
