@@ -299,6 +299,8 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
         return sum(s.elapsed_time(e) for s, e in ev)
 
     ctx = lib.Context(sims, device=int(os.environ.get("LOCAL_RANK", "0")), stream=stream.cuda_stream)
+    if args.fused:
+        ctx.set_fused(True)
     for k in range(len(sims)):
         ctx.init_state(k)
     barrier()
@@ -307,6 +309,8 @@ def run_batched(args, rank, world, flush, barrier, max_over_ranks):
     ms_seq = 0.0
     for s in sims:
         c1 = lib.Context(s, device=int(os.environ.get("LOCAL_RANK", "0")), stream=stream.cuda_stream)
+        if args.fused:
+            c1.set_fused(True)
         c1.init_state(0)
         ms_seq += timed(c1)
         c1.close()
@@ -390,8 +394,8 @@ def main():
                     help="steps per launch-shape candidate for the autotuner (0: built-in shapes)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=500)
-    ap.add_argument("--eight", action="store_true",
-                    help="time the eight-kernel substep instead of the fused one")
+    ap.add_argument("--fused", action="store_true",
+                    help="time the fused substep (k_prep + k_sweep) instead of the eight kernels")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -427,8 +431,8 @@ def main():
     nin = interior_cells(sim)
     stream = torch.cuda.Stream()
     ctx = lib.Context(sim, device=local, stream=stream.cuda_stream)
-    if args.eight:
-        ctx.set_fused(False)
+    if args.fused:
+        ctx.set_fused(True)
     ctx.init_state(0)
     L = lib.load()
     # launch shapes of the heavy kernels timed on this disk (state restored)

@@ -1286,15 +1286,50 @@ __device__ __forceinline__ void sweep_wait(const DevPtrs &d, int a, int v) {
   __syncthreads();
 }
 
-// The update of annulus b's cells (update_cell) once its increments are in
-// place, with the annulus's constants of the substep.
-__device__ __forceinline__ void sweep_update(const DevPtrs &d, const TanPtrs &tp, int b, int substep,
-                                             const InstState &S, double dt) {
+// The phases of k_sweep for the block's annulus (the block's threads stride
+// over the annulus's faces or cells).  Inlined: as separate calls they spill
+// more across the call boundaries and run slower (measured).
+#define SWEEP_FN __device__ __forceinline__
+SWEEP_FN void sweep_slopes(const DevPtrs &d, int a) {
+  const TanPtrs tp = {};
+  const Annulus &A = d.ann[a];
+  const int nf = d.pair_nf[a];
+  for (int n = threadIdx.x; n < nf; n += BLK) rslope_face<double, false>(d, tp, A.face_base + n);
+}
+SWEEP_FN void sweep_grad(const DevPtrs &d, int a) {
+  const TanPtrs tp = {};
+  const Annulus &A = d.ann[a];
+  for (int j = threadIdx.x; j < A.np; j += BLK) plm_r_grad<double, false>(d, tp, A.cell_off + j);
+}
+SWEEP_FN void sweep_flux_r(const DevPtrs &d, int b, const InstState &S, double dt) {
+  const TanPtrs tp = {};
+  const Annulus &Q = d.ann[b];
+  const int nf = d.pair_nf[b];
+  for (int n = threadIdx.x; n < nf; n += BLK) flux_r_face<double, false>(d, tp, Q.face_base + n, S, dt);
+}
+SWEEP_FN void sweep_cells(const DevPtrs &d, int a, const InstState &S, double dt) {
+  const TanPtrs tp = {};
+  const Annulus &A = d.ann[a];
+  double md0 = 0.0, md1 = 0.0;
+  for (int j = threadIdx.x; j < A.np; j += BLK) {
+    const int g = A.cell_off + j;
+    flux_phi_cell<double, false>(d, tp, g, S, dt);
+    source_cell_k<double, false>(d, tp, g, S, dt, md0, md1);
+  }
+}
+SWEEP_FN void sweep_update_cells(const DevPtrs &d, int b, int substep, double dt) {
+  const TanPtrs tp = {};
   const Annulus &B = d.ann[b];
-  if (threadIdx.x == 0) ann_consts(d, b, S, dt);
-  __syncthreads();
   for (int j = threadIdx.x; j < B.np; j += BLK)
     update_cell<double, false, true>(d, tp, B.cell_off + j, substep, 7, dt, nullptr, nullptr);
+}
+
+// The update of annulus b's cells (update_cell) once its increments are in
+// place, with the annulus's constants of the substep.
+__device__ __forceinline__ void sweep_update(const DevPtrs &d, int b, int substep, const InstState &S, double dt) {
+  if (threadIdx.x == 0) ann_consts(d, b, S, dt);
+  __syncthreads();
+  sweep_update_cells(d, b, substep, dt);
 }
 
 // k_sweep: the rest of the substep as one wavefront over the annuli.  Each
@@ -1314,11 +1349,10 @@ __device__ __forceinline__ void sweep_update(const DevPtrs &d, const TanPtrs &tp
 // trips between eight kernels, and phases of different annuli overlap on the
 // SMs.
 template <int MB>
-__global__ void __launch_bounds__(BLK, MB) k_sweep(DevPtrs d, int substep) {
+__global__ void __launch_bounds__(BLK, MB) k_sweep(const __grid_constant__ DevPtrs d, int substep) {
   __shared__ int s_a;
   __shared__ InstState s_S;
   __shared__ bool s_last;
-  const TanPtrs tp = {};
   if (threadIdx.x == 0) s_a = (int)atomicAdd(&d.counters[3], 1u);
   __syncthreads();
   const int a = s_a;
@@ -1340,40 +1374,29 @@ __global__ void __launch_bounds__(BLK, MB) k_sweep(DevPtrs d, int substep) {
   }
   __syncthreads();
   const double dt = (substep == 1 ? 1.0 : 0.5) * s_S.dt;
+  const int first = A.i == 0, last = A.i == P.NR - 1;
   // 1. face slopes of pair (a, a+1)
-  if (A.i < P.NR - 1) {
-    const int nf = d.pair_nf[a];
-    for (int n = threadIdx.x; n < nf; n += BLK) rslope_face<double, false>(d, tp, A.face_base + n);
-  }
+  if (!last) sweep_slopes(d, a);
   sweep_publish(d, a, 1);
   // 2. r slopes of annulus a
-  if (A.i > 0) sweep_wait(d, a - 1, 1);
-  for (int j = threadIdx.x; j < A.np; j += BLK) plm_r_grad<double, false>(d, tp, A.cell_off + j);
+  if (!first) sweep_wait(d, a - 1, 1);
+  sweep_grad(d, a);
   sweep_publish(d, a, 2);
   // 3. fluxes of pair (a-1, a); phi faces and sources of annulus a
-  if (A.i > 0) {
+  if (!first) {
     sweep_wait(d, a - 1, 2);
-    const Annulus &Q = d.ann[a - 1];
-    const int nf = d.pair_nf[a - 1];
-    for (int n = threadIdx.x; n < nf; n += BLK) flux_r_face<double, false>(d, tp, Q.face_base + n, s_S, dt);
+    sweep_flux_r(d, a - 1, s_S, dt);
   }
-  {
-    double md0 = 0.0, md1 = 0.0;
-    for (int j = threadIdx.x; j < A.np; j += BLK) {
-      const int g = A.cell_off + j;
-      flux_phi_cell<double, false>(d, tp, g, s_S, dt);
-      source_cell_k<double, false>(d, tp, g, s_S, dt, md0, md1);
-    }
-  }
+  sweep_cells(d, a, s_S, dt);
   sweep_publish(d, a, 3);
   // 4. update of annulus a-1, then of the disk's last annulus
-  if (A.i > 0) {
+  if (!first) {
     sweep_wait(d, a - 1, 3);
-    sweep_update(d, tp, a - 1, substep, s_S, dt);
+    sweep_update(d, a - 1, substep, s_S, dt);
   }
-  if (A.i == P.NR - 1) {
+  if (last) {
     __syncthreads();
-    sweep_update(d, tp, a, substep, s_S, dt);
+    sweep_update(d, a, substep, s_S, dt);
   }
   // the last block: the GravMass of every disk.  It reads nothing that
   // another block of this kernel writes.

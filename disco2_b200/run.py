@@ -1,6 +1,6 @@
 """Run a named workload for a few RK2 steps on cuda:0.
 
-    python -m disco2_b200.run --workload circumbinary --steps 3 [--timed] [--batch N] [--eight]
+    python -m disco2_b200.run --workload circumbinary --steps 3 [--timed] [--batch N] [--fused]
     python -m disco2_b200.run --workload circumbinary --num-r 192 --steps 0 --adjoint 10 --ckpt 5
 
 Used for profiling (ncu attaches to this process) and as a minimal example of
@@ -8,7 +8,7 @@ the C ABI from Python.  --timed adds one step launched kernel by kernel
 with CUDA events and prints the per-kernel device times.  --batch N steps N
 copies of the disk in one context.  --adjoint N then runs the gradient of an
 N-step run (objectives over its second half, checkpoints every --ckpt steps).
---eight steps with the eight-kernel substep instead of the fused one.
+--fused steps with the fused substep (k_prep + k_sweep) instead of the eight kernels.
 """
 from __future__ import annotations
 
@@ -28,13 +28,13 @@ def main() -> None:
     ap.add_argument("--batch", type=int, default=1)
     ap.add_argument("--adjoint", type=int, default=0)
     ap.add_argument("--ckpt", type=int, default=25)
-    ap.add_argument("--eight", action="store_true")
+    ap.add_argument("--fused", action="store_true")
     args = ap.parse_args()
     p = WORKLOADS[args.workload]() if args.num_r is None else WORKLOADS[args.workload](num_r=args.num_r)
     sims = [lib.Sim(p) for _ in range(args.batch)]
     ctx = lib.Context(sims)
-    if args.eight:
-        ctx.set_fused(False)
+    if args.fused:
+        ctx.set_fused(True)
     for k in range(args.batch):
         ctx.init_state(k)
     if args.steps:

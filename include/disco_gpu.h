@@ -114,12 +114,13 @@ int dgpu_synchronize(dgpu_ctx *ctx);
  * cell_plm_p and, in substep 1, the CFL minimum) and k_sweep (one wavefront
  * over the annuli: face slopes, r slopes, the r- and phi-face fluxes, the
  * sources and the update).  The other form is eight kernels per substep
- * (cellprep, merge, rslope, plm_r, source, flux_phi, flux_r, update).  A
- * context uses the fused form when all its disks allow it (no passive scalar,
- * no outflow radial boundary, no sink); dgpu_set_fused(ctx, 0) selects the
- * eight kernels, dgpu_set_fused(ctx, 1) the fused form (DGPU_ERR_UNSUPPORTED
- * where not allowed).  dgpu_fused returns 1 when the step uses the fused
- * form.  The tangent, adjoint and stage runs always use the eight kernels. */
+ * (cellprep, merge, rslope, plm_r, source, flux_phi, flux_r, update), the
+ * default, which is the faster on B200.  dgpu_set_fused(ctx, 1) selects the
+ * fused form where every disk of the context allows it (no passive scalar, no
+ * outflow radial boundary, no sink; else DGPU_ERR_UNSUPPORTED),
+ * dgpu_set_fused(ctx, 0) the eight kernels.  dgpu_fused returns 1 when the
+ * step uses the fused form.  The tangent, adjoint and stage runs always use
+ * the eight kernels. */
 int dgpu_set_fused(dgpu_ctx *ctx, int fused);
 int dgpu_fused(const dgpu_ctx *ctx);
 /* The same steps launched one kernel at a time with CUDA events between the

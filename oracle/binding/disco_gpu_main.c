@@ -13,9 +13,10 @@
  * into the reference's own structures, which are dumped in the oracle
  * driver's state format.
  *
- *   disco_gpu_main <par> <nsteps> <out.bin> [--eight]
+ *   disco_gpu_main <par> <nsteps> <out.bin> [--fused]
  *
- * --eight steps with the eight-kernel substep instead of the fused one.
+ * --fused steps with the fused substep (k_prep + k_sweep) instead of the
+ * eight kernels.
  * Test infrastructure: the parity test compares its dump with the reference
  * build's own run of the same parfile (disco_ref run).
  */
@@ -88,7 +89,7 @@ static int dump(const char *path, struct Sim *s, struct Cell ***cells, struct Gr
 
 int main(int argc, char **argv) {
   char parbuf[1024];
-  int nsteps, step, p, eight = 0, N, NQ;
+  int nsteps, step, p, fused = 0, N, NQ;
   double g6[12], t, dt;
   double *prim, *cons, *tiph, *dphi;
   struct MPIsetup *mpi;
@@ -99,13 +100,13 @@ int main(int argc, char **argv) {
   dgpu_sim *gs = NULL;
   dgpu_ctx *gctx = NULL;
   if (argc < 4) {
-    fprintf(stderr, "usage: disco_gpu_main <parfile> <nsteps> <out.bin> [--eight]\n");
+    fprintf(stderr, "usage: disco_gpu_main <parfile> <nsteps> <out.bin> [--fused]\n");
     return 2;
   }
   strncpy(parbuf, argv[1], sizeof(parbuf) - 1);
   parbuf[sizeof(parbuf) - 1] = 0;
   nsteps = atoi(argv[2]);
-  if (argc > 4 && !strcmp(argv[4], "--eight")) eight = 1;
+  if (argc > 4 && !strcmp(argv[4], "--fused")) fused = 1;
   /* the reference prints read notices on stdout */
   if (!freopen("/dev/null", "w", stdout)) return 2;
 
@@ -148,7 +149,7 @@ int main(int argc, char **argv) {
   if (dgpu_sim_num_cells(gs) != N) return die("grid", "the library's grid differs from the reference's");
   if (dgpu_create((const dgpu_sim *const *)&gs, 1, 0, NULL, &gctx) != DGPU_OK)
     return die("dgpu_create", dgpu_last_error(NULL));
-  if (eight && dgpu_set_fused(gctx, 0) != DGPU_OK) return die("dgpu_set_fused", dgpu_last_error(gctx));
+  if (fused && dgpu_set_fused(gctx, 1) != DGPU_OK) return die("dgpu_set_fused", dgpu_last_error(gctx));
   cell_pack(cells, s, prim, tiph, dphi);
   for (p = 0; p < 2; ++p) {
     g6[6 * p + 0] = gm[p].r;

@@ -24,8 +24,8 @@ EXACT = {"gresho16"}
 
 
 @pytest.mark.parametrize("name", ["gresho16", "kepler24", "cbd32"])
-@pytest.mark.parametrize("eight", [False, True])
-def test_c_main_loop_through_the_library_matches_the_reference(name, eight):
+@pytest.mark.parametrize("fused", [False, True])
+def test_c_main_loop_through_the_library_matches_the_reference(name, fused):
     if not (os.path.exists(oracle.BINDING_BIN) and oracle.have_ref()):
         pytest.skip("binding or reference build absent (built where the reference sources are mounted)")
     g = golden(name)
@@ -34,7 +34,7 @@ def test_c_main_loop_through_the_library_matches_the_reference(name, eight):
         with open(par, "w") as f:
             f.write(str(g["parfile"]))
         out = os.path.join(td, "gpu.bin")
-        cmd = [oracle.BINDING_BIN, par, "5", out] + (["--eight"] if eight else [])
+        cmd = [oracle.BINDING_BIN, par, "5", out] + (["--fused"] if fused else [])
         r = subprocess.run(cmd, capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
         got = oracle.read_state(out)

@@ -2,10 +2,9 @@
 
 Both forms evaluate the same per-face and per-cell functions in the same
 order, so the fused step must equal the eight-kernel step bit for bit: state,
-time, dt and the GravMass orbit.  The eight-kernel form is itself pinned to
-the reference build (test_gpu_parity.py, test_gpu_fullsize_parity.py), and the
-default step of a context that allows it is the fused one, so those tests
-check the fused form against the reference directly as well.
+time, dt and the GravMass orbit.  The eight-kernel form, the default, is
+itself pinned to the reference build (test_gpu_parity.py,
+test_gpu_fullsize_parity.py).
 """
 import numpy as np
 import pytest
@@ -43,9 +42,13 @@ def _same(a, b, what):
 
 def _eligible(sim) -> bool:
     ctx = lib.Context(sim)
-    ok = ctx.fused
-    ctx.close()
-    return ok
+    try:
+        ctx.set_fused(True)
+        return True
+    except lib.DiscoError:
+        return False
+    finally:
+        ctx.close()
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -81,8 +84,10 @@ def test_fused_equals_eight_kernels_with_many_disks():
         _same(f[k], e[k], k)
 
 
-def test_fused_is_the_default_and_refused_where_not_covered():
+def test_fused_is_opt_in_and_refused_where_not_covered():
     ctx = lib.Context(lib.Sim(configs.gresho(num_r=16)))
+    assert not ctx.fused and len(ctx.kernels) == 8
+    ctx.set_fused(True)
     assert ctx.fused and ctx.kernels == ("prep", "sweep")
     ctx.close()
     g = golden("vortex16dye")  # passive scalar
@@ -98,6 +103,7 @@ def test_fused_timed_step_equals_graph_step():
     sim = lib.Sim(configs.circumbinary(num_r=64))
     a = _advance([sim], True, 2)[0]
     ctx = lib.Context(sim)
+    ctx.set_fused(True)
     ctx.init_state(0)
     ms = ctx.step_timed(2)
     assert set(ms) == {"prep", "sweep"} and all(v[0] > 0 and v[1] > 0 for v in ms.values())
