@@ -896,22 +896,30 @@ int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
 }
 
 int dgpu_stage(dgpu_ctx *c, int phase) {
-  if (!c || phase < 0 || phase > 7) return DGPU_ERR_ARG;
+  int sub = phase >= 8 ? 2 : 1, stop = phase & 7;
+  if (!c || phase < 0 || phase > 15) return DGPU_ERR_ARG;
   cudaSetDevice(c->device);
-  CKK(dgk_cellprep(&c->d, NULL, 1, c->stream));
-  CKK(dgk_merge(&c->d, 1, c->stream));
+  /* phases 8-15: the whole first substep (its k_update also moves the
+   * GravMass, as timestep_rk2 does between the substeps), then the second */
+  if (sub == 2) {
+    int rc = dctx_substep(c, NULL, 1, DCTX_FULL, NULL, NULL);
+    if (rc) return rc;
+  }
+  CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
+  CKK(dgk_merge(&c->d, sub, c->stream));
   /* the CFL minimum (and dt) come from k_plm_r; PLM results are kept only from phase 1 on */
   CKK(dgk_rslope(&c->d, NULL, c->stream));
-  CKK(dgk_plm_r(&c->d, NULL, 1, c->stream));
-  CKK(dgk_source(&c->d, NULL, 1, c->stream));
-  if (phase >= 2) {
-    CKK(dgk_flux_phi(&c->d, NULL, 1, c->stream));
-    CKK(dgk_flux_r(&c->d, NULL, 1, c->stream));
+  CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
+  CKK(dgk_source(&c->d, NULL, sub, c->stream));
+  if (stop >= 2) {
+    CKK(dgk_flux_phi(&c->d, NULL, sub, c->stream));
+    CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
   }
-  CKK(dgk_update_stage(&c->d, 1, phase, c->stream));
-  if (phase >= 6 && c->n_ob > 0) CKK(dgk_outflow(&c->d, phase, c->stream));
-  /* from phase 5 on the advanced phi edges live in the substep's output buffer */
-  if (phase >= 5)
+  CKK(dgk_update_stage(&c->d, sub, stop, c->stream));
+  if (stop >= 6 && c->n_ob > 0) CKK(dgk_outflow(&c->d, stop, c->stream));
+  /* from phase 5 of substep 1 on the advanced phi edges live in the substep's
+   * output buffer (substep 2 writes them where the state is read) */
+  if (sub == 1 && stop >= 5)
     CK(cudaMemcpyAsync(c->d.tiph0, c->d.tiph1, sizeof(double) * (size_t)c->n_cells,
                        cudaMemcpyDeviceToDevice, c->stream));
   return dgpu_synchronize(c);

@@ -148,7 +148,10 @@ int dgpu_autotune(dgpu_ctx *ctx, int steps, int *choice);
 /* Stage parity: the prologue of timestep_rk2 and the first substep
  * (src/TimeStep/timestep_routines.c:16-113) stopped after `phase`
  * (0 faces/clean_pi/set_w/RK blend, 1 PLM, 2 phi fluxes, 3 r fluxes,
- * 4 sources, 5 mesh motion + cons2prim, 6 boundary + damping, 7 calc_cons).
+ * 4 sources, 5 mesh motion + cons2prim, 6 boundary + damping, 7 calc_cons);
+ * phases 8-15: the whole first substep and gravMass_move
+ * (src/TimeStep/timestep_algorithm.c:23-28), then the second substep stopped
+ * after phase - 8 (its RKtiph is not stored: only the first substep's is).
  * Leaves the context mid-step; reload the state before stepping again. */
 int dgpu_stage(dgpu_ctx *ctx, int phase);
 /* Per-cell intermediates after dgpu_stage: grad, gradp ([N][NUM_Q]), wiph[N],

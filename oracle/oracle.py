@@ -183,7 +183,9 @@ def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = No
 
 
 def stage(parfile: str, phase: int, *, impl: str = "ref", load: State | None = None) -> State:
-    """Run the prologue of one RK2 step and the first substep up to `phase`."""
+    """Run the prologue of one RK2 step and the first substep up to `phase`
+    (0-7), or all of the first substep and the second up to `phase` - 8
+    (8-15)."""
     exe = _exe(impl)
     with tempfile.TemporaryDirectory() as td:
         out = os.path.join(td, "out.bin")

@@ -1360,6 +1360,18 @@ void port_prologue(Port *p) {
   p->RK = 0.0;
 }
 
+void port_stage(Port *p, int phase) {
+  port_prologue(p);
+  if (phase >= 8) {
+    port_substep(p, 1.0, 7);
+    gm_move(p, p->t, 1.0 * p->dt);
+    p->RK = 0.5;
+    port_substep(p, 0.5, phase - 8);
+  } else {
+    port_substep(p, 1.0, phase);
+  }
+}
+
 void port_step_rk2(Port *p) {
   int k;
   port_prologue(p);

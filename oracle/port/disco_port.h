@@ -70,5 +70,8 @@ void port_build_faces(Port *p);        /* face_create(..., 0) */
 void port_step_rk2(Port *p);           /* timestep_rk2 */
 void port_prologue(Port *p);           /* timestep_rk2 up to the first substep */
 void port_substep(Port *p, double fac, int stop);  /* timestep_substep, stopped after a phase */
+/* the prologue of timestep_rk2, then phase 0-7 of substep 1, or (8-15) all of
+ * substep 1, gravMass_move, and phase - 8 of substep 2 */
+void port_stage(Port *p, int phase);
 
 #endif

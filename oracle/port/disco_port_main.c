@@ -4,7 +4,7 @@
  * and the CPU baseline run either oracle interchangeably:
  *   disco_port run <par> <nsteps> <out.bin> [--load in.bin] [--faces f.bin]
  *                  [--dtlog log.txt] [--warmup W]
- *   disco_port stage <par> <phase> <out.bin> [--load in.bin]
+ *   disco_port stage <par> <phase> <out.bin> [--load in.bin]   (phase 0-15)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -141,8 +141,7 @@ int main(int argc, char **argv) {
     if (flog) fclose(flog);
     dump_state(out, &P, 0);
   } else if (!strcmp(mode, "stage")) {
-    port_prologue(&P);
-    port_substep(&P, 1.0, n);
+    port_stage(&P, n);
     dump_state(out, &P, 1);
   } else {
     return 2;

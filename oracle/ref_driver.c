@@ -40,7 +40,10 @@
  *       the same reference functions in the same order, and stops after
  *       <phase> (0: faces+clean_pi+set_w+RK blend, 1: PLM, 2: phi fluxes,
  *       3: r fluxes, 4: sources, 5: mesh motion+cons2prim, 6: BC+damping,
- *       7: calc_cons), dumping the extended cell data.
+ *       7: calc_cons), dumping the extended cell data.  Phases 8-15: the
+ *       whole first substep (timestep_substep, then gravMass_move and
+ *       timestep_set_RK(0.5) as timestep_rk2 does), then the second substep
+ *       stopped after <phase> - 8.
  *
  * State file (little endian): "DSTATE1\0", int32 NR NZ NUM_Q Ncells ext,
  * double t dt, double gm[2][6] (r phi M omega Mdot Macc), int32 N_p[NR],
@@ -425,7 +428,15 @@ int main(int argc, char **argv) {
     cell_copy(cells, s);
     gravMass_copy(gm, s);
     timestep_set_RK(ts, 0.0);
-    substep_phases(ts, cells, s, gm, mpi, 1.0, nsteps);
+    if (nsteps >= 8) {
+      /* timestep_algorithm.c:23-29 */
+      timestep_substep(ts, cells, s, gm, mpi, 1.0);
+      gravMass_move(s, gm, timestep_get_t(ts), 1.0 * timestep_dt(ts));
+      timestep_set_RK(ts, 0.5);
+      substep_phases(ts, cells, s, gm, mpi, 0.5, nsteps - 8);
+    } else {
+      substep_phases(ts, cells, s, gm, mpi, 1.0, nsteps);
+    }
     dump_state(out, s, cells, gm, ts, 1);
   } else {
     fprintf(stderr, "unknown mode %s\n", mode);

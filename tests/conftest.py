@@ -38,6 +38,11 @@ def golden(name: str) -> dict:
         return {k: z[k] for k in z.files}
 
 
+def golden_sub2(name: str) -> dict:
+    """The second substep's phases of a case (make_golden.py --substep2)."""
+    return golden(name + "_sub2")
+
+
 @pytest.fixture(params=CASES)
 def case(request):
     return request.param, golden(request.param)

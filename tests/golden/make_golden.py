@@ -3,7 +3,8 @@
 Run where the reference sources are mounted (oracle/_ref/disco_ref is built
 from them by oracle/Makefile):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py               # <case>.npz
+    python tests/golden/make_golden.py --substep2    # <case>_sub2.npz
 
 Every fixture is the reference's own output (timestep_rk2 / face_create /
 the substep phases of timestep_substep) on a small disk, stored as a
@@ -137,6 +138,39 @@ def face_cases(par: str, st0: oracle.State, rng: np.random.Generator) -> dict:
     return out
 
 
+# the second substep's phases (dgpu_stage / the driver's stage mode 8-15):
+# the whole first substep, gravMass_move, then the second substep stopped
+# after phase - 8.  Its RKtiph is left out: the reference re-adjusts RKtiph by
+# whole turns in the second cell_update_phi, a copy that nothing reads after
+# the substep and that the GPU does not store.
+PHASES2 = tuple(range(8, 16))
+PHASE2_KEYS = {ph: tuple(k for k in PHASE_KEYS[ph - 8] if k != "RKtiph") for ph in PHASES2}
+
+
+def substep2(names: list[str]) -> None:
+    """Writes <name>_sub2.npz: the second substep's phases of each case, from
+    the same 5-step state as the first substep's phases."""
+    if not oracle.have_ref():
+        oracle.build(ref=True, port=False)
+    with tempfile.TemporaryDirectory() as td:
+        for name, p in CASES.items():
+            if names and name not in names:
+                continue
+            par = configs.write_parfile(p, os.path.join(td, name + ".par"))
+            data = {"parfile": np.array(configs.parfile_text(p))}
+            st5 = oracle.run(par, 5)[0]
+            for ph in PHASES2:
+                st = oracle.stage(par, ph, load=st5)
+                full = _state_dict(st, "", ext=True)
+                for k in PHASE2_KEYS[ph]:
+                    data[f"stage{ph}_{k}"] = full[k]
+                data[f"stage{ph}_dt"] = np.float64(st.dt)
+                data[f"stage{ph}_gm"] = st.gm
+            path = os.path.join(HERE, name + "_sub2.npz")
+            np.savez_compressed(path, **data)
+            print(name, "second substep", os.path.getsize(path), "bytes")
+
+
 def main(names: list[str]) -> None:
     """Writes the fixtures of the named cases (all cases when none is named);
     each case draws its face layouts from its own seeded generator."""
@@ -174,4 +208,7 @@ def main(names: list[str]) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:])
+    if sys.argv[1:2] == ["--substep2"]:
+        substep2(sys.argv[2:])
+    else:
+        main(sys.argv[1:])

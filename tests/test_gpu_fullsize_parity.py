@@ -133,14 +133,20 @@ def test_sweep_disks_in_one_context_match_the_oracle(impl):
     ctx.close()
 
 
-def test_circumbinary_full_size_100_steps_l1(impl):
-    """The headline correctness bar on the headline disk: the 258,078-cell
-    circumbinary disk after 100 RK2 steps, against the reference run on the
-    host from the same initial state. rho (D), momenta (S_r, L) and energy
-    (tau) agree to L1-relative 1e-10; t to 1e-12 relative."""
-    p = configs.circumbinary()
+@pytest.mark.parametrize("name,make,exact", [("gresho_96", configs.gresho, True),
+                                              ("kepler_ring_256", configs.kepler_ring, False),
+                                              ("circumbinary_400", configs.circumbinary, False)])
+def test_full_size_100_steps_l1(name, make, exact, impl):
+    """The headline correctness bar on the three benchmark disks at their full
+    sizes: the Gresho vortex (96 annuli, 36k cells), the viscous Keplerian ring
+    (256 annuli, 199k cells) and the circumbinary disk (400 annuli, 258k cells)
+    after 100 RK2 steps, against the reference run on the host from the same
+    initial state. rho (D), momenta (S_r, L) and energy (tau) agree to
+    L1-relative 1e-10 and t to 1e-12 relative; the Gresho vortex (no device
+    transcendental on its path) bit for bit."""
+    p = make()
     with tempfile.TemporaryDirectory() as td:
-        par = configs.write_parfile(p, os.path.join(td, "cbd400.par"))
+        par = configs.write_parfile(p, os.path.join(td, name + ".par"))
         want, _, _ = oracle.run(par, 100, impl=impl)
     sim = lib.Sim(p)
     ctx = lib.Context(sim)
@@ -149,6 +155,10 @@ def test_circumbinary_full_size_100_steps_l1(impl):
     got = ctx.get_state(0)
     t, _ = ctx.time(0)
     ctx.close()
+    if exact:
+        for k in ("prim", "cons", "tiph", "dphi"):
+            assert np.array_equal(got[k], getattr(want, k)), (k, float(np.abs(got[k] - getattr(want, k)).max()))
+        assert t == want.t
     for q in (0, 2, 3, 1):
         assert l1_rel(got["cons"][:, q], want.cons[:, q]) <= 1e-10, (q, l1_rel(got["cons"][:, q], want.cons[:, q]))
     assert abs(t - want.t) <= 1e-12 * abs(want.t)

@@ -94,3 +94,26 @@ def test_case_tolerances_cover_last_ulp_sensitivity(name):
         l1 = max(l1_rel(st.cons[:, q], g["step100_cons"][:, q]) for q in (0, 1, 2, 3))
     assert 1e-12 < worst <= step_tol
     assert 1e-10 < l1 <= l1_tol
+
+
+@pytest.mark.parametrize("impl", IMPLS)
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_second_substep_phases_match_reference(impl, name):
+    """Phases 8-15: the whole first substep and gravMass_move, then the second
+    substep stopped after each phase."""
+    from conftest import golden_sub2
+    g = golden_sub2(name)
+    with tempfile.TemporaryDirectory() as td:
+        par = _par(g, td)
+        st5 = oracle.run(par, 5, impl=impl)[0]
+        for ph in range(8, 16):
+            st = oracle.stage(par, ph, impl=impl, load=st5)
+            full = {"prim": st.prim, "cons": st.cons, "tiph": st.tiph, "dphi": st.dphi, **st.ext}
+            for k in [k for k in g if k.startswith(f"stage{ph}_")]:
+                key = k.split("_", 1)[1]
+                if key in ("dt", "gm"):
+                    want = g[k]
+                    got = np.float64(st.dt) if key == "dt" else st.gm
+                    assert np.array_equal(got, want), (ph, key)
+                else:
+                    assert np.array_equal(full[key], g[k]), (ph, key)
