@@ -28,6 +28,17 @@ CASES = ("gresho16", "kepler24", "cbd32", "kepler24out", "cbd32out", "kepler12no
 # ones (tests/test_oracle.py checks both).
 CASE_TOL = {"sstest32": (1e-9, 1e-7)}
 
+# The second substep's phases start from the first substep's results, which
+# carry the last-ulp differences of the device transcendentals.  Its slope
+# arrays (grad, gradp) are limiter outputs: where a limiter branch sits at a
+# tie, such a difference flips it, so they are compared in L1-relative.
+# SUB2_SLOPE_L1 holds the cases whose branches flip (the one-ulp-noise oracle
+# moves their L1 by 0.26 and 0.18, tests/test_oracle.py), SUB2_STATE the
+# max-relative bar of the state arrays where it is not the 1e-12 of a phase.
+SUB2_SLOPE_L1 = {"raddom16": 1e-5, "middle16": 1e-3}
+SUB2_SLOPE_L1_DEFAULT = 1e-10
+SUB2_STATE = {"kepler1out": 1e-11}
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")

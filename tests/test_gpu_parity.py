@@ -17,7 +17,8 @@ unmodified reference sources by make_golden.py).  Bars:
 import numpy as np
 import pytest
 
-from conftest import CASE_TOL, CASES, golden, golden_sub2, l1_rel, max_rel
+from conftest import (CASE_TOL, CASES, SUB2_SLOPE_L1, SUB2_SLOPE_L1_DEFAULT, SUB2_STATE, golden, golden_sub2,
+                      l1_rel, max_rel)
 from disco2_b200 import lib
 
 pytestmark = pytest.mark.gpu
@@ -159,9 +160,15 @@ def test_second_substep_phases(name, phase):
     ext = ctx.stage_data(0)
     got = dict(st)
     got.update(ext)
+    tol = SUB2_STATE.get(name, STAGE_TOL)
     for k in STAGE_KEYS[phase]:
+        want = g2[f"stage{8 + phase}_{k}"]
         if k == "RKtiph":
             continue
-        compare(name, got[k], g2[f"stage{8 + phase}_{k}"], STAGE_TOL, k)
+        if k in ("grad", "gradp") and name not in EXACT:
+            bar = SUB2_SLOPE_L1.get(name, SUB2_SLOPE_L1_DEFAULT)
+            assert l1_rel(got[k].ravel(), want.ravel()) <= bar, (k, l1_rel(got[k].ravel(), want.ravel()))
+        else:
+            compare(name, got[k], want, tol, k)
     _, dt = ctx.time(0)
-    compare(name, np.array([dt]), np.array([g2[f"stage{8 + phase}_dt"]]), STAGE_TOL)
+    compare(name, np.array([dt]), np.array([g2[f"stage{8 + phase}_dt"]]), tol)
