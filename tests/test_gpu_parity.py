@@ -162,9 +162,9 @@ def test_second_substep_phases(name, phase):
     got.update(ext)
     tol = SUB2_STATE.get(name, STAGE_TOL)
     for k in STAGE_KEYS[phase]:
-        want = g2[f"stage{8 + phase}_{k}"]
         if k == "RKtiph":
             continue
+        want = g2[f"stage{8 + phase}_{k}"]
         if k in ("grad", "gradp") and name not in EXACT:
             bar = SUB2_SLOPE_L1.get(name, SUB2_SLOPE_L1_DEFAULT)
             assert l1_rel(got[k].ravel(), want.ravel()) <= bar, (k, l1_rel(got[k].ravel(), want.ravel()))
