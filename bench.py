@@ -340,7 +340,8 @@ def run_adjoint(args):
     """Cost of the gradient against the forward it differentiates: the
     circumbinary disk at 192 annuli, 500 RK2 steps, both objectives averaged
     over steps 251-500; forward = dgpu_objective (graph-replayed steps plus the
-    objective after each step), adjoint = dgpu_adjoint (forward sweep with a
+    objective after each step), plain = the same number of dgpu_step_rk2
+    steps with no objective, adjoint = dgpu_adjoint (forward sweep with a
     checkpoint every 25 steps, then each segment replayed and reversed),
     tangent = dgpu_tangent along q.  Wall time of the synchronous calls."""
     from disco2_b200 import configs, lib
@@ -353,8 +354,11 @@ def run_adjoint(args):
     ctx.adjoint(4, 2, ckpt_every=2)
     ctx.init_state(0)
     ctx.tangent(4, 2, dq=1.0)
+    ctx.init_state(0)
+    ctx.step(2)                  # the plain step's graph
     res = {}
     for name, fn in (("forward", lambda: ctx.objective(n, w0)),
+                     ("plain", lambda: ctx.step(n)),
                      ("adjoint", lambda: ctx.adjoint(n, w0, ckpt_every=K)),
                      ("tangent", lambda: ctx.tangent(n, w0, dq=1.0))):
         best = None
@@ -370,8 +374,10 @@ def run_adjoint(args):
     ctx.close()
     return {"workload": f"circumbinary disk, 192 annuli ({s.num_cells} cells), {n} steps, objectives "
                         f"averaged over steps {w0 + 1}-{n}, checkpoints every {K} steps",
-            "forward_s": res["forward"], "adjoint_s": res["adjoint"], "tangent_s": res["tangent"],
+            "forward_s": res["forward"], "plain_steps_s": res["plain"], "adjoint_s": res["adjoint"],
+            "tangent_s": res["tangent"],
             "adjoint_over_forward": res["adjoint"] / res["forward"],
+            "adjoint_over_plain_steps": res["adjoint"] / res["plain"],
             "tangent_over_forward": res["tangent"] / res["forward"],
             "how": "wall time of the synchronous library calls, best of 2, same initial state"}
 
