@@ -13,6 +13,15 @@ u ~ N(0, 1) per cell from numpy's default_rng(1000 + k)); relative steps
 
     python tests/golden/make_fd_reference.py [--jobs 8]
 writes tests/golden/cbd192_fd.json.
+
+    python tests/golden/make_fd_reference.py --short
+writes tests/golden/cbd192_fd_short.json: the same disk without its initial
+1e-4 noise (IC_Noise 0) over 20 steps, the objectives averaged over steps
+11-20, relative steps 1e-6, 1e-7 and 1e-8.  With the noise the phi slopes
+are noise-dominated and a perturbation of 1e-6 reorders the limiter's
+candidates in many cells, so no step converges; without it the base phi
+slopes are smooth.  The spread of the three steps measures how far the
+differences themselves have converged.
 """
 from __future__ import annotations
 
@@ -38,6 +47,7 @@ except ImportError:
 
 NUM_R, NSTEPS, WINDOW = 192, 500, 250
 Q0, ALPHA0 = 1.0, 0.1
+EXTRA = {}  # parameters over the circumbinary defaults (the converged case: IC_Noise 0)
 STEPS = (1e-6, 1e-8)
 N_DIRS = 16
 OUT = os.path.join(HERE, "cbd192_fd.json")
@@ -51,11 +61,15 @@ def direction(prim0: np.ndarray, k: int) -> np.ndarray:
     return d
 
 
+def _set_extra(extra: dict) -> None:
+    EXTRA.update(extra)
+
+
 def _objective(args) -> list[float]:
     """J = (torque, accretion) means over the window for one perturbed run."""
-    work, tag, q, alpha, prim_file, dtfile = args
+    work, tag, q, alpha, prim_file, dtfile, NSTEPS, WINDOW = args
     par = os.path.join(work, f"{tag}.par")
-    configs.write_parfile(configs.circumbinary(num_r=NUM_R, q=q, alpha=alpha), par)
+    configs.write_parfile(configs.circumbinary(num_r=NUM_R, q=q, alpha=alpha, **EXTRA), par)
     out = os.path.join(work, f"{tag}.txt")
     cmd = [oracle.REF_BIN, "objective", par, str(NSTEPS), out, "--load", prim_file]
     if dtfile:
@@ -69,11 +83,19 @@ def _objective(args) -> list[float]:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
+    ap.add_argument("--short", action="store_true")
     args = ap.parse_args()
+    if args.short:
+        NSTEPS, WINDOW, STEPS_ = 20, 10, (1e-6, 1e-7, 1e-8)
+        EXTRA.update({"IC_Noise": 0.0})
+        out_path = OUT.replace(".json", "_short.json")
+    else:
+        NSTEPS, WINDOW, STEPS_ = globals()["NSTEPS"], globals()["WINDOW"], STEPS
+        out_path = OUT
     oracle.build(ref=True, port=False)
     work = tempfile.mkdtemp(prefix="fdref_")
     par0 = os.path.join(work, "base.par")
-    configs.write_parfile(configs.circumbinary(num_r=NUM_R, q=Q0, alpha=ALPHA0), par0)
+    configs.write_parfile(configs.circumbinary(num_r=NUM_R, q=Q0, alpha=ALPHA0, **EXTRA), par0)
     init = oracle.run(par0, 0)[0]  # the reference's initial state
     base_state = os.path.join(work, "init.bin")
     oracle.write_state(base_state, init)
@@ -88,24 +110,24 @@ def main() -> None:
     J0 = [float(np.sum(w0 * a0[WINDOW:, 3]) / np.sum(w0)), float(np.sum(w0 * a0[WINDOW:, 4]) / np.sum(w0))]
 
     jobs, keys = [], []
-    for h in STEPS:
+    for h in STEPS_:
         for sgn in (+1, -1):
-            jobs.append((work, f"q_{h}_{sgn}", Q0 * (1 + sgn * h), ALPHA0, base_state, dtfile))
+            jobs.append((work, f"q_{h}_{sgn}", Q0 * (1 + sgn * h), ALPHA0, base_state, dtfile, NSTEPS, WINDOW))
             keys.append(("q", h, sgn))
-            jobs.append((work, f"a_{h}_{sgn}", Q0, ALPHA0 * (1 + sgn * h), base_state, dtfile))
+            jobs.append((work, f"a_{h}_{sgn}", Q0, ALPHA0 * (1 + sgn * h), base_state, dtfile, NSTEPS, WINDOW))
             keys.append(("alpha", h, sgn))
             for k in range(N_DIRS):
                 st = oracle.read_state(base_state)
                 st.prim = init.prim + sgn * h * direction(init.prim, k)
                 f = os.path.join(work, f"s{k}_{h}_{sgn}.bin")
                 oracle.write_state(f, st)
-                jobs.append((work, f"s{k}_{h}_{sgn}", Q0, ALPHA0, f, dtfile))
+                jobs.append((work, f"s{k}_{h}_{sgn}", Q0, ALPHA0, f, dtfile, NSTEPS, WINDOW))
                 keys.append((f"sigma{k}", h, sgn))
-    with mp.get_context("spawn").Pool(args.jobs) as pool:
+    with mp.get_context("spawn").Pool(args.jobs, initializer=_set_extra, initargs=(dict(EXTRA),)) as pool:
         res = pool.map(_objective, jobs)
     J = {key: np.array(r) for key, r in zip(keys, res)}
     fd = {}
-    for h in STEPS:
+    for h in STEPS_:
         d = {}
         d["q"] = ((J[("q", h, 1)] - J[("q", h, -1)]) / (2 * h * Q0)).tolist()
         d["alpha"] = ((J[("alpha", h, 1)] - J[("alpha", h, -1)]) / (2 * h * ALPHA0)).tolist()
@@ -113,13 +135,14 @@ def main() -> None:
                       for k in range(N_DIRS)]
         fd[f"{h:g}"] = d
     out = {"workload": f"circumbinary disk, {NUM_R} annuli, q={Q0}, alpha={ALPHA0}",
+           "params": dict(EXTRA),
            "num_r": NUM_R, "nsteps": NSTEPS, "window_start": WINDOW, "cells": int(init.N),
            "J": J0, "dt_sum_window": float(np.sum(w0)), "fd": fd,
            "direction": "d rho = rho0 u, d P = P0 u, u = numpy default_rng(1000 + k).standard_normal(N)",
            "generator": "tests/golden/make_fd_reference.py (reference objective mode, frozen dt)"}
-    with open(OUT, "w") as fh:
+    with open(out_path, "w") as fh:
         json.dump(out, fh, indent=1)
-    print("wrote", OUT, "J", J0)
+    print("wrote", out_path, "J", J0)
 
 
 if __name__ == "__main__":

@@ -215,6 +215,57 @@ def test_gradient_matches_reference_finite_differences():
     assert np.max(r8) < 1e-3, np.max(r8)
 
 
+def test_gradient_matches_converged_reference_differences():
+    """Where the reference's own central differences converge: the disk of
+    the gradient check without its 1e-4 initial noise, over 20 steps, the
+    objectives averaged over steps 11-20 (tests/golden/cbd192_fd_short.json,
+    relative steps 1e-6, 1e-7 and 1e-8 of the reference C code, frozen dt).
+    Each adjoint entry (q, alpha, 16 directions of Sigma_0; torque and
+    accretion rate) must agree with the reference's difference at step 1e-7
+    to 1e-6 relative, or, where the reference's differences at steps 1e-7
+    and 1e-8 disagree by more than that (limiter and Riemann-state branches
+    that flip within the step), to within twice their own spread."""
+    import json
+    import os
+    ref = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "cbd192_fd_short.json")))
+    s = lib.Sim(configs.circumbinary(num_r=ref["num_r"], **ref["params"]))
+    assert s.num_cells == ref["cells"]
+    grads = []
+    for w in ((1.0, 0.0), (0.0, 1.0)):
+        ctx = lib.Context(s)
+        ctx.init_state(0)
+        prim0 = ctx.get_state(0)["prim"]
+        grads.append(ctx.adjoint(ref["nsteps"], ref["window_start"], ckpt_every=5, weights=w))
+        ctx.close()
+    assert np.allclose([grads[0]["J"][0], grads[1]["J"][1]], ref["J"], rtol=1e-8, atol=0)
+    fd = ref["fd"]
+
+    def fdv(h, name, k):
+        return fd[h]["sigma"][int(name[5:])][k] if name.startswith("sigma") else fd[h][name][k]
+
+    rows = []
+    for k in range(2):
+        g = grads[k]
+        vals = [("q", g["dq"]), ("alpha", g["dalpha"])]
+        for d in range(len(fd["1e-07"]["sigma"])):
+            u = np.random.default_rng(1000 + d).standard_normal(prim0.shape[0])
+            dirv = np.zeros_like(prim0)
+            dirv[:, 0] = prim0[:, 0] * u
+            dirv[:, 1] = prim0[:, 1] * u
+            vals.append((f"sigma{d}", float(np.sum(g["dprim"] * dirv))))
+        for name, a in vals:
+            f7, f8 = fdv("1e-07", name, k), fdv("1e-08", name, k)
+            spread = abs(f7 - f8) / abs(f7)
+            rows.append((name, k, a, f7, abs(a - f7) / abs(f7), spread))
+    met = 0
+    for name, k, a, f7, r, spread in rows:
+        print(f"{name:8s} {'torque' if k == 0 else 'mdot':6s} adjoint={a:+.10e} reference_fd(1e-7)={f7:+.10e} "
+              f"rel={r:.2e} fd spread(1e-7,1e-8)={spread:.2e}")
+        met += r <= 1e-6
+        assert r <= max(1e-6, 2.0 * spread), (name, k, r, spread)
+    print(f"{met} of {len(rows)} entries within 1e-6 relative of the reference's differences")
+
+
 def test_autograd_wrapper_matches_adjoint(base):
     """The torch.autograd.Function of the check harness: backward of a scalar
     function of J is one dgpu_adjoint call with the incoming weights."""
