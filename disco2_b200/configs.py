@@ -183,6 +183,16 @@ def torus_2d(num_r: int = 80, **over) -> dict:
     return p
 
 
+def torus_3d(num_r: int = 80, num_z: int = 80, **over) -> dict:
+    """The reference's own 3-D parfile (parfiles/torus.par): a torus about a
+    point mass, 80 annuli x 80 layers, at most 20 cells per ring, two ghost
+    annuli and layers, outflow in r, periodic in z, HLLC, no viscosity."""
+    p = torus_2d(num_r=num_r, NumZ=num_z, ng=2, Z_Min=-1.0, Z_Max=1.0, NPCAP=20, BoundTypeZ=2,
+                 BoundTypeR=1, Grav_2D=0)
+    p.update(over)
+    return p
+
+
 def milos_macfadyen(num_r: int = 128, **over) -> dict:
     """Circumbinary disk of MacFadyen & Milosavljevic (MILOS_MACFADYEN): binary,
     Keplerian mesh, no inner boundary, outflow, an outer damping zone."""
@@ -238,6 +248,7 @@ WORKLOADS = {
     "sstest": sstest,
     "vortex": vortex_test,
     "torus": torus_2d,
+    "torus3d": torus_3d,
     "milos_macfadyen": milos_macfadyen,
     "rad_dom": rad_dom,
     "middle": middle,

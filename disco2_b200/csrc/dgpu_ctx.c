@@ -107,7 +107,7 @@ int dgpu_sim_param(const dgpu_sim *sim, const char *key, double *value) {
   P_D("ZLogScale", ZLogScale) P_D("HiResSigma", HiResSigma) P_D("HiResR0a", HiResR0a)
   P_D("HiResR0b", HiResR0b) P_D("HiResFac", HiResFac) P_I("w_analytic_type", w_analytic_type)
   P_D("IC_HoR", IC_HoR) P_D("IC_Noise", IC_Noise) P_I("IC_Seed", IC_Seed)
-  P_I("NR", NR) P_I("Ncells", Ncells)
+  P_I("NR", NR) P_I("NZ", NZ) P_I("Ncells", Ncells)
 #undef P_I
 #undef P_D
   return DGPU_ERR_ARG;
@@ -139,12 +139,35 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
     memset(&rd, 0, sizeof(rd));
     memset(state, 0, sizeof(state));
     initstate_r(666, state, sizeof(state), &rd);
-    for (i = 0; i < s->NR && rc == DGPU_OK; ++i)
-      for (j = 0; j < s->N_p[i]; ++j, ++idx)
-        if (dsim_grid_init(s, i, idx, t[idx], d[idx], g, &rd, prim + (size_t)s->NQ * idx) != 0) {
-          rc = fail(NULL, DGPU_ERR_UNSUPPORTED, "InitialDataType %d has no whole-grid initialiser here", s->InitialDataType);
-          break;
-        }
+    int k;
+    for (k = 0; k < s->NZ && rc == DGPU_OK; ++k)
+      for (i = 0; i < s->NR && rc == DGPU_OK; ++i)
+        for (j = 0; j < s->N_p[i]; ++j, ++idx)
+          if (dsim_grid_init(s, k, i, idx, t[idx], d[idx], g, &rd, prim + (size_t)s->NQ * idx) != 0) {
+            rc = fail(NULL, DGPU_ERR_UNSUPPORTED, "InitialDataType %d has no whole-grid initialiser here", s->InitialDataType);
+            break;
+          }
+  }
+  if (rc == DGPU_OK && s->NZ > 1) {
+    /* main.c:66-67,111-112: the single-rank cell_syncproc_z after cell_create
+     * and after the initial data copies tiph and prim (and RKcons, still 0)
+     * of layers NZ-2ng .. NZ-ng-1 into the ng lowest layers and of layers
+     * ng .. 2ng-1 into the ng highest (src/Cell/cell_sync.c:156-205) */
+    const long per = (long)s->Ncells / s->NZ;
+    const int ng = s->ng_min[1], shift = s->NZ - 2 * ng;
+    int k;
+    for (k = 0; k < s->NZ; ++k) {
+      int ks;
+      long c0;
+      if (k < ng) ks = k + shift;
+      else if (k >= s->NZ - ng) ks = k - shift;
+      else continue;
+      for (c0 = 0; c0 < per; ++c0) {
+        const long dst = (long)k * per + c0, src = (long)ks * per + c0;
+        t[dst] = t[src];
+        if (prim) memcpy(prim + (size_t)s->NQ * dst, prim + (size_t)s->NQ * src, sizeof(double) * (size_t)s->NQ);
+      }
+    }
   }
   if (t != tiph) free(t);
   if (d != dphi) free(d);
@@ -155,7 +178,18 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
 
 static int check_supported(const struct dgpu_sim *s, int k, char *err, int n) {
   int i;
-  if (s->NumZ != 1) return snprintf(err, (size_t)n, "disk %d: NumZ > 1 (3-D z faces) is not implemented", k), DGPU_ERR_UNSUPPORTED;
+  if (s->NumZ != 1) {
+    /* 3-D: z faces, z slopes and fluxes, and the single-rank periodic z copy
+     * (cell_syncproc_z) */
+    if (s->BoundTypeZ != DB_PERIODIC)
+      return snprintf(err, (size_t)n, "disk %d: NumZ > 1 needs BoundTypeZ 2 (periodic): on one rank the reference's z copy is periodic whatever the boundary type", k), DGPU_ERR_UNSUPPORTED;
+    if (s->InitialDataType != DI_TORUS)
+      return snprintf(err, (size_t)n, "disk %d: NumZ > 1 is implemented for the torus initial data (InitialDataType 3)", k), DGPU_ERR_UNSUPPORTED;
+    if (s->NUM_N > 0)
+      return snprintf(err, (size_t)n, "disk %d: passive scalars with NumZ > 1 are not implemented", k), DGPU_ERR_UNSUPPORTED;
+    if (s->NumZ < s->ng)
+      return snprintf(err, (size_t)n, "disk %d: the periodic z copy needs NumZ >= ng", k), DGPU_ERR_UNSUPPORTED;
+  }
   if (s->NUM_C != 5 || s->NUM_N < 0 || s->NUM_N > DGPU_MAX_PASSIVE)
     return snprintf(err, (size_t)n, "disk %d: only NUM_C = 5 with NUM_N <= %d is implemented", k, DGPU_MAX_PASSIVE), DGPU_ERR_UNSUPPORTED;
   if (s->NUM_N > 0 && s->DAMP_TIME > 0.0)
@@ -203,7 +237,9 @@ void dgpu_destroy(dgpu_ctx *c) {
                   c->d.dphi, c->d.w_ann, c->d.fphi, c->d.frf, c->d.fS, c->d.fdp, c->d.ann_c, c->d.src, c->d.rr, c->d.fstart, c->d.fL, c->d.fR, c->d.fdphi,
                   c->d.fcm, c->d.pair_nf, c->d.pair_jpmin, c->d.pair_T, c->d.pair_seq, c->d.runs,
                   c->d.mdot_part, c->d.counters, c->d.err, c->d.obuf, c->d_stage, c->d_torque,
-                  c->d.cfl_ann, c->d.sweep_flag};
+                  c->d.cfl_ann, c->d.sweep_flag, c->d_zslot_ann, c->d.zfL, c->d.zfR, c->d.zfdphi, c->d.zfcm,
+                  c->d.zfstart, c->d.zrr, c->d.zruns, c->d.zpair_nf, c->d.zpair_jpmin, c->d.zpair_T,
+                  c->d.zpair_seq, c->d.zfS, c->d.zfdp, c->d.zfrf, c->d.gradz};
     for (k = 0; k < (int)(sizeof(ps) / sizeof(ps[0])); ++k)
       if (ps[k]) cudaFree(ps[k]);
   }
@@ -222,9 +258,10 @@ void dgpu_destroy(dgpu_ctx *c) {
 
 int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dgpu_ctx **out) {
   struct dgpu_ctx *c;
-  int k, i, rc, ok = 1;
-  int ann = 0, cells = 0, slots = 0, runs = 0, maxcells = 0, n_ob = 0, n_pass = 0;
-  int *h_cell_ann, *h_slot_ann;
+  int k, i, kz, rc, ok = 1;
+  int ann = 0, cells = 0, slots = 0, runs = 0, zslots = 0, zruns = 0, maxcells = 0, n_ob = 0, n_pass = 0;
+  int has_z = 0;
+  int *h_cell_ann, *h_slot_ann, *h_zslot_ann;
   if (!sims || n < 1 || !out) return fail(NULL, DGPU_ERR_ARG, "bad arguments to dgpu_create");
   for (k = 0; k < n; ++k) {
     if (!sims[k]) return fail(NULL, DGPU_ERR_ARG, "sim %d is null", k);
@@ -243,8 +280,9 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
       dgpu_destroy(c);
       return fail(NULL, DGPU_ERR_NOMEM, "out of host memory");
     }
-    ann += sims[k]->NR;
+    ann += sims[k]->NR * sims[k]->NZ;
     cells += sims[k]->Ncells;
+    if (sims[k]->NZ > 1) has_z = 1;
     if (sims[k]->NUM_N > n_pass) n_pass = sims[k]->NUM_N;
     if (sims[k]->Ncells > maxcells) maxcells = sims[k]->Ncells;
   }
@@ -261,50 +299,69 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     dsim_fill_params(s, p);
     p->ann_base = ann;
     p->cell_base = cells;
-    for (i = 0; i < s->NR; ++i) {
-      Annulus *a = &c->h_ann[ann + i];
-      int j;
-      dsim_fill_annulus(s, i, a);
-      a->inst = k;
-      a->cell_off = cells;
-      /* the outflow boundary reads annuli 1 and NR-3 and writes 0, NR-2 and NR-1 */
-      if (s->BoundTypeR == DB_OUTFLOW && (i >= s->NR - 3 || (s->NoInnerBC != 1 && i <= 1))) {
-        a->ob_off = n_ob;
-        n_ob += s->N_p[i];
-      } else {
-        a->ob_off = -1;
-      }
-      for (j = 0; j < s->N_p[i]; ++j) h_cell_ann[cells + j] = ann + i;
-      cells += s->N_p[i];
-      if (i < s->NR - 1) {
+    /* rings k-major, in the reference's (k, i, j) cell order */
+    for (kz = 0; kz < s->NZ; ++kz) {
+      for (i = 0; i < s->NR; ++i) {
+        Annulus *a = &c->h_ann[ann + kz * s->NR + i];
+        int j;
+        dsim_fill_annulus(s, kz, i, a);
+        a->inst = k;
+        a->cell_off = cells;
+        /* the outflow boundary reads annuli 1 and NR-3 and writes 0, NR-2 and NR-1 */
+        if (s->BoundTypeR == DB_OUTFLOW && (i >= s->NR - 3 || (s->NoInnerBC != 1 && i <= 1))) {
+          a->ob_off = n_ob;
+          n_ob += s->N_p[i];
+        } else {
+          a->ob_off = -1;
+        }
+        for (j = 0; j < s->N_p[i]; ++j) h_cell_ann[cells + j] = ann + kz * s->NR + i;
+        cells += s->N_p[i];
         a->face_base = slots;
-        a->face_cap = s->N_p[i] + s->N_p[i + 1] + DGPU_FACE_SLACK;
-        slots += a->face_cap;
         a->run_base = runs;
-        a->run_cap = s->N_p[i + 1] + DGPU_RUN_SLACK;
-        runs += a->run_cap;
-      } else {
-        a->face_base = slots;
-        a->face_cap = 0;
-        a->run_base = runs;
-        a->run_cap = 0;
+        a->face_cap = a->run_cap = 0;
+        if (i < s->NR - 1) {
+          a->face_cap = s->N_p[i] + s->N_p[i + 1] + DGPU_FACE_SLACK;
+          slots += a->face_cap;
+          a->run_cap = s->N_p[i + 1] + DGPU_RUN_SLACK;
+          runs += a->run_cap;
+        }
+        /* z pair (k, k+1) of annulus i: both rings hold N_p[i] cells */
+        a->zface_base = zslots;
+        a->zrun_base = zruns;
+        a->zface_cap = a->zrun_cap = 0;
+        if (s->NZ > 1 && kz < s->NZ - 1) {
+          a->zface_cap = 2 * s->N_p[i] + DGPU_FACE_SLACK;
+          zslots += a->zface_cap;
+          a->zrun_cap = s->N_p[i] + DGPU_RUN_SLACK;
+          zruns += a->zrun_cap;
+        }
       }
     }
-    ann += s->NR;
+    ann += s->NR * s->NZ;
   }
   c->n_slots = slots;
   c->n_runs = runs;
   c->n_ob = n_ob;
   h_slot_ann = (int *)malloc(sizeof(int) * (size_t)(slots > 0 ? slots : 1));
+  h_zslot_ann = (int *)malloc(sizeof(int) * (size_t)(zslots > 0 ? zslots : 1));
+  h_zslot_ann[0] = -1;
   for (i = 0; i < c->n_ann; ++i) {
     int f;
     for (f = 0; f < c->h_ann[i].face_cap; ++f) h_slot_ann[c->h_ann[i].face_base + f] = i;
+    for (f = 0; f < c->h_ann[i].zface_cap; ++f) h_zslot_ann[c->h_ann[i].zface_base + f] = i;
   }
+  c->d.n_zslots = zslots;
+  c->d.n_zruns = zruns;
+  c->d.has_z = has_z;
+  c->d.max_nz = 1;
+  for (k = 0; k < n; ++k)
+    if (c->sims[k]->NZ > c->d.max_nz) c->d.max_nz = c->sims[k]->NZ;
   c->n_upd_blocks = dgk_update_blocks(c->n_cells);
 
   if (cudaSetDevice(device) != cudaSuccess) {
     free(h_cell_ann);
     free(h_slot_ann);
+    free(h_zslot_ann);
     dgpu_destroy(c);
     return fail(NULL, DGPU_ERR_CUDA, "cudaSetDevice(%d) failed", device);
   }
@@ -314,6 +371,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
       free(h_cell_ann);
       free(h_slot_ann);
+      free(h_zslot_ann);
       dgpu_destroy(c);
       return fail(NULL, DGPU_ERR_CUDA, "cudaStreamCreate failed");
     }
@@ -326,6 +384,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     if (bad) {
       free(h_cell_ann);
       free(h_slot_ann);
+      free(h_zslot_ann);
       dgpu_destroy(c);
       return fail(NULL, DGPU_ERR_CUDA, "stream/event creation failed");
     }
@@ -371,6 +430,25 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     c->d.counters = (unsigned int *)dmalloc(sizeof(unsigned int) * 8, &ok);
     c->d.cfl_ann = (unsigned long long *)dmalloc(sizeof(unsigned long long) * A, &ok);
     c->d.sweep_flag = (int *)dmalloc(sizeof(int) * A, &ok);
+    if (has_z) {
+      const size_t ZS = (size_t)(zslots > 0 ? zslots : 1);
+      c->d_zslot_ann = (int *)dmalloc(sizeof(int) * ZS, &ok);
+      c->d.zfL = (int *)dmalloc(sizeof(int) * ZS, &ok);
+      c->d.zfR = (int *)dmalloc(sizeof(int) * ZS, &ok);
+      c->d.zfdphi = (double *)dmalloc(sizeof(double) * ZS, &ok);
+      c->d.zfcm = (double *)dmalloc(sizeof(double) * ZS, &ok);
+      c->d.zfstart = (int *)dmalloc(sizeof(int) * N, &ok);
+      c->d.zrr = (int *)dmalloc(sizeof(int) * 4 * N, &ok);
+      c->d.zruns = (int *)dmalloc(sizeof(int) * (size_t)(zruns > 0 ? zruns : 1), &ok);
+      c->d.zpair_nf = (int *)dmalloc(sizeof(int) * A, &ok);
+      c->d.zpair_jpmin = (int *)dmalloc(sizeof(int) * A, &ok);
+      c->d.zpair_T = (int *)dmalloc(sizeof(int) * A, &ok);
+      c->d.zpair_seq = (int *)dmalloc(sizeof(int) * A, &ok);
+      c->d.zfS = (double *)dmalloc(sizeof(double) * 5 * ZS, &ok);
+      c->d.zfdp = (double *)dmalloc(sizeof(double) * 2 * ZS, &ok);
+      c->d.zfrf = (double *)dmalloc(sizeof(double) * 5 * ZS, &ok);
+      c->d.gradz = (double *)dmalloc(sizeof(double) * 5 * N, &ok);
+    }
     c->d.err = (int *)dmalloc(sizeof(int), &ok);
     if (n_ob > 0) c->d.obuf = (double *)dmalloc(sizeof(double) * NQ * (size_t)n_ob, &ok);
     c->d_stage = (double *)dmalloc(sizeof(double) * NQ * (size_t)maxcells, &ok);
@@ -379,6 +457,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   if (!ok) {
     free(h_cell_ann);
     free(h_slot_ann);
+    free(h_zslot_ann);
     dgpu_destroy(c);
     return fail(NULL, DGPU_ERR_NOMEM, "device allocation failed");
   }
@@ -390,7 +469,10 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
       const Annulus *A = &c->h_ann[a];
       int m = 2 * (int)sizeof(double) * (A->np + (A->face_cap > 0 ? c->h_ann[a + 1].np : 0)) +
               (int)sizeof(int) * A->run_cap;
+      /* a z pair stages two rings of N_p cells and the upper ring's runs */
+      int mz = A->zface_cap > 0 ? 2 * (int)sizeof(double) * 2 * A->np + (int)sizeof(int) * A->zrun_cap : 0;
       if (m > mx) mx = m;
+      if (mz > mx) mx = mz;
     }
     c->d.smem_face = mx <= 48 * 1024 ? mx : 0;
   }
@@ -398,7 +480,7 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
    * scalars, outflow radial boundary or sink; it is opt-in (dgpu_set_fused):
    * on B200 the eight-kernel graph is faster (0.375 against 0.55 ms per step
    * on the 258k-cell circumbinary disk) */
-  c->fused_ok = c->n_pass == 0 && c->n_ob == 0;
+  c->fused_ok = c->n_pass == 0 && c->n_ob == 0 && !has_z;
   for (k = 0; k < n; ++k)
     if (c->h_par[k].rho_sink_on == 1) c->fused_ok = 0;
   c->fused = 0;
@@ -414,18 +496,23 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   c->d.ann = c->d_ann;
   c->d.cell_ann = c->d_cell_ann;
   c->d.slot_ann = c->d_slot_ann;
+  c->d.zslot_ann = c->d_zslot_ann;
   if (cudaMemcpy(c->d_par, c->h_par, sizeof(DiskParams) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_ann, c->h_ann, sizeof(Annulus) * (size_t)c->n_ann, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_cell_ann, h_cell_ann, sizeof(int) * (size_t)c->n_cells, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_slot_ann, h_slot_ann, sizeof(int) * (size_t)(c->n_slots ? c->n_slots : 1),
-                 cudaMemcpyHostToDevice) != cudaSuccess) {
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      (has_z && cudaMemcpy(c->d_zslot_ann, h_zslot_ann, sizeof(int) * (size_t)(zslots ? zslots : 1),
+                           cudaMemcpyHostToDevice) != cudaSuccess)) {
     free(h_cell_ann);
     free(h_slot_ann);
+    free(h_zslot_ann);
     dgpu_destroy(c);
     return fail(NULL, DGPU_ERR_CUDA, "table upload failed");
   }
   free(h_cell_ann);
   free(h_slot_ann);
+  free(h_zslot_ann);
   *out = c;
   return DGPU_OK;
 }
@@ -681,8 +768,36 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double
   return DGPU_OK;
 }
 
+/* One substep of a context holding a 3-D disk, on the context's stream: the
+ * z faces join after the r fluxes (timestep_routines.c:63-71), the viscous
+ * source reads the z slopes, and the periodic z copy closes the substep. */
+static int launch_substep_3d(struct dgpu_ctx *c, int sub) {
+  CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
+  CKK(dgk_merge(&c->d, sub, c->stream));
+  CKK(dgk_zmerge(&c->d, sub, c->stream));
+  CKK(dgk_rslope(&c->d, NULL, c->stream));
+  CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
+  CKK(dgk_flux_phi(&c->d, NULL, sub, c->stream));
+  CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
+  CKK(dgk_zslope(&c->d, c->stream));
+  CKK(dgk_plm_z(&c->d, c->stream));
+  CKK(dgk_flux_z(&c->d, sub, c->stream));
+  CKK(dgk_source(&c->d, NULL, sub, c->stream));
+  CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
+  if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
+  CKK(dgk_zsync(&c->d, sub, c->stream));
+  return DGPU_OK;
+}
+
 int dctx_launch_step(struct dgpu_ctx *c) {
   int sub;
+  if (c->d.has_z) {
+    for (sub = 1; sub <= 2; ++sub) {
+      int rc = launch_substep_3d(c, sub);
+      if (rc) return rc;
+    }
+    return DGPU_OK;
+  }
   if (c->fused) {
     /* per substep: k_prep (face list, phi slopes, CFL minima), then k_sweep */
     for (sub = 1; sub <= 2; ++sub) {
@@ -789,10 +904,16 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
       CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_merge(&c->d, sub, c->stream));
+      CKK(dgk_zmerge(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_rslope(&c->d, NULL, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
+      /* 3-D: the z faces, whose slopes the viscous source reads, in the
+       * plm_r slot (no-ops for 2-D disks) */
+      CKK(dgk_zslope(&c->d, c->stream));
+      CKK(dgk_plm_z(&c->d, c->stream));
+      CKK(dgk_flux_z(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_source(&c->d, NULL, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
@@ -802,6 +923,7 @@ int dgpu_step_rk2_timed(dgpu_ctx *c, int nsteps, double *kernel_ms) {
       CK(cudaEventRecord(ev[e++], c->stream));
       CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
       if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
+      CKK(dgk_zsync(&c->d, sub, c->stream));
       CK(cudaEventRecord(ev[e++], c->stream));
     }
     CK(cudaEventSynchronize(ev[DGPU_STEP_KERNELS]));
@@ -898,6 +1020,7 @@ int dgpu_autotune(dgpu_ctx *c, int steps, int *choice) {
 int dgpu_stage(dgpu_ctx *c, int phase) {
   int sub = phase >= 8 ? 2 : 1, stop = phase & 7;
   if (!c || phase < 0 || phase > 15) return DGPU_ERR_ARG;
+  if (c->d.has_z) return fail(c, DGPU_ERR_UNSUPPORTED, "stage parity of 3-D disks (NumZ > 1) is not implemented");
   cudaSetDevice(c->device);
   /* phases 8-15: the whole first substep (its k_update also moves the
    * GravMass, as timestep_rk2 does between the substeps), then the second */
@@ -925,64 +1048,93 @@ int dgpu_stage(dgpu_ctx *c, int phase) {
   return dgpu_synchronize(c);
 }
 
-int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, double *r, double *dphi,
-                   double *dA, double *deltaL, double *deltaR, double *cm, int *nf_out) {
+/* The r faces (z = 0) or the z faces (z = 1) of one disk in the reference's
+ * face-list order: face_create lists the r faces annulus pair by annulus
+ * pair, the layers inside each, and the z faces layer pair by layer pair, the
+ * annuli inside each (src/Face/face_create_destroy.c:130-193).  off[] gets
+ * the first face of each pair (timestep_n's nri / nzk). */
+static int face_list_dir(dgpu_ctx *c, int inst, int z, int cap, int *off, int *L, int *R, double *r,
+                         double *dphi, double *dA, double *deltaL, double *deltaR, double *cm, int *nf_out) {
   const struct dgpu_sim *s;
   const DiskParams *p;
-  int i, total = 0, rc = check_inst(c, inst);
+  int i, k, total = 0, rc = check_inst(c, inst), nrings, nslots;
   int *nf, *fL, *fR;
   double *fd, *fc;
   if (rc) return rc;
   s = c->sims[inst];
   p = &c->h_par[inst];
-  /* build the list of the current state: one k_merge pass (substep-1 buffers) */
-  CKK(dgk_merge(&c->d, 1, c->stream));
+  if (z && s->NZ == 1) return fail(c, DGPU_ERR_ARG, "a 2-D disk has no z faces");
+  nrings = s->NR * s->NZ;
+  nslots = z ? c->d.n_zslots : c->n_slots;
+  /* build the list of the current state: one merge pass (substep-1 buffers) */
+  if (z) CKK(dgk_zmerge(&c->d, 1, c->stream));
+  else CKK(dgk_merge(&c->d, 1, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
-  nf = (int *)malloc(sizeof(int) * (size_t)s->NR);
-  fL = (int *)malloc(sizeof(int) * (size_t)c->n_slots);
-  fR = (int *)malloc(sizeof(int) * (size_t)c->n_slots);
-  fd = (double *)malloc(sizeof(double) * (size_t)c->n_slots);
-  fc = (double *)malloc(sizeof(double) * (size_t)c->n_slots);
+  nf = (int *)malloc(sizeof(int) * (size_t)nrings);
+  fL = (int *)malloc(sizeof(int) * (size_t)(nslots > 0 ? nslots : 1));
+  fR = (int *)malloc(sizeof(int) * (size_t)(nslots > 0 ? nslots : 1));
+  fd = (double *)malloc(sizeof(double) * (size_t)(nslots > 0 ? nslots : 1));
+  fc = (double *)malloc(sizeof(double) * (size_t)(nslots > 0 ? nslots : 1));
   if (!nf || !fL || !fR || !fd || !fc) {
     free(nf); free(fL); free(fR); free(fd); free(fc);
     return fail(c, DGPU_ERR_NOMEM, "out of host memory");
   }
-  if (cudaMemcpy(nf, c->d.pair_nf + p->ann_base, sizeof(int) * (size_t)s->NR, cudaMemcpyDeviceToHost) ||
-      cudaMemcpy(fL, c->d.fL, sizeof(int) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
-      cudaMemcpy(fR, c->d.fR, sizeof(int) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
-      cudaMemcpy(fd, c->d.fdphi, sizeof(double) * (size_t)c->n_slots, cudaMemcpyDeviceToHost) ||
-      cudaMemcpy(fc, c->d.fcm, sizeof(double) * (size_t)c->n_slots, cudaMemcpyDeviceToHost)) {
+  if (cudaMemcpy(nf, (z ? c->d.zpair_nf : c->d.pair_nf) + p->ann_base, sizeof(int) * (size_t)nrings,
+                 cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fL, z ? c->d.zfL : c->d.fL, sizeof(int) * (size_t)nslots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fR, z ? c->d.zfR : c->d.fR, sizeof(int) * (size_t)nslots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fd, z ? c->d.zfdphi : c->d.fdphi, sizeof(double) * (size_t)nslots, cudaMemcpyDeviceToHost) ||
+      cudaMemcpy(fc, z ? c->d.zfcm : c->d.fcm, sizeof(double) * (size_t)nslots, cudaMemcpyDeviceToHost)) {
     free(nf); free(fL); free(fR); free(fd); free(fc);
     return fail(c, DGPU_ERR_CUDA, "face download failed");
   }
-  for (i = 0; i < s->NR - 1; ++i) total += nf[i];
+  /* pairs: r -- ring (k, i) with i < NR-1; z -- ring (k, i) with k < NZ-1 */
+  for (k = 0; k < s->NZ; ++k)
+    for (i = 0; i < s->NR; ++i)
+      if (z ? k < s->NZ - 1 : i < s->NR - 1) total += nf[k * s->NR + i];
   if (nf_out) *nf_out = total;
   if (total > cap) {
     free(nf); free(fL); free(fR); free(fd); free(fc);
     return fail(c, DGPU_ERR_ARG, "face list has %d faces, capacity %d", total, cap);
   }
   {
-    int n = 0;
-    for (i = 0; i < s->NR - 1; ++i) {
-      const Annulus *A = &c->h_ann[p->ann_base + i];
-      int f;
-      if (nri) nri[i] = n;
-      for (f = 0; f < nf[i]; ++f, ++n) {
-        int slot = A->face_base + f;
-        if (L) L[n] = fL[slot] - p->cell_base;
-        if (R) R[n] = fR[slot] - p->cell_base;
-        if (r) r[n] = A->f_r;
-        if (dphi) dphi[n] = fd[slot];
-        if (dA) dA[n] = A->f_r * fd[slot] * A->f_dperp;
-        if (deltaL) deltaL[n] = A->f_dl;
-        if (deltaR) deltaR[n] = A->f_dr;
-        if (cm) cm[n] = fc[slot];
+    const int nouter = z ? s->NZ - 1 : s->NR - 1, ninner = z ? s->NR : s->NZ;
+    int o, n = 0;
+    for (o = 0; o < nouter; ++o) {
+      if (off) off[o] = n;
+      for (i = 0; i < ninner; ++i) {
+        const int ring = z ? o * s->NR + i : i * s->NR + o;
+        const Annulus *A = &c->h_ann[p->ann_base + ring];
+        const int base = z ? A->zface_base : A->face_base;
+        const double fr = z ? A->zf_r : A->f_r, fperp = z ? A->zf_dperp : A->f_dperp;
+        int f;
+        for (f = 0; f < nf[ring]; ++f, ++n) {
+          const int slot = base + f;
+          if (L) L[n] = fL[slot] - p->cell_base;
+          if (R) R[n] = fR[slot] - p->cell_base;
+          if (r) r[n] = fr;
+          if (dphi) dphi[n] = fd[slot];
+          if (dA) dA[n] = fr * fd[slot] * fperp;
+          if (deltaL) deltaL[n] = z ? A->zf_dl : A->f_dl;
+          if (deltaR) deltaR[n] = z ? A->zf_dr : A->f_dr;
+          if (cm) cm[n] = fc[slot];
+        }
       }
     }
-    if (nri) nri[s->NR - 1] = n;
+    if (off) off[nouter] = n;
   }
   free(nf); free(fL); free(fR); free(fd); free(fc);
   return DGPU_OK;
+}
+
+int dgpu_face_list(dgpu_ctx *c, int inst, int cap, int *nri, int *L, int *R, double *r, double *dphi,
+                   double *dA, double *deltaL, double *deltaR, double *cm, int *nf_out) {
+  return face_list_dir(c, inst, 0, cap, nri, L, R, r, dphi, dA, deltaL, deltaR, cm, nf_out);
+}
+
+int dgpu_face_list_z(dgpu_ctx *c, int inst, int cap, int *nzk, int *L, int *R, double *r, double *dphi,
+                     double *dA, double *deltaL, double *deltaR, double *cm, int *nf_out) {
+  return face_list_dir(c, inst, 1, cap, nzk, L, R, r, dphi, dA, deltaL, deltaR, cm, nf_out);
 }
 
 int dgpu_diagnostics(dgpu_ctx *c, int inst, double *vector, double *scalar, double *equat, double *extra) {
@@ -992,6 +1144,7 @@ int dgpu_diagnostics(dgpu_ctx *c, int inst, double *vector, double *scalar, doub
   size_t need, nr;
   double *rows, *dv, *ds, *de, *dx;
   if (rc) return rc;
+  if (c->h_par[inst].NZ > 1) return fail(c, DGPU_ERR_UNSUPPORTED, "diagnostics of a 3-D disk (NumZ > 1) are not implemented");
   s = c->sims[inst];
   p = &c->h_par[inst];
   dgk_diag_sizes(&nvec, &neq, &nextra, &nrow);
@@ -1030,6 +1183,7 @@ int dgpu_torque(dgpu_ctx *c, int inst, double *torque) {
   if (rc) return rc;
   if (!torque) return fail(c, DGPU_ERR_ARG, "null torque");
   p = &c->h_par[inst];
+  if (p->NZ > 1) return fail(c, DGPU_ERR_UNSUPPORTED, "the torque of a 3-D disk (NumZ > 1) is not implemented");
   nb = (p->n_cells + dgk_block_size() - 1) / dgk_block_size();
   CKK(dgk_torque(&c->d, inst, c->d_torque, c->d_torque + nb, p->n_cells, c->stream));
   CK(cudaMemcpyAsync(torque, c->d_torque + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -30,7 +30,7 @@ struct dgpu_ctx {
   DiskParams *d_par;
   InstState *d_ist;
   Annulus *d_ann;
-  int *d_cell_ann, *d_slot_ann;
+  int *d_cell_ann, *d_slot_ann, *d_zslot_ann;
   double *d_stage;    /* AoS staging buffer: max cells of a disk x NQ */
   double *d_torque;   /* partial sums + result */
   cudaGraphExec_t graph;

@@ -298,7 +298,7 @@ HD T fgrav(const T &M, const T &r, double eps, int n) {
 // ---------------------------------------------------------------------------
 // Riemann solver: riemann_set_vel / _set_state / _set_flux / _set_star_hll /
 // _set_star_hllc and the flux choice of riemann_AddFlux
-// (src/Riemann/Riemann_routines.c:14-191,314-371).  dir 0 = r face, 1 = phi.
+// (src/Riemann/Riemann_routines.c:14-191,314-371).  dir 0 = r face, 1 = phi, 2 = z.
 // ---------------------------------------------------------------------------
 template <typename T>
 HD void phys_flux(const T *p, double r, double n0, double n1, double n2, double gam, T *F) {
@@ -342,7 +342,7 @@ template <typename T>
 // differentiated runs carry no passive scalar (np = 0).
 HD void riemann_flux(const T *pL, const T *pR, double r, int dir, double w, double gam, int solver, T *F,
                      int np = 0, const double *qL = nullptr, const double *qR = nullptr, double *Fq = nullptr) {
-  const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = 0.0;
+  const double n0 = dir == 0 ? 1.0 : 0.0, n1 = dir == 1 ? 1.0 : 0.0, n2 = dir == 2 ? 1.0 : 0.0;
   T vnL, cf2L, vnR, cf2R;
   {
     T P = pL[D_PPP], rho = pL[D_RHO], vr = pL[D_URR], vp = r * pL[D_UPP], vz = pL[D_UZZ];
@@ -744,6 +744,39 @@ __device__ __forceinline__ void for_cell_rface_ranges(const DevPtrs &d, const An
     int n1 = (j + 1 < A.np) ? rd(d.fstart + g + 1) : nf;
     if (nf <= 0) n1 = n0;
     f(A.face_base + n0, A.face_base + n1, 0);
+  }
+}
+
+// The z faces of cell g of ring a (3-D disks) in the reference's face order
+// (face_create with direction 1 lists them layer pair after layer pair):
+// those of the z pair (a-NR, a), where g is the upper cell, then those of
+// (a, a+NR), where it is the lower cell, as contiguous slot ranges:
+// f(first slot, end slot, side), side 1 for the upper cell, 0 for the lower.
+template <typename Fn>
+__device__ __forceinline__ void for_cell_zface_ranges(const DevPtrs &d, const Annulus &A, int a, int g, int NR,
+                                                      int NZ, Fn f) {
+  const int j = g - A.cell_off;
+  if (A.k > 0) {
+    const Annulus &Q = d.ann[a - NR];
+    const int4 rr = rd(reinterpret_cast<const int4 *>(d.zrr) + g);
+    if (rr.z != INT_MIN) {
+      f(Q.zface_base + rr.x, Q.zface_base + rr.y, 1);
+      f(Q.zface_base + rr.z, Q.zface_base + rr.w, 1);
+    } else {
+      const int T = rd(d.zpair_T + a - NR);
+      const int jpmin = rd(d.zpair_jpmin + a - NR);
+      int dd = j - jpmin;
+      if (dd < 0) dd += A.np;
+      const int *runs = d.zruns + Q.zrun_base;
+      for (int s = dd; s <= T; s += A.np) f(Q.zface_base + rd(runs + s), Q.zface_base + rd(runs + s + 1), 1);
+    }
+  }
+  if (A.k < NZ - 1) {
+    const int nf = rd(d.zpair_nf + a);
+    int n0 = rd(d.zfstart + g);
+    int n1 = (j + 1 < A.np) ? rd(d.zfstart + g + 1) : nf;
+    if (nf <= 0) n1 = n0;
+    f(A.zface_base + n0, A.zface_base + n1, 0);
   }
 }
 

@@ -147,6 +147,7 @@ static int diff_check(struct dgpu_ctx *c) {
   if (P->cooling) return fail(c, DGPU_ERR_UNSUPPORTED, "differentiation with Cooling is not implemented");
   if (P->rho_sink_on) return fail(c, DGPU_ERR_UNSUPPORTED, "differentiation with RhoSinkOn is not implemented");
   if (P->outflow) return fail(c, DGPU_ERR_UNSUPPORTED, "differentiation with the outflow radial boundary is not implemented");
+  if (P->NZ > 1) return fail(c, DGPU_ERR_UNSUPPORTED, "differentiation of a 3-D disk (NumZ > 1) is not implemented");
   if (P->num_n) return fail(c, DGPU_ERR_UNSUPPORTED, "differentiation with passive scalars is not implemented");
   return DGPU_OK;
 }

@@ -70,16 +70,22 @@ typedef struct {
   int num_sinks;    /* GravMassType (cell_source.c:177) */
   int outflow;      /* bit 0: outflow radial boundary; bit 1: also the inner annulus (NoInnerBC != 1) */
   int num_n;        /* passive scalars (NUM_N): planes 5.. of prim, cons, rkcons, grad, gradp */
+  int NZ;           /* layers incl. ghosts, sim_N(Z_DIR); a disk's rings (k, i) are numbered k * NR + i */
+  int ngz;          /* ghost layers at each z end (0 for NumZ = 1) */
   double gamma, plm, cfl, visc, g_eps;
   double rho_floor, cs_floor, cs_cap, vel_cap;
   double t_max, poro_r1, orb_tscale, orb_t0;
-  double dz, z;     /* z-extent and centre of the single z layer */
+  double dz, z;     /* z-extent and centre of layer 0 (the single layer of a 2-D disk) */
 } DiskParams;
 
-/* Per-annulus constants (host-computed with the host libm, like the reference). */
+/* Per-ring constants (host-computed with the host libm, like the reference).
+ * A ring is annulus i of layer k; a 2-D disk has one layer, so its rings are
+ * its annuli.  The rings of a disk are numbered k * NR + i, so the r-face pair
+ * of ring a is (a, a+1) and its z-face pair (a, a+NR). */
 typedef struct {
   int inst;         /* owning disk */
   int i;            /* annulus index within the disk */
+  int k;            /* layer index within the disk */
   int np;           /* N_p */
   int cell_off;     /* global cell index of j = 0 */
   int kind;         /* DGPU_AK_* bits */
@@ -100,6 +106,12 @@ typedef struct {
   /* pair (i, i+1) constants (build_jloop, face_create_destroy.c:27-35) */
   double f_r, f_dl, f_dr, f_dperp;
   double f_rdrom;   /* sim_rdrOm_a at the face radius (riemann_visc_flux) */
+  double z, dz;     /* centre and extent of layer k */
+  /* z pair (ring a, ring a+NR) (build_jloop with zDir, face_create_destroy.c:37-46):
+     slab of z faces and their runs, r = the ring's centre, deltaL/deltaR the
+     half heights of layers k and k+1, deltaPerp = dr */
+  int zface_base, zface_cap, zrun_base, zrun_cap;
+  double zf_r, zf_dl, zf_dr, zf_dperp;
 } Annulus;
 
 /* Per-disk dynamic state (device-resident, updated by the kernels). */
@@ -165,6 +177,21 @@ typedef struct {
   /* the fused substep (k_prep, k_sweep) */
   unsigned long long *cfl_ann; /* [n_ann] CFL minimum of each annulus (bit pattern; ~0: none) */
   int *sweep_flag;             /* [n_ann] last k_sweep phase done for each annulus */
+  /* z faces of 3-D disks (NZ > 1): the same structures as the r faces, per
+     z pair (ring a, ring a+NR) of each ring a with k < NZ-1 */
+  int n_zslots, n_zruns, has_z;
+  int max_nz;             /* largest NZ of the disks */
+  const int *zslot_ann;   /* z-face slot -> ring of its pair (the lower ring) */
+  int *zfL, *zfR;         /* z-face cells (global); zfL = -1 past the list of a pair */
+  double *zfdphi, *zfcm;
+  int *zfstart;           /* first z face (within the slab) of each lower-ring cell */
+  int *zrr;               /* [n_cells][4] z-face ranges of each upper-ring cell (as rr) */
+  int *zruns;
+  int *zpair_nf, *zpair_jpmin, *zpair_T, *zpair_seq;
+  double *zfS;            /* [5][n_zslots] z-face slopes */
+  double *zfdp;           /* [2][n_zslots] z-face offsets dpL, dpR */
+  double *zfrf;           /* [5][n_zslots] z-face increments dt*dA*F */
+  double *gradz;          /* [5][n_cells] z slopes (cell_plm_rz with Z_DIR, which overwrites grad) */
 } DevPtrs;
 
 /* Forward-mode tangent: d/de of the state and of the substep intermediates
@@ -227,6 +254,14 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream);
 /* the outflow radial boundary, its damping and cell_calc_cons on the annuli
  * it rewrites (one block per disk); after k_update, for stop >= 6 */
 int dgk_outflow(const DevPtrs *d, int stop, void *stream);
+/* 3-D disks: the z-face list (zmerge), z-face slopes, z slopes (cell_plm_rz
+ * with Z_DIR), z-face fluxes, and the single-rank periodic z copy of
+ * cell_syncproc_z with the cell_calc_cons of the copied cells */
+int dgk_zmerge(const DevPtrs *d, int substep, void *stream);
+int dgk_zslope(const DevPtrs *d, void *stream);
+int dgk_plm_z(const DevPtrs *d, void *stream);
+int dgk_flux_z(const DevPtrs *d, int substep, void *stream);
+int dgk_zsync(const DevPtrs *d, int substep, void *stream);
 /* the fused substep: k_prep (face list, phi slopes, CFL minima) then k_sweep
  * (the wavefront over the annuli); forward, no passive scalar, no outflow
  * boundary, no sink */

@@ -228,6 +228,10 @@ __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_cellprep(DevPtrs d, Tan
 // Per annulus pair (i, i+1) of a disk, one block: the r-face list of
 // face_create/build_jloop (src/Face/face_create_destroy.c:22-193) as a checked
 // parallel merge, and cell_set_w (src/Cell/cell_set_w.c:12-102) of annulus i.
+// Z: the z pair (ring a, ring a+NR) of a 3-D disk (build_jloop with zDir:
+// both rings have N_p cells of annulus i) into the z-face arrays; no
+// cell_set_w then.
+template <bool Z>
 __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep) {
   __shared__ int sh_i[BLK / 32];
   __shared__ int sh_j[BLK];
@@ -243,11 +247,21 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
   const int np = A.np, off = A.cell_off;
   const int N = d.n_cells;
   const bool rigid = P.w_numeric == DC_RIGID;
-  if (tid == 0 && !rigid) d.w_ann[a] = A.wnum;
-  if (A.i < P.NR - 1) {
-    const int npo = d.ann[a + 1].np;
-    const int offo = d.ann[a + 1].cell_off;
-    const int rcap = A.run_cap;
+  if (!Z && tid == 0 && !rigid) d.w_ann[a] = A.wnum;
+  // the pair's arrays: r faces of (a, a+1), or z faces of (a, a+NR)
+  int *const pfL = Z ? d.zfL : d.fL, *const pfR = Z ? d.zfR : d.fR;
+  double *const pfdphi = Z ? d.zfdphi : d.fdphi, *const pfcm = Z ? d.zfcm : d.fcm;
+  int *const pruns = Z ? d.zruns : d.runs, *const pfstart = Z ? d.zfstart : d.fstart;
+  int *const prr = Z ? d.zrr : d.rr;
+  int *const p_nf = Z ? d.zpair_nf : d.pair_nf, *const p_jpmin = Z ? d.zpair_jpmin : d.pair_jpmin;
+  int *const p_T = Z ? d.zpair_T : d.pair_T, *const p_seq = Z ? d.zpair_seq : d.pair_seq;
+  const int fbase = Z ? A.zface_base : A.face_base, fcap = Z ? A.zface_cap : A.face_cap;
+  const int rbase = Z ? A.zrun_base : A.run_base;
+  const int partner = Z ? a + P.NR : a + 1;
+  if (Z ? A.k < P.NZ - 1 : A.i < P.NR - 1) {
+    const int npo = d.ann[partner].np;
+    const int offo = d.ann[partner].cell_off;
+    const int rcap = Z ? A.zrun_cap : A.run_cap;
     const bool staged = d.smem_face >= (int)sizeof(double) * 2 * (np + npo) + (int)sizeof(int) * rcap;
     const double *tin = traw + off, *din = d.dphi + off;
     const double *tout = traw + offo, *dout = d.dphi + offo;
@@ -274,14 +288,14 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
     c.dout = dout;
     c.Nin = np;
     c.Nout = npo;
-    c.fL = d.fL + A.face_base;
-    c.fR = d.fR + A.face_base;
-    c.fdphi = d.fdphi + A.face_base;
-    c.fcm = d.fcm + A.face_base;
-    c.runs = d.runs + A.run_base;
+    c.fL = pfL + fbase;
+    c.fR = pfR + fbase;
+    c.fdphi = pfdphi + fbase;
+    c.fcm = pfcm + fbase;
+    c.runs = pruns + rbase;
     c.sruns = staged ? reinterpret_cast<int *>(sm + 2 * (np + npo)) : c.runs;
-    c.fstart = d.fstart + off;
-    c.cap = A.face_cap;
+    c.fstart = pfstart + off;
+    c.cap = fcap;
     c.rcap = rcap;
     c.err = d.err;
     c.offL = off;
@@ -374,8 +388,8 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
       if (ntot > c.cap || stot + 2 > c.rcap) {
         if (tid == 0) {
           set_err(d.err, DGPU_EF_FACE_OVERFLOW);
-          d.pair_nf[a] = 0;
-          d.pair_T[a] = 0;
+          p_nf[a] = 0;
+          p_T[a] = 0;
           sh_nf = 0;
           sh_T = 0;
         }
@@ -386,10 +400,10 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
         if (tid == 0) {
           c.runs[0] = c.sruns[0] = 0;
           c.runs[stot + 1] = c.sruns[stot + 1] = ntot;
-          d.pair_nf[a] = ntot;
-          d.pair_jpmin[a] = jpmin;
-          d.pair_T[a] = stot;
-          d.pair_seq[a] = 0;
+          p_nf[a] = ntot;
+          p_jpmin[a] = jpmin;
+          p_T[a] = stot;
+          p_seq[a] = 0;
           sh_nf = ntot;
           sh_T = stot;
         }
@@ -401,17 +415,17 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
       for (int j = 0; j < np; ++j) face_cell<true>(c, j, jp, n, s);
       if (n > c.cap || s + 2 > c.rcap) {
         set_err(d.err, DGPU_EF_FACE_OVERFLOW);
-        d.pair_nf[a] = 0;
-        d.pair_T[a] = 0;
+        p_nf[a] = 0;
+        p_T[a] = 0;
         sh_nf = 0;
         sh_T = 0;
       } else {
         c.runs[0] = c.sruns[0] = 0;
         c.runs[s + 1] = c.sruns[s + 1] = n;
-        d.pair_nf[a] = n;
-        d.pair_jpmin[a] = jpmin;
-        d.pair_T[a] = s;
-        d.pair_seq[a] = 1;
+        p_nf[a] = n;
+        p_jpmin[a] = jpmin;
+        p_T[a] = s;
+        p_seq[a] = 1;
         sh_nf = n;
         sh_T = s;
       }
@@ -430,7 +444,7 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
           if (s0 + npo <= T) rr.z = c.sruns[s0 + npo], rr.w = c.sruns[s0 + npo + 1];
           if (s0 + 2 * npo <= T) rr.z = INT_MIN;
         }
-        reinterpret_cast<int4 *>(d.rr)[offo + jq] = rr;
+        reinterpret_cast<int4 *>(prr)[offo + jq] = rr;
       }
       // slab slots past the list hold no face
       for (int n = nf + tid; n < c.cap; n += nt) c.fL[n] = -1;
@@ -438,7 +452,7 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
   }
   // C_RIGID: the mass-weighted mean v_phi of the annulus, summed in j order
   // like the reference (cell_set_w.c:41-49); one lane, after the merge
-  if (rigid && tid == nt - 32) {
+  if (!Z && rigid && tid == nt - 32) {
     double w = 0.0, Mring = 0.0;
     for (int j = 0; j < np; ++j) {
       double vp = A.r * ld(d.prim, D_UPP, N, off + j);
@@ -451,7 +465,12 @@ __device__ __forceinline__ void merge_pair(const DevPtrs &d, int a, int substep)
 }
 
 __global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_merge(DevPtrs d, int substep) {
-  merge_pair(d, blockIdx.x, substep);
+  merge_pair<false>(d, blockIdx.x, substep);
+}
+
+// The z-face lists of a 3-D disk: one block per ring a with k < NZ-1.
+__global__ void __launch_bounds__(BLK, DGPU_MINB_FACE) k_zmerge(DevPtrs d, int substep) {
+  merge_pair<true>(d, blockIdx.x, substep);
 }
 
 // ---------------------------------------------------------------------------
@@ -523,7 +542,7 @@ __device__ __forceinline__ void plm_r_grad(const DevPtrs &d, const TanPtrs &tp, 
   });
   double dAtot;
   {
-    double dz = P.dz, dp = d.dphi[g];
+    double dz = A.dz, dp = d.dphi[g];
     if (A.i == 0) dAtot = dz * A.rp * dp;
     else if (A.i == P.NR - 1) dAtot = dz * A.rm * dp;
     else dAtot = dz * (A.rp + A.rm) * dp;
@@ -572,7 +591,7 @@ __device__ __forceinline__ unsigned long long cfl_key(const DevPtrs &d, const An
   double dx = dr;
   double rdphi = .5 * (A.rp + A.rm) * d.dphi[g];
   if (rdphi < dr) dx = rdphi;
-  if (dx > P.dz) dx = P.dz;
+  if (dx > A.dz) dx = A.dz;
   double Pp = ld(d.prim, D_PPP, N, g), rho = ld(d.prim, D_RHO, N, g);
   double vp = ld(d.prim, D_UPP, N, g) * r - w;
   double vr = ld(d.prim, D_URR, N, g), vz = ld(d.prim, D_UZZ, N, g);
@@ -692,7 +711,7 @@ __device__ __forceinline__ void flux_phi_cell(const DevPtrs &d, const TanPtrs &t
   const int j = g - A.cell_off;
   const int cL = g, cR = (j == A.np - 1) ? A.cell_off : g + 1;
   const double dpL = d.dphi[cL], dpR = d.dphi[cR];
-  const double dz = P.dz;
+  const double dz = A.dz;
   const double dr = A.rp - A.rm;
   const double r = .5 * (A.rp + A.rm);
   const double dA = dr * dz;
@@ -828,6 +847,155 @@ __global__ void __launch_bounds__(BLK, MB) k_flux_r(DevPtrs d, TanPtrs tp, int s
 }
 
 // ---------------------------------------------------------------------------
+// z faces of 3-D disks (face_create with direction 1, cell_plm_rz with
+// Z_DIR, the z-face riemann_setup_rz + riemann_AddFlux of
+// src/TimeStep/timestep_routines.c:63-71)
+// ---------------------------------------------------------------------------
+// z-face slope and reconstruction offsets, once per face: as k_rslope, with
+// the half heights of the two layers in place of the radial half widths.
+__global__ void __launch_bounds__(BLK) k_zslope(DevPtrs d) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= d.n_zslots) return;
+  const int cL = rd(d.zfL + slot);
+  if (cL < 0) return;  // slot past the face list of its pair
+  const int cR = rd(d.zfR + slot);
+  const int a = rd(d.zslot_ann + slot);
+  const Annulus &A = d.ann[a];
+  const int N = d.n_cells, NS = d.n_zslots;
+  const double cm = rd(d.zfcm + slot);
+  double pL = rd(d.tiphw + cL) - .5 * rd(d.dphi + cL);
+  double pR = rd(d.tiphw + cR) - .5 * rd(d.dphi + cR);
+  double dpL = cm - pL;
+  dpL = wrap_pm(dpL, d.err);
+  double dpR = pR - cm;
+  dpR = wrap_pm(dpR, d.err);
+  d.zfdp[slot] = dpL;
+  d.zfdp[(size_t)NS + slot] = dpR;
+  const double den = A.zf_dr + A.zf_dl;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const double WL = ldr(d.prim, q, N, cL) + dpL * ldr(d.gradp, q, N, cL);
+    const double WR = ldr(d.prim, q, N, cR) - dpR * ldr(d.gradp, q, N, cR);
+    d.zfS[(size_t)q * NS + slot] = (WR - WL) / den;
+  }
+}
+
+// cell_plm_rz with Z_DIR (src/Cell/cell_plm.c:13-114) per cell of a 3-D disk:
+// the face-area-weighted mean of the z-face slopes over
+// dAtot = 2*.5*(rp^2 - rm^2)*dphi, then the limiter in face order.  The
+// reference overwrites grad with it; here it goes to gradz, which the z
+// fluxes and (in 3-D) the viscous source read.
+__global__ void __launch_bounds__(BLK) k_plm_z(DevPtrs d) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells, NS = d.n_zslots;
+  if (g >= N) return;
+  const int a = d.cell_ann[g];
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  if (P.NZ == 1) return;
+  const double rm = A.rm, rp = A.rp;
+  const double zr = .5 * (rp + rm), zperp = rp - rm;  // build_jloop's r and deltaPerp of a z face
+  double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for_cell_zface_ranges(d, A, a, g, P.NR, P.NZ, [&](int s, int e, int) {
+    for (int n = s; n < e; ++n) {
+      const double dA = zr * rd(d.zfdphi + n) * zperp;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) gq[q] += ld(d.zfS, q, NS, n) * dA;
+    }
+  });
+  const double dp = d.dphi[g];
+  const double dAtot = 2. * .5 * (rp * rp - rm * rm) * dp;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) gq[q] /= dAtot;
+  for_cell_zface_ranges(d, A, a, g, P.NR, P.NZ, [&](int s, int e, int) {
+    for (int n = s; n < e; ++n) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const double Sq = ld(d.zfS, q, NS, n);
+        if (Sq * gq[q] < 0.0) gq[q] = 0.0;
+        else if (fabs(P.plm * Sq) < fabs(gq[q])) gq[q] = P.plm * Sq;
+      }
+    }
+  });
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d.gradz[(size_t)q * N + g] = gq[q];
+}
+
+// z faces: thread per face slot (riemann_setup_rz with ZDIRECTION,
+// Riemann_setup.c:11-44, and riemann_AddFlux with w = 0): the states are
+// reconstructed with the z slopes; the viscous flux of a z face is zero, and
+// only the reference's v_z check remains.
+__global__ void __launch_bounds__(BLK) k_flux_z(DevPtrs d, int substep) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= d.n_zslots) return;
+  const int cL = d.zfL[slot];
+  if (cL < 0) return;
+  const int cR = d.zfR[slot];
+  const int a = d.zslot_ann[slot];
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  const InstState &S = d.ist[A.inst];
+  const int N = d.n_cells, NS = d.n_zslots;
+  const double fac = substep == 1 ? 1.0 : 0.5;
+  const double deltaL = A.zf_dl, deltaR = A.zf_dr;
+  const double dpL = d.zfdp[slot], dpR = d.zfdp[(size_t)NS + slot];
+  const double r = A.zf_r;
+  const double dA = r * d.zfdphi[slot] * A.zf_dperp;
+  double pL[5], pR[5], F[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    pL[q] = ld(d.prim, q, N, cL) + ld(d.gradz, q, N, cL) * deltaL + ld(d.gradp, q, N, cL) * dpL;
+    pR[q] = ld(d.prim, q, N, cR) - ld(d.gradz, q, N, cR) * deltaR - ld(d.gradp, q, N, cR) * dpR;
+  }
+  riemann_flux(pL, pR, r, 2, 0.0, P.gamma, P.riemann, F);
+  const double k = fac * S.dt * dA;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d.zfrf[(size_t)q * NS + slot] = k * F[q];
+  if (P.has_visc) {
+    // riemann_visc_flux averages the reconstructed states on a z face and
+    // exits on a nonzero v_z (Riemann_routines.c:271-274)
+    const double vz = .5 * (pL[D_UZZ] + pR[D_UZZ]);
+    if (fabs(vz) > 1.e-12) set_err(d.err, DGPU_EF_VISC_VZ);
+  }
+}
+
+// The single-rank cell_syncproc_z (src/Cell/cell_sync.c:156-205) at the end
+// of a substep of a 3-D disk, then cell_calc_cons of the cells it wrote: the
+// ng lowest layers take prim, RKcons and tiph of layers NZ-2ng .. NZ-ng-1, the
+// ng highest those of layers ng .. 2ng-1 (dphi stays the cell's own).  Runs
+// after k_update and the radial boundary, which have finished every layer.
+__global__ void __launch_bounds__(BLK) k_zsync(DevPtrs d, int substep) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells;
+  if (g >= N) return;
+  const int a = d.cell_ann[g];
+  const Annulus &A = d.ann[a];
+  const DiskParams &P = d.par[A.inst];
+  if (P.NZ == 1) return;
+  const int ng = P.ngz, shift = P.NZ - 2 * ng;
+  int ks;
+  if (A.k < ng) ks = A.k + shift;
+  else if (A.k >= P.NZ - ng) ks = A.k - shift;
+  else return;
+  const Annulus &Sr = d.ann[a + (ks - A.k) * P.NR];
+  const int gs = Sr.cell_off + (g - A.cell_off);
+  double *tout = substep == 1 ? d.tiph1 : d.tiph0;
+  double pr[5], c[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    pr[q] = d.prim[(size_t)q * N + gs];
+    d.prim[(size_t)q * N + g] = pr[q];
+    d.rkcons[(size_t)q * N + g] = d.rkcons[(size_t)q * N + gs];
+  }
+  tout[g] = tout[gs];
+  const double r = .5 * (A.rm + A.rp);
+  const double dV = A.dv_half * d.dphi[g] * A.dz;
+  prim2cons(pr, c, r, dV, P.gamma);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
+}
+
+// ---------------------------------------------------------------------------
 // Per-cell update: flux gather + sources + mesh motion + prim/cons + BC + damping
 // ---------------------------------------------------------------------------
 
@@ -891,12 +1059,12 @@ __device__ __forceinline__ void source_cell_k(const DevPtrs &d, const TanPtrs &t
     SrcGeom sg;
     sg.r = r;
     sg.dt = dt;
-    sg.dV = dphi * .5 * A.dv_diff * P.dz;
+    sg.dV = dphi * .5 * A.dv_diff * A.dz;
     sincos(phi, &sg.sinp, &sg.cosp);
     sg.xpos = r * sg.cosp;
     sg.ypos = r * sg.sinp;
     {
-      double z = P.z;
+      double z = A.z;
       double R = sqrt(r * r + z * z);
       if (P.grav2d == 1) {
         sg.sint = 1.0;
@@ -916,7 +1084,9 @@ __device__ __forceinline__ void source_cell_k(const DevPtrs &d, const TanPtrs &t
     grav_t(G, S, P, tp, A.inst);
     T gu = 0.0, gpu = 0.0;
     if (P.has_visc) {
-      gu = ldq<T>(d.grad, tp.grad, D_UPP, N, g);
+      // in 3-D cell_plm_rz(Z_DIR) has overwritten grad with the z slopes by the
+      // time cell_add_visc_src reads it (timestep_routines.c:63-81)
+      gu = (d.has_z && P.NZ > 1) ? T(d.gradz[(size_t)D_UPP * N + g]) : ldq<T>(d.grad, tp.grad, D_UPP, N, g);
       gpu = ldq<T>(d.gradp, tp.gradp, D_URR, N, g);
     }
     T sv[6];
@@ -1044,7 +1214,7 @@ __device__ __forceinline__ void update_cell(const DevPtrs &d, const TanPtrs &tp,
       }
       // cell_calc_prim -> cell_cons2prim (src/Cell/cell_conversion.c:57-122)
       const double r = .5 * (A.rm + A.rp);
-      const double dV = A.dv_half * dphi_n * P.dz;
+      const double dV = A.dv_half * dphi_n * A.dz;
       T pr[5];
       cons2prim(c, dV, r, P, pr);
       // passive scalars: prim = cons / cons[DDD] (cell_conversion.c:98-101)
@@ -1188,7 +1358,7 @@ __global__ void __launch_bounds__(BLK, MB) k_prep(DevPtrs d, int substep) {
   __shared__ double sh_rk[6];
   const int a = blockIdx.x;
   const TanPtrs tp = {};
-  merge_pair(d, a, substep);
+  merge_pair<false>(d, a, substep);
   __syncthreads();  // w_ann[a] (one lane) before the CFL
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -1428,7 +1598,7 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
   const Annulus &A = d.ann[d.cell_ann[g]];
   const DiskParams &P = d.par[A.inst];
   double r = .5 * (A.rp + A.rm);
-  double dV = A.dv_half * d.dphi[g] * P.dz;
+  double dV = A.dv_half * d.dphi[g] * A.dz;
   T p[5], c[5];
 #pragma unroll
   for (int q = 0; q < 5; ++q) p[q] = ldq<T>(d.prim, tp.prim, q, N, g);
@@ -1447,11 +1617,11 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
 // (prim - 0 * grad * (...) / 2.) * dA is prim * dA for a finite slope.  A cell
 // with no face keeps its own value, divided (the reference zeroes only the
 // cells its face loop visits).
-__device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int i, int outer) {
-  const int a = P.ann_base + i + outer;
+__device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int base, int i, int outer) {
+  const int a = base + i + outer;
   const Annulus &A = d.ann[a];
-  const Annulus &S = d.ann[P.ann_base + i + 1 - outer];  // the annulus read
-  const double rf = d.ann[P.ann_base + i].f_r;           // FacePos(i)
+  const Annulus &S = d.ann[base + i + 1 - outer];  // the annulus read
+  const double rf = d.ann[base + i].f_r;           // FacePos(i)
   const size_t NB = d.n_ob;
   const int nq = 5 + P.num_n;
   for (int j = threadIdx.x; j < A.np; j += blockDim.x) {
@@ -1466,30 +1636,33 @@ __device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int i, int o
       for (int q = 0; q < nq; ++q) s[q] += d.obuf[q * NB + o] * dA;
       ++nface;
     });
-    const double dA = P.dz * rf * d.dphi[g];
+    const double dA = A.dz * rf * d.dphi[g];
     const size_t self = (size_t)A.ob_off + j;
     for (int q = 0; q < nq; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
   }
 }
 
-// The outflow radial boundary of one disk per block, in the reference's order:
-// annulus 0 from annulus 1 (unless NoInnerBC == 1), NR-2 from NR-3, NR-1 from
-// the new NR-2; each pass reads the previous one's results.  Then the
-// rewritten annuli get cell_bc_damp and, for stop 7, cell_calc_cons.
+// The outflow radial boundary of one layer of a disk per block (blockIdx.x:
+// the disk, blockIdx.y: the layer), in the reference's order: annulus 0 from
+// annulus 1 (unless NoInnerBC == 1), NR-2 from NR-3, NR-1 from the new NR-2;
+// each pass reads the previous one's results.  The r faces join rings of one
+// layer, so the layers are independent.  Then the rewritten annuli get
+// cell_bc_damp and, for stop 7, cell_calc_cons.
 __global__ void __launch_bounds__(BLK) k_outflow(DevPtrs d, int stop) {
   const DiskParams &P = d.par[blockIdx.x];
-  if (!(P.outflow & 1)) return;
+  if (!(P.outflow & 1) || (int)blockIdx.y >= P.NZ) return;
   const int NR = P.NR, N = d.n_cells;
+  const int base = P.ann_base + (int)blockIdx.y * NR;
   const size_t NB = d.n_ob;
-  if (P.outflow & 2) outflow_pass(d, P, 0, 0);
+  if (P.outflow & 2) outflow_pass(d, P, base, 0, 0);
   __syncthreads();
-  outflow_pass(d, P, NR - 3, 1);
+  outflow_pass(d, P, base, NR - 3, 1);
   __syncthreads();
-  outflow_pass(d, P, NR - 2, 1);
+  outflow_pass(d, P, base, NR - 2, 1);
   __syncthreads();
   for (int k = 0; k < 3; ++k) {
     const int i = k == 0 ? 0 : NR - 3 + k;
-    const int a = P.ann_base + i;
+    const int a = base + i;
     const Annulus &A = d.ann[a];
     if (!(A.kind & DGPU_AK_OUT_DST)) continue;
     const double r = .5 * (A.rm + A.rp);
@@ -1503,7 +1676,7 @@ __global__ void __launch_bounds__(BLK) k_outflow(DevPtrs d, int stop) {
       for (int q = 0; q < 5; ++q) d.prim[(size_t)q * N + g] = pr[q];
       for (int q = 5; q < 5 + P.num_n; ++q) d.prim[(size_t)q * N + g] = d.obuf[q * NB + A.ob_off + j];
       if (stop >= 7) {
-        const double dV = A.dv_half * d.dphi[g] * P.dz;
+        const double dV = A.dv_half * d.dphi[g] * A.dz;
         prim2cons(pr, c, r, dV, P.gamma);
 #pragma unroll
         for (int q = 0; q < 5; ++q) d.cons[(size_t)q * N + g] = c[q];
@@ -1690,6 +1863,31 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
                                                                                         tail, nullptr, nullptr);
   return (int)cudaGetLastError();
 }
+int dgk_zmerge(const DevPtrs *d, int substep, void *stream) {
+  if (!d->has_z) return 0;
+  k_zmerge<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_zslope(const DevPtrs *d, void *stream) {
+  if (!d->has_z || d->n_zslots <= 0) return 0;
+  k_zslope<<<(d->n_zslots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
+  return (int)cudaGetLastError();
+}
+int dgk_plm_z(const DevPtrs *d, void *stream) {
+  if (!d->has_z) return 0;
+  k_plm_z<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d);
+  return (int)cudaGetLastError();
+}
+int dgk_flux_z(const DevPtrs *d, int substep, void *stream) {
+  if (!d->has_z || d->n_zslots <= 0) return 0;
+  k_flux_z<<<(d->n_zslots + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
+int dgk_zsync(const DevPtrs *d, int substep, void *stream) {
+  if (!d->has_z) return 0;
+  k_zsync<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  return (int)cudaGetLastError();
+}
 int dgk_prep(const DevPtrs *d, int substep, void *stream) {
   k_prep<DGPU_MINB_PREP><<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
@@ -1705,7 +1903,7 @@ int dgk_sweep(const DevPtrs *d, int substep, void *stream) {
 }
 int dgk_outflow(const DevPtrs *d, int stop, void *stream) {
   if (d->n_ob <= 0 || stop < 6) return 0;
-  k_outflow<<<d->n_inst, BLK, 0, (cudaStream_t)stream>>>(*d, stop);
+  k_outflow<<<dim3(d->n_inst, d->max_nz), BLK, 0, (cudaStream_t)stream>>>(*d, stop);
   return (int)cudaGetLastError();
 }
 int dgk_calc_cons(const DevPtrs *d, const TanPtrs *t, void *stream) {

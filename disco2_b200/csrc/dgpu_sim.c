@@ -483,7 +483,7 @@ static double gm_dist(const double *gm, int p, double r, double phi, double z) {
   return sqrt((x - xbh) * (x - xbh) + (y - ybh) * (y - ybh) + z * z);
 }
 
-int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, double dphi, const double *gm,
+int dsim_grid_init(const struct dgpu_sim *s, int k, int i, long idx, double tiph, double dphi, const double *gm,
                    struct random_data *rnd, double *prim) {
   double rm = dsim_rface(s, i - 1);
   double rp = dsim_rface(s, i);
@@ -510,16 +510,18 @@ int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, doubl
     return 0;
   }
   if (t == DI_TORUS) {
-    /* cell_init_torus (src/Cell/initial_data/cell_init_torus.c:17-89) for the
-     * single z layer (z = 0); one rand() per cell after srand(666).  The
-     * magnetic terms of the file are never stored, and its Pp = rho branch
-     * follows a clamp that already holds PoRho >= 1e-5, so neither is here. */
+    /* cell_init_torus (src/Cell/initial_data/cell_init_torus.c:17-89): z is
+     * the centre of layer k (0 for a single layer); one rand() per cell after
+     * srand(666), layer after layer.  The magnetic terms of the file are never
+     * stored, and its Pp = rho branch follows a clamp that already holds
+     * PoRho >= 1e-5, so neither is here. */
     double gam = s->Adiabatic_Index, M = 1.0, r_inner = 0.7, r_max = 1.0, q = 2.;
     double sx = 2. * q - q;
     double GammaFac = (gam - 1.) / gam;
     double Phi_inner = -1.0 / r_inner, Phi_max = -1.0 / r_max;
     double Rho_norm = pow(GammaFac * (Phi_inner - Phi_max + pow(r_inner, -sx) / sx - pow(1.0, -sx) / sx), 1.0 / (gam - 1.0));
     double z = 0.0;
+    if (s->NumZ != 1) z = 0.5 * (dsim_zface(s, k - 1) + dsim_zface(s, k));
     double R = sqrt(r * r + z * z);
     double Phi = -M / R;
     double omega = pow(r, -q);
@@ -656,13 +658,20 @@ void dsim_fill_params(const struct dgpu_sim *s, DiskParams *p) {
     p->dz = zp - zm;
     p->z = .5 * (zp + zm);
   }
+  p->NZ = s->NZ;
+  p->ngz = s->ng_min[1];
 }
 
-void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a) {
+void dsim_fill_annulus(const struct dgpu_sim *s, int k, int i, Annulus *a) {
   double rm = dsim_rface(s, i - 1), rp = dsim_rface(s, i);
   double r = .5 * (rp + rm);
-  int NR = s->NR;
+  double zm = dsim_zface(s, k - 1), zp = dsim_zface(s, k);
+  int NR = s->NR, NZ = s->NZ;
+  int kreal = k >= s->ng_min[1] && k < NZ - s->ng_max[1];
   a->i = i;
+  a->k = k;
+  a->dz = zp - zm;
+  a->z = .5 * (zp + zm);
   a->np = s->N_p[i];
   a->rm = rm;
   a->rp = rp;
@@ -681,12 +690,14 @@ void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a) {
     default: a->wnum = 0.0; break;
   }
   a->kind = 0;
-  if (i >= s->ng_min[0] && i < NR - s->ng_max[0]) a->kind |= DGPU_AK_CFL;
+  /* cell_mindt and the Mdot sum skip the ghost layers too (cell_mindt.c:38-42,
+   * cell_source.c:86-88) */
+  if (i >= s->ng_min[0] && i < NR - s->ng_max[0] && kreal) a->kind |= DGPU_AK_CFL;
   /* the accretion-rate objective is measured on the innermost non-ghost annulus */
   if (i == s->ng_min[0]) a->kind |= DGPU_AK_MDOT;
   {
     int imin = (s->ng_min[0] == 1) ? 0 : s->ng_min[0];
-    if (i >= imin && i < NR - s->ng_max[0]) a->kind |= DGPU_AK_SINK_SUM;
+    if (i >= imin && i < NR - s->ng_max[0] && kreal) a->kind |= DGPU_AK_SINK_SUM;
   }
   if (dsim_single_init(s, i, a->ic) == 1) {
     a->kind |= DGPU_AK_IC;
@@ -712,14 +723,24 @@ void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a) {
       a->kind |= DGPU_AK_DAMP;
     }
   }
+  /* build_jloop (src/Face/face_create_destroy.c:27-46): the r pair (i, i+1)
+   * of layer k, and the z pair (k, k+1) of annulus i */
   if (i < NR - 1) {
     a->f_r = dsim_rface(s, i);
     a->f_dl = .5 * (dsim_rface(s, i) - dsim_rface(s, i - 1));
     a->f_dr = .5 * (dsim_rface(s, i + 1) - dsim_rface(s, i));
-    a->f_dperp = dsim_zface(s, 0) - dsim_zface(s, -1);
+    a->f_dperp = zp - zm;
     a->f_rdrom = dsim_rdrOm_a(s, a->f_r, 1.0);
   } else {
     a->f_r = a->f_dl = a->f_dr = a->f_dperp = a->f_rdrom = 0.0;
+  }
+  if (NZ > 1 && k < NZ - 1) {
+    a->zf_dl = .5 * (dsim_zface(s, k) - dsim_zface(s, k - 1));
+    a->zf_dr = .5 * (dsim_zface(s, k + 1) - dsim_zface(s, k));
+    a->zf_dperp = rp - rm;
+    a->zf_r = .5 * (rp + rm);
+  } else {
+    a->zf_dl = a->zf_dr = a->zf_dperp = a->zf_r = 0.0;
   }
 }
 

@@ -69,11 +69,11 @@ int dsim_single_init(const struct dgpu_sim *s, int i, double *prim);
  * srand(666), drawn once per cell for that type only.  Returns 0 or -1
  * (unsupported type). */
 struct random_data;
-int dsim_grid_init(const struct dgpu_sim *s, int i, long idx, double tiph, double dphi, const double *gm,
+int dsim_grid_init(const struct dgpu_sim *s, int k, int i, long idx, double tiph, double dphi, const double *gm,
                    struct random_data *rnd, double *prim);
 
 /* Fill the per-annulus table entries that depend only on the Sim. */
-void dsim_fill_annulus(const struct dgpu_sim *s, int i, Annulus *a);
+void dsim_fill_annulus(const struct dgpu_sim *s, int k, int i, Annulus *a);
 void dsim_fill_params(const struct dgpu_sim *s, DiskParams *p);
 
 /* Initial phi edges of cell_create: srand(666), one rand() per annulus. */

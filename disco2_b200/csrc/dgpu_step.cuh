@@ -162,6 +162,35 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
       }
     });
   }
+  // z faces of a 3-D disk, after the r faces (timestep_routines.c:63-71): the
+  // increments of pair (a-NR, a) are added, those of (a, a+NR) subtracted.  Their
+  // viscous flux is zero (riemann_visc_flux sets neither the r nor the phi
+  // terms); adding its +0 to the upper cell keeps the reference's signed zeros.
+  if constexpr (std::is_same<T, double>::value) {
+    if (d.has_z && P.NZ > 1) {
+      const int NSZ = d.n_zslots;
+      const bool visc = P.has_visc;
+      for_cell_zface_ranges(d, A, a, g, P.NR, P.NZ, [&](int s, int e, int up) {
+        for (int n = s; n < e; ++n) {
+          double u[5];
+#pragma unroll
+          for (int q = 0; q < 5; ++q) u[q] = NC ? ldr(d.zfrf, q, NSZ, n) : ld(d.zfrf, q, NSZ, n);
+          if (up) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) c[q] += u[q];
+            if (visc) {
+              c[D_SRR] += 0.0;
+              c[D_LLL] += 0.0;
+              c[D_TAU] += 0.0;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) c[q] -= u[q];
+          }
+        }
+      });
+    }
+  }
   if (stop == 3) return false;
   // cell_add_src, cell_add_visc_src, cell_add_split_fictitious: the source
   // increments come from k_source; added here in the reference's order
@@ -178,7 +207,7 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
   if (P.cooling == 1) {
     // cooling reads the running tau (cell_source.c:187-203)
     const T rho = ldqr<T>(d.prim, tp.prim, D_RHO, N, g), Pp = ldqr<T>(d.prim, tp.prim, D_PPP, N, g);
-    const double dV = rd(d.dphi + g) * .5 * A.dv_diff * P.dz;
+    const double dV = rd(d.dphi + g) * .5 * A.dv_diff * A.dz;
     if (P.init_type == DI_SHEAR) {
       T cooling_term = (Pp - .01) / (P.gamma - 1.) * dV / 1.e-2;
       if (cooling_term < 0.0) cooling_term = 0.0;

@@ -51,6 +51,7 @@ SIGNATURES = {
     "dgpu_stage": (_I, [_P, _I]),
     "dgpu_get_stage_data": (_I, [_P, _I, _dp, _dp, _dp, _dp, _dp]),
     "dgpu_face_list": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
+    "dgpu_face_list_z": (_I, [_P, _I, _I, _ip, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
     "dgpu_torque": (_I, [_P, _I, _dp]),
     "dgpu_face_list_noalloc": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P, _P, _ip, _P]),
     "dgpu_autotune": (_I, [_P, _I, _ip]),
@@ -255,21 +256,24 @@ class Context:
     def stage(self, phase: int):
         self._ck(load().dgpu_stage(self._h, phase))
 
-    def face_list(self, inst: int = 0) -> dict:
+    def face_list(self, inst: int = 0, z: bool = False) -> dict:
+        """The r-face list (z: the z-face list of a 3-D disk) in the
+        reference's order; "nri" holds the pair offsets."""
         lib = load()
         s = self.sims[inst]
+        fn = lib.dgpu_face_list_z if z else lib.dgpu_face_list
         nf = C.c_int()
-        lib.dgpu_face_list(self._h, inst, 0, None, None, None, None, None, None, None, None, None,
-                           C.byref(nf))
+        fn(self._h, inst, 0, None, None, None, None, None, None, None, None, None, C.byref(nf))
         n = nf.value
-        out = {"nri": np.zeros(s.num_annuli, np.int32), "L": np.zeros(n, np.int32),
+        npairs = int(s.param("NZ" if z else "NR"))
+        out = {"nri": np.zeros(npairs, np.int32), "L": np.zeros(n, np.int32),
                "R": np.zeros(n, np.int32)}
         for k in ("r", "dphi", "dA", "deltaL", "deltaR", "cm"):
             out[k] = np.zeros(n)
-        self._ck(lib.dgpu_face_list(self._h, inst, n, _iptr(out["nri"]), _iptr(out["L"]),
-                                    _iptr(out["R"]), _dptr(out["r"]), _dptr(out["dphi"]),
-                                    _dptr(out["dA"]), _dptr(out["deltaL"]), _dptr(out["deltaR"]),
-                                    _dptr(out["cm"]), C.byref(nf)))
+        self._ck(fn(self._h, inst, n, _iptr(out["nri"]), _iptr(out["L"]),
+                    _iptr(out["R"]), _dptr(out["r"]), _dptr(out["dphi"]),
+                    _dptr(out["dA"]), _dptr(out["deltaL"]), _dptr(out["deltaR"]),
+                    _dptr(out["cm"]), C.byref(nf)))
         return out
 
     def torque(self, inst: int = 0) -> float:

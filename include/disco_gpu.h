@@ -169,6 +169,15 @@ int dgpu_get_stage_data(dgpu_ctx *ctx, int inst, double *grad, double *gradp, do
 int dgpu_face_list(dgpu_ctx *ctx, int inst, int cap, int *nri, int *L, int *R, double *r,
                    double *dphi, double *dA, double *deltaL, double *deltaR, double *cm,
                    int *nf);
+/* The z-face list of a 3-D disk (NumZ > 1), as face_create(..., 1) builds it
+ * (src/Face/face_create_destroy.c:165-191) and in its order: layer pair
+ * (k, k+1) after layer pair, the annuli inside each; nzk[NZ] offsets
+ * (timestep_n(..., Z_DIR)), r = the annulus centre, dA = r dphi dr, deltaL and
+ * deltaR the half heights of the two layers.  Arguments as for
+ * dgpu_face_list; DGPU_ERR_ARG for a 2-D disk. */
+int dgpu_face_list_z(dgpu_ctx *ctx, int inst, int cap, int *nzk, int *L, int *R, double *r,
+                     double *dphi, double *dA, double *deltaL, double *deltaR, double *cm,
+                     int *nf);
 
 /* ---- Face list without allocation ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -157,8 +157,9 @@ def read_faces(path: str) -> Faces:
 
 
 def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = None,
-        faces: bool = False, dtlog: bool = False, workdir: str | None = None):
-    """Run `nsteps` RK2 steps; returns (final State, Faces|None, dt log array|None)."""
+        faces: bool = False, dtlog: bool = False, workdir: str | None = None, zfaces: bool = False):
+    """Run `nsteps` RK2 steps; returns (final State, Faces|None, dt log array|None).
+    zfaces (reference build, 3-D disks): the Faces are the z faces."""
     exe = _exe(impl)
     if not os.path.exists(exe):
         raise FileNotFoundError(f"oracle binary missing: {exe} (run oracle.build())")
@@ -171,7 +172,7 @@ def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = No
             cmd += ["--load", lp]
         fp = os.path.join(td, "faces.bin")
         if faces:
-            cmd += ["--faces", fp]
+            cmd += ["--zfaces" if zfaces else "--faces", fp]
         lg = os.path.join(td, "dt.log")
         if dtlog:
             cmd += ["--dtlog", lg]

@@ -14,7 +14,8 @@
  *       times and dumps the final state.  --load replaces prim/tiph/dphi after
  *       the initial data (then calc_cons); --faces dumps the r-face list
  *       (face_create, src/Face/face_create_destroy.c:130-193) of the initial
- *       state; --dtlog writes "t dt" per step.  The wall time of the step
+ *       state, --zfaces the z-face list of a 3-D disk in the same format (its
+ *       offsets are nzk); --dtlog writes "t dt" per step.  The wall time of the step
  *       loop alone goes to stderr as "steps_wall_s <seconds>"; --warmup runs W
  *       untimed steps first (not dumped).
  *
@@ -165,10 +166,12 @@ static void load_state(const char *path, struct Sim *s, struct Cell ***cells) {
   fclose(f);
 }
 
-static void dump_faces(const char *path, struct Sim *s, struct Cell ***cells, struct TimeStep *ts) {
-  struct Face *F = face_create(cells, s, ts, 0);
-  int NR = sim_N(s, R_DIR);
-  int Nf = ts->nri[NR - 1];
+/* the r faces (dir 0: face_create's nri offsets) or the z faces (dir 1: nzk) */
+static void dump_faces(const char *path, struct Sim *s, struct Cell ***cells, struct TimeStep *ts, int dir) {
+  struct Face *F = face_create(cells, s, ts, dir);
+  int NR = dir ? sim_N(s, Z_DIR) : sim_N(s, R_DIR);
+  int *off = dir ? ts->nzk : ts->nri;
+  int Nf = off[NR - 1];
   struct Cell *c0 = cell_base(cells);
   FILE *f = fopen(path, "wb");
   int n;
@@ -179,7 +182,7 @@ static void dump_faces(const char *path, struct Sim *s, struct Cell ***cells, st
   wr(f, "DFACES1", 1, 8);
   wr(f, &NR, sizeof(int), 1);
   wr(f, &Nf, sizeof(int), 1);
-  wr(f, ts->nri, sizeof(int), NR);
+  wr(f, off, sizeof(int), NR);
   for (n = 0; n < Nf; ++n) { int x = (int)(F[n].L - c0); wr(f, &x, sizeof(int), 1); }
   for (n = 0; n < Nf; ++n) { int x = (int)(F[n].R - c0); wr(f, &x, sizeof(int), 1); }
   for (n = 0; n < Nf; ++n) wr(f, &F[n].r, sizeof(double), 1);
@@ -298,7 +301,7 @@ static void objectives(struct Sim *s, struct Cell ***cells, struct GravMass *gm,
 }
 
 int main(int argc, char **argv) {
-  const char *mode, *par, *out, *load = NULL, *faces = NULL, *dtlog = NULL, *dtfile = NULL;
+  const char *mode, *par, *out, *load = NULL, *faces = NULL, *zfaces = NULL, *dtlog = NULL, *dtfile = NULL;
   int nsteps, a, step, warmup = 0;
   char parbuf[1024];
   struct MPIsetup *mpi;
@@ -318,6 +321,7 @@ int main(int argc, char **argv) {
   for (a = 5; a < argc; ++a) {
     if (!strcmp(argv[a], "--load") && a + 1 < argc) load = argv[++a];
     else if (!strcmp(argv[a], "--faces") && a + 1 < argc) faces = argv[++a];
+    else if (!strcmp(argv[a], "--zfaces") && a + 1 < argc) zfaces = argv[++a];
     else if (!strcmp(argv[a], "--dtlog") && a + 1 < argc) dtlog = argv[++a];
     else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--dtfile") && a + 1 < argc) dtfile = argv[++a];
@@ -364,7 +368,8 @@ int main(int argc, char **argv) {
   cell_calc_cons(cells, s);
 
   if (!strcmp(mode, "run")) {
-    if (faces) dump_faces(faces, s, cells, ts);
+    if (faces) dump_faces(faces, s, cells, ts, 0);
+    if (zfaces && sim_N_global(s, Z_DIR) > 1) dump_faces(zfaces, s, cells, ts, 1);
     struct timespec t0, t1;
     if (dtlog) flog = fopen(dtlog, "w");
     for (step = 0; step < warmup; ++step) timestep_rk2(ts, s, cells, gm, mpi);

@@ -5,6 +5,7 @@ from them by oracle/Makefile):
 
     python tests/golden/make_golden.py               # <case>.npz
     python tests/golden/make_golden.py --substep2    # <case>_sub2.npz
+    python tests/golden/make_golden.py --three-d     # the 3-D cases' <case>.npz
 
 Every fixture is the reference's own output (timestep_rk2 / face_create /
 the substep phases of timestep_substep) on a small disk, stored as a
@@ -171,6 +172,39 @@ def substep2(names: list[str]) -> None:
             print(name, "second substep", os.path.getsize(path), "bytes")
 
 
+# 3-D disks (NumZ > 1): the reference's own torus.par reduced in size.  The C
+# restatement of the oracle is 2-D only, so these pin the GPU path alone.
+CASES3D = {
+    "torus3d16": configs.torus_3d(num_r=16, num_z=8),
+}
+
+
+def three_d(names: list[str]) -> None:
+    """Writes <name>.npz for the 3-D cases: the initial state, its r- and
+    z-face lists, and the states after 1, 5 and 100 RK2 steps."""
+    if not oracle.have_ref():
+        oracle.build(ref=True, port=False)
+    with tempfile.TemporaryDirectory() as td:
+        for name, p in CASES3D.items():
+            if names and name not in names:
+                continue
+            par = configs.write_parfile(p, os.path.join(td, name + ".par"))
+            data = {"parfile": np.array(configs.parfile_text(p))}
+            st0, fr, _ = oracle.run(par, 0, faces=True)
+            _, fz, _ = oracle.run(par, 0, faces=True, zfaces=True)
+            data.update(_state_dict(st0, "init_"))
+            data["N_p"] = st0.N_p
+            data.update(_faces_dict(fr, "init_face_"))
+            data.update(_faces_dict(fz, "init_zface_"))
+            for n in STEPS:
+                st, _, log = oracle.run(par, n, dtlog=True)
+                data.update(_state_dict(st, f"step{n}_"))
+                data[f"step{n}_dtlog"] = log
+            path = os.path.join(HERE, name + ".npz")
+            np.savez_compressed(path, **data)
+            print(name, st0.N, "cells", os.path.getsize(path), "bytes")
+
+
 def main(names: list[str]) -> None:
     """Writes the fixtures of the named cases (all cases when none is named);
     each case draws its face layouts from its own seeded generator."""
@@ -210,5 +244,7 @@ def main(names: list[str]) -> None:
 if __name__ == "__main__":
     if sys.argv[1:2] == ["--substep2"]:
         substep2(sys.argv[2:])
+    elif sys.argv[1:2] == ["--three-d"]:
+        three_d(sys.argv[2:])
     else:
         main(sys.argv[1:])
