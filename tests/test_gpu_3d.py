@@ -111,3 +111,23 @@ def test_three_d_refusals():
     ctx.close()
     with pytest.raises(lib.DiscoError):
         lib.Context(lib.Sim(configs.torus_3d(num_r=16, num_z=8, BoundTypeZ=1)))
+
+
+def test_torus_par_full_size_100_steps_l1():
+    """torus.par at its own size after 100 RK2 steps against the reference on
+    the host: L1-relative 1e-10 in rho, S_r, L and tau."""
+    if not oracle.have_ref():
+        pytest.skip("the reference build is needed for the full-size run")
+    p = configs.torus_3d()
+    with tempfile.TemporaryDirectory() as td:
+        par = configs.write_parfile(p, os.path.join(td, "torus.par"))
+        want, _, _ = oracle.run(par, 100)
+    ctx = lib.Context(lib.Sim(p))
+    ctx.init_state(0)
+    ctx.step(100)
+    got = ctx.get_state(0)
+    t, _ = ctx.time(0)
+    ctx.close()
+    for q in (0, 2, 3, 1):
+        assert l1_rel(got["cons"][:, q], want.cons[:, q]) <= 1e-10, (q, l1_rel(got["cons"][:, q], want.cons[:, q]))
+    assert abs(t - want.t) <= 1e-12 * abs(want.t)
