@@ -1,6 +1,6 @@
 /*
  * The reference's own main loop with timestep_rk2 handed to the B200 library:
- * the binding that INTEGRATION.md describes, compiled from the reference's
+ * the Disco2-side binding a maintainer would add, compiled from the reference's
  * objects (oracle/Makefile, target `binding`) and linked against
  * libdisco_gpu.so.
  *
