@@ -22,9 +22,9 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CC = shutil.which("gcc") or "gcc"
 
-C_SOURCES = ["dgpu_sim.c", "dgpu_ctx.c", "dgpu_diff.c"]
+C_SOURCES = ["dgpu_sim.c", "dgpu_ctx.c", "dgpu_diff.c", "dgpu_h5.c", "dgpu_io.c"]
 CU_SOURCES = ["dgpu_kernels.cu", "dgpu_adjoint.cu", "dgpu_diag.cu"]
-HEADERS = ["dgpu_internal.h", "dgpu_sim.h", "dgpu_ctx.h", "dgpu_device.cuh", "dgpu_step.cuh", "dgpu_adjoint.cuh"]
+HEADERS = ["dgpu_internal.h", "dgpu_sim.h", "dgpu_ctx.h", "dgpu_h5.h", "dgpu_device.cuh", "dgpu_step.cuh", "dgpu_adjoint.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-fmad=false",

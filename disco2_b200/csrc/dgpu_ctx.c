@@ -148,27 +148,9 @@ int dgpu_sim_initial_state(const dgpu_sim *s, double *prim, double *tiph, double
             break;
           }
   }
-  if (rc == DGPU_OK && s->NZ > 1) {
-    /* main.c:66-67,111-112: the single-rank cell_syncproc_z after cell_create
-     * and after the initial data copies tiph and prim (and RKcons, still 0)
-     * of layers NZ-2ng .. NZ-ng-1 into the ng lowest layers and of layers
-     * ng .. 2ng-1 into the ng highest (src/Cell/cell_sync.c:156-205) */
-    const long per = (long)s->Ncells / s->NZ;
-    const int ng = s->ng_min[1], shift = s->NZ - 2 * ng;
-    int k;
-    for (k = 0; k < s->NZ; ++k) {
-      int ks;
-      long c0;
-      if (k < ng) ks = k + shift;
-      else if (k >= s->NZ - ng) ks = k - shift;
-      else continue;
-      for (c0 = 0; c0 < per; ++c0) {
-        const long dst = (long)k * per + c0, src = (long)ks * per + c0;
-        t[dst] = t[src];
-        if (prim) memcpy(prim + (size_t)s->NQ * dst, prim + (size_t)s->NQ * src, sizeof(double) * (size_t)s->NQ);
-      }
-    }
-  }
+  /* main.c:66-67,111-112: the syncs after cell_create and after the initial
+   * data */
+  if (rc == DGPU_OK) dsim_host_zsync(s, t, prim);
   if (t != tiph) free(t);
   if (d != dphi) free(d);
   return rc;

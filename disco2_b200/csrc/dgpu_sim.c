@@ -803,3 +803,25 @@ int dsim_initial_gravmass(const struct dgpu_sim *s, double *gm) {
   }
   return DGPU_OK;
 }
+
+void dsim_host_zsync(const struct dgpu_sim *s, double *tiph, double *prim) {
+  /* the single-rank cell_syncproc_z (src/Cell/cell_sync.c:156-205) copies
+   * tiph and prim (and RKcons) of layers NZ-2ng .. NZ-ng-1 into the ng lowest
+   * layers and of layers ng .. 2ng-1 into the ng highest: a periodic copy */
+  const long per = s->NZ > 0 ? (long)s->Ncells / s->NZ : 0;
+  const int ng = s->ng_min[1], shift = s->NZ - 2 * ng;
+  int k;
+  if (s->NZ <= 1) return;
+  for (k = 0; k < s->NZ; ++k) {
+    int ks;
+    long c0;
+    if (k < ng) ks = k + shift;
+    else if (k >= s->NZ - ng) ks = k - shift;
+    else continue;
+    for (c0 = 0; c0 < per; ++c0) {
+      const long dst = (long)k * per + c0, src = (long)ks * per + c0;
+      if (tiph) tiph[dst] = tiph[src];
+      if (prim) memcpy(prim + (size_t)s->NQ * dst, prim + (size_t)s->NQ * src, sizeof(double) * (size_t)s->NQ);
+    }
+  }
+}

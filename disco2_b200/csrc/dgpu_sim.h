@@ -78,6 +78,10 @@ void dsim_fill_params(const struct dgpu_sim *s, DiskParams *p);
 
 /* Initial phi edges of cell_create: srand(666), one rand() per annulus. */
 void dsim_initial_tiph(const struct dgpu_sim *s, double *tiph, double *dphi);
+/* The periodic z copy of the single-rank cell_syncproc_z on host arrays in
+ * (k, i, j) order: tiph[Ncells] and prim[Ncells][NQ] (either may be NULL).
+ * Nothing for NZ 1. */
+void dsim_host_zsync(const struct dgpu_sim *s, double *tiph, double *prim);
 
 /* GravMass initialisers (src/GravMass/GravMass_init.c:9-84) + gravMass_clean_pi;
  * gm[2][6] = r, phi, M, omega, Mdot, Macc. */

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdisco_gpu.so")
 
 OK = 0
 ERR_NAMES = {-1: "ARG", -2: "PARFILE", -3: "UNSUPPORTED", -4: "CUDA", -5: "FACE_OVERFLOW",
-             -6: "NUMERIC", -7: "NOMEM"}
+             -6: "NUMERIC", -7: "NOMEM", -8: "IO"}
 
 # Every symbol the header declares, with its ctypes signature.
 _P, _I, _D = C.c_void_p, C.c_int, C.c_double
@@ -59,6 +59,13 @@ SIGNATURES = {
     "dgpu_objective": (_I, [_P, _I, _I, _dp, _dp, _dp]),
     "dgpu_tangent": (_I, [_P, _I, _I, _D, _D, _dp, _dp, _dp]),
     "dgpu_adjoint": (_I, [_P, _I, _I, _I, _dp, _dp, _dp, _dp, _dp]),
+    "dgpu_hdf5_out": (_I, [C.c_char_p, _D, _dp, _dp, C.c_longlong, _I]),
+    "dgpu_hdf5_dims": (_I, [C.c_char_p, C.POINTER(C.c_longlong), _ip]),
+    "dgpu_hdf5_dataset": (_I, [C.c_char_p, C.c_char_p, _ip, C.POINTER(C.c_longlong), _dp]),
+    "dgpu_hdf5_in": (_I, [C.c_char_p, C.c_longlong, C.c_longlong, _I, _dp, _dp, _dp]),
+    "dgpu_sim_restart_state": (_I, [_P, C.c_char_p, _dp, _dp, _dp, _dp, _dp]),
+    "dgpu_checkpoint_out": (_I, [_P, _I, C.c_char_p]),
+    "dgpu_checkpoint_in": (_I, [_P, _I, C.c_char_p]),
 }
 
 _lib = None
@@ -138,6 +145,20 @@ class Sim:
             raise DiscoError(rc, load().dgpu_last_error(None).decode())
         return out
 
+    def restart_state(self, path) -> dict:
+        """Host-computed restart state from a checkpoint file (what
+        Context.checkpoint_in uploads): prim, tiph, dphi, gm and t."""
+        n = self.num_cells
+        out = {"prim": np.zeros((n, self.num_q)), "tiph": np.zeros(n), "dphi": np.zeros(n),
+               "gm": np.zeros((2, 6))}
+        t = C.c_double(0.0)
+        rc = load().dgpu_sim_restart_state(self._h, os.fsencode(path), _dptr(out["prim"]), _dptr(out["tiph"]),
+                                          _dptr(out["dphi"]), _dptr(out["gm"]), C.byref(t))
+        if rc != OK:
+            raise DiscoError(rc, load().dgpu_last_error(None).decode())
+        out["t"] = t.value
+        return out
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.dgpu_sim_destroy(self._h)
@@ -183,6 +204,14 @@ class Context:
         assert prim.shape == (n, self.sims[inst].num_q) and tiph.shape == (n,) and dphi.shape == (n,)
         self._ck(load().dgpu_set_state(self._h, inst, _dptr(prim), _dptr(tiph), _dptr(dphi)))
         self._ck(load().dgpu_synchronize(self._h))
+
+    def checkpoint_out(self, path, inst: int = 0) -> None:
+        """Write disk inst as a checkpoint file in the reference's layout."""
+        self._ck(load().dgpu_checkpoint_out(self._h, inst, os.fsencode(path)))
+
+    def checkpoint_in(self, path, inst: int = 0) -> None:
+        """Restart disk inst from a checkpoint file (the reference's restart set-up)."""
+        self._ck(load().dgpu_checkpoint_in(self._h, inst, os.fsencode(path)))
 
     def get_state(self, inst: int = 0) -> dict:
         n, nq = self.sims[inst].num_cells, self.sims[inst].num_q
@@ -340,3 +369,46 @@ class Context:
         self._ck(load().dgpu_adjoint(self._h, nsteps, window_start, ckpt_every, _dptr(w), _dptr(J),
                                      C.byref(dq), C.byref(da), _dptr(dprim)))
         return {"J": J, "dq": dq.value, "dalpha": da.value, "dprim": dprim}
+
+
+def hdf5_out(path, t: float, gravmass, data) -> None:
+    """Write a checkpoint file: T = t, GravMass [2][4], Data [rows][cols]."""
+    gravmass = np.ascontiguousarray(gravmass, np.float64)
+    data = np.ascontiguousarray(data, np.float64)
+    assert gravmass.shape == (2, 4) and data.ndim == 2
+    rc = load().dgpu_hdf5_out(os.fsencode(path), float(t), _dptr(gravmass), _dptr(data), data.shape[0], data.shape[1])
+    if rc != OK:
+        raise DiscoError(rc, load().dgpu_last_error(None).decode())
+
+
+def hdf5_in(path, row0: int = 0, nrows: int | None = None) -> dict:
+    """Read a checkpoint file: t, gravmass [2][4] and rows of Data."""
+    lib = load()
+    rows, cols = C.c_longlong(0), C.c_int(0)
+    rc = lib.dgpu_hdf5_dims(os.fsencode(path), C.byref(rows), C.byref(cols))
+    if rc != OK:
+        raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+    if nrows is None:
+        nrows = rows.value - row0
+    data = np.zeros((max(nrows, 0), cols.value))
+    gm = np.zeros((2, 4))
+    t = C.c_double(0.0)
+    rc = lib.dgpu_hdf5_in(os.fsencode(path), row0, nrows, cols.value, C.byref(t), _dptr(gm), _dptr(data))
+    if rc != OK:
+        raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+    return {"t": t.value, "gravmass": gm, "data": data}
+
+
+def hdf5_dataset(path, name: str) -> np.ndarray:
+    """One 64-bit float dataset of an HDF5 file's root group."""
+    lib = load()
+    rank = C.c_int(0)
+    dims = (C.c_longlong * 2)()
+    rc = lib.dgpu_hdf5_dataset(os.fsencode(path), name.encode(), C.byref(rank), dims, None)
+    if rc != OK:
+        raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+    out = np.zeros(tuple(int(d) for d in dims[:rank.value]))
+    rc = lib.dgpu_hdf5_dataset(os.fsencode(path), name.encode(), C.byref(rank), dims, _dptr(out))
+    if rc != OK:
+        raise DiscoError(rc, lib.dgpu_last_error(None).decode())
+    return out

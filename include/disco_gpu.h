@@ -35,12 +35,15 @@ extern "C" {
 #define DGPU_OK 0
 #define DGPU_ERR_ARG (-1)          /* bad argument or index */
 #define DGPU_ERR_PARFILE (-2)      /* parfile missing, unreadable or missing a key */
-#define DGPU_ERR_UNSUPPORTED (-3)  /* option outside the implemented path (e.g. NumZ > 1) */
+#define DGPU_ERR_UNSUPPORTED (-3)  /* option outside the implemented path (e.g. NumZ > 1
+                                      without a periodic z boundary) */
 #define DGPU_ERR_CUDA (-4)         /* a CUDA runtime call failed */
 #define DGPU_ERR_FACE_OVERFLOW (-5)/* face list exceeded its buffer (device flag) */
 #define DGPU_ERR_NUMERIC (-6)      /* device-detected condition the reference exit()s on or
                                       loops forever on, or a NaN in a non-ghost cell's state */
 #define DGPU_ERR_NOMEM (-7)        /* host or device allocation failed */
+#define DGPU_ERR_IO (-8)           /* checkpoint file unreadable, unwritable or not in the
+                                      layout of the reference's checkpoints */
 
 typedef struct dgpu_sim dgpu_sim; /* host-side Sim: parameters + grid */
 typedef struct dgpu_ctx dgpu_ctx; /* device context: state of one or more disks */
@@ -261,6 +264,49 @@ int dgpu_tangent(dgpu_ctx *ctx, int nsteps, int window_start, double dq, double 
  * nsteps / ckpt_every + 2 ckpt_every stored states of 19 doubles per cell). */
 int dgpu_adjoint(dgpu_ctx *ctx, int nsteps, int window_start, int ckpt_every, const double *weights, double *J,
                  double *dJ_dq, double *dJ_dalpha, double *dJ_dprim);
+
+/* ---- Checkpoint and restart ------------------------------------------------
+ * The reference's checkpoint files (src/IO/io_hdf5.c:15-266) without an HDF5
+ * library: datasets T [1], GravMass [2][4] (r, phi, M, omega per mass) and
+ * Data [rows][NUM_Q+3] of 64-bit floats in the root group of an HDF5 file
+ * (superblock 0, symbol-table root group, version-1 object headers,
+ * contiguous storage: the structures the HDF5 library writes by default).
+ * Host-only; every pointer is a host pointer.
+ *
+ * dgpu_hdf5_out replaces io_hdf5_out for one rank: writes a new file (it
+ * does not advance the reference's tcheck/nfile, which the caller keeps, as
+ * io_hdf5_out does at :152-155). */
+int dgpu_hdf5_out(const char *path, double t, const double *gravmass, const double *data, long long nrows, int ncols);
+/* One dataset of 64-bit floats (rank 0-2) in the root group of any HDF5
+ * file in the formats above: rank, dims[2] (1 past the rank) and, when data
+ * is not NULL, its values in row-major order. */
+int dgpu_hdf5_dataset(const char *path, const char *name, int *rank, long long *dims, double *data);
+/* Row and column counts of a checkpoint's Data. */
+int dgpu_hdf5_dims(const char *path, long long *nrows, int *ncols);
+/* Replaces io_hdf5_in (:161-266): T, GravMass (either pointer may be NULL)
+ * and rows [row0, row0 + nrows) of Data (the hyperslab at sim_offset of
+ * Ncells rows).  Unlike the reference, which ignores every HDF5 status, a
+ * missing dataset, a shape other than [rows][ncols] or rows outside Data is
+ * DGPU_ERR_IO. */
+int dgpu_hdf5_in(const char *path, long long row0, long long nrows, int ncols, double *t, double *gravmass,
+                 double *data);
+/* Host-only restart state: the restart branch of src/main.c:74-117 --
+ * cell_create's phi widths (dphi = 2pi/N_p; the file holds no dphi), tiph and
+ * prim from the file with prim[UZZ] = 0 when NumZ is 1 (io_readbuf,
+ * src/IO/io_buffer.c:60-81), the GravMass (r, phi, M, omega) from the file
+ * then gravMass_clean_pi, and the periodic z copy.  gm[2][6] as
+ * dgpu_get_gravmass (Mdot = Macc = 0: the reference leaves them
+ * uninitialised), t the file's T.  Any output pointer may be NULL. */
+int dgpu_sim_restart_state(const dgpu_sim *sim, const char *path, double *prim, double *tiph, double *dphi,
+                           double *gm, double *t);
+/* io_setbuf + io_hdf5_out for one disk of the context: Data rows in (k, i, j)
+ * order over all cells, ghosts included: tiph, annulus centre r, layer centre
+ * z, prim[NUM_Q] (src/IO/io_buffer.c:26-58). */
+int dgpu_checkpoint_out(dgpu_ctx *ctx, int inst, const char *path);
+/* Restart of one disk from a checkpoint: dgpu_sim_restart_state, then the
+ * state, GravMass and t uploaded and cons recomputed (cell_calc_cons,
+ * main.c:115).  The next dgpu_step_rk2 continues from there. */
+int dgpu_checkpoint_in(dgpu_ctx *ctx, int inst, const char *path);
 
 #ifdef __cplusplus
 }

@@ -17,18 +17,28 @@
  *
  * --fused steps with the fused substep (k_prep + k_sweep) instead of the
  * eight kernels.
+ *
+ * Checkpoints follow the reference too: with Restart 1 the state comes from
+ * input.h5 (main.c:95-102), and after a step that passes the next checkpoint
+ * time the state is written to checkpoint_%04d.h5 (main.c:132-139), both in
+ * the working directory.  The reference's io_setbuf / io_readbuf fill and
+ * read its checkpoint buffer; io_hdf5_out and io_hdf5_in, the two functions
+ * that need an HDF5 library, become dgpu_hdf5_out and dgpu_hdf5_in.  Each
+ * checkpoint written is reported on stderr as "checkpoint <file> step <n>".
  * Test infrastructure: the parity test compares its dump with the reference
  * build's own run of the same parfile (disco_ref run).
  */
 #define CELL_PRIVATE_DEFS
 #define PLANET_PRIVATE_DEFS
 #define TIMESTEP_PRIVATE_DEFS
+#define IO_PRIVATE_DEFS
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include "Headers/Cell.h"
 #include "Headers/GravMass.h"
+#include "Headers/IO.h"
 #include "Headers/MPIsetup.h"
 #include "Headers/Sim.h"
 #include "Headers/TimeStep.h"
@@ -87,6 +97,25 @@ static int dump(const char *path, struct Sim *s, struct Cell ***cells, struct Gr
   return 0;
 }
 
+/* download the GPU state into the reference's cells and GravMasses */
+static int download(dgpu_ctx *gctx, struct Sim *s, struct Cell ***cells, struct GravMass *gm, double *prim,
+                    double *cons, double *tiph, double *dphi) {
+  double g6[12];
+  int p;
+  if (dgpu_get_state(gctx, 0, prim, cons, tiph, dphi) != DGPU_OK || dgpu_get_gravmass(gctx, 0, g6) != DGPU_OK)
+    return die("state download", dgpu_last_error(gctx));
+  cell_unpack(cells, s, prim, cons, tiph, dphi);
+  for (p = 0; p < 2; ++p) {
+    gm[p].r = g6[6 * p + 0];
+    gm[p].phi = g6[6 * p + 1];
+    gm[p].M = g6[6 * p + 2];
+    gm[p].omega = g6[6 * p + 3];
+    gm[p].Mdot = g6[6 * p + 4];
+    gm[p].Macc = g6[6 * p + 5];
+  }
+  return 0;
+}
+
 int main(int argc, char **argv) {
   char parbuf[1024];
   int nsteps, step, p, fused = 0, N, NQ;
@@ -97,6 +126,7 @@ int main(int argc, char **argv) {
   struct GravMass *gm;
   struct Cell ***cells;
   struct TimeStep *ts;
+  struct IO *io;
   dgpu_sim *gs = NULL;
   dgpu_ctx *gctx = NULL;
   if (argc < 4) {
@@ -130,9 +160,25 @@ int main(int argc, char **argv) {
   cell_syncproc_r(cells, s, mpi);
   cell_syncproc_z(cells, s, mpi);
   ts = timestep_create(s);
-  (*gravMass_init_ptr(s))(gm, s);
-  (*cell_init_ptr(s))(cells, s, gm, mpi);
+  io = io_create(s);
+  if (sim_Restart(s) == 1) {
+    /* main.c:95-102 with io_hdf5_in -> dgpu_hdf5_in; Mdot and Macc, which the
+     * file does not hold, are zeroed rather than left as malloc returned them */
+    double tr;
+    memset(gm, 0, sizeof(struct GravMass) * (size_t)sim_NumGravMass(s));
+    io_allocbuf(io, s);
+    if (dgpu_hdf5_in("input.h5", sim_offset(s), sim_Ncells(s), sim_NUM_Q(s) + 3, &tr, &io->GravMassBuffer[0][0],
+                     io->buffer[0]) != DGPU_OK)
+      return die("dgpu_hdf5_in", dgpu_last_error(NULL));
+    timestep_set_t(ts, tr);
+    io_readbuf(io, cells, s, gm);
+    io_deallocbuf(io);
+  } else {
+    (*gravMass_init_ptr(s))(gm, s);
+    (*cell_init_ptr(s))(cells, s, gm, mpi);
+  }
   gravMass_clean_pi(gm, s);
+  io_setup(io, s, ts);
   cell_syncproc_r(cells, s, mpi);
   cell_syncproc_z(cells, s, mpi);
   cell_calc_cons(cells, s);
@@ -169,21 +215,27 @@ int main(int argc, char **argv) {
       return die("dgpu_step_rk2", dgpu_last_error(gctx));
     ts->t = t;
     ts->dt = dt;
+    if (timestep_get_t(ts) > io_tcheck(io)) {
+      /* main.c:132-139 with io_hdf5_out -> dgpu_hdf5_out, and the bookkeeping
+       * of io_hdf5.c:152-155 */
+      if (download(gctx, s, cells, gm, prim, cons, tiph, dphi)) return 2;
+      io_allocbuf(io, s);
+      io_setbuf(io, cells, s, gm);
+      if (dgpu_hdf5_out(io->filename, timestep_get_t(ts), &io->GravMassBuffer[0][0], io->buffer[0], sim_Ncells(s),
+                        sim_NUM_Q(s) + 3) != DGPU_OK)
+        return die("dgpu_hdf5_out", dgpu_last_error(NULL));
+      io_deallocbuf(io);
+      fprintf(stderr, "checkpoint %s step %d\n", io->filename, step + 1);
+      io->tcheck += io->dtcheck;
+      ++io->nfile;
+      sprintf(io->filename, "checkpoint_%04d.h5", io_nfile(io));
+    }
   }
 
   /* and back into the reference's structures */
-  if (dgpu_get_state(gctx, 0, prim, cons, tiph, dphi) != DGPU_OK || dgpu_get_gravmass(gctx, 0, g6) != DGPU_OK)
-    return die("state download", dgpu_last_error(gctx));
-  cell_unpack(cells, s, prim, cons, tiph, dphi);
-  for (p = 0; p < 2; ++p) {
-    gm[p].r = g6[6 * p + 0];
-    gm[p].phi = g6[6 * p + 1];
-    gm[p].M = g6[6 * p + 2];
-    gm[p].omega = g6[6 * p + 3];
-    gm[p].Mdot = g6[6 * p + 4];
-    gm[p].Macc = g6[6 * p + 5];
-  }
+  if (download(gctx, s, cells, gm, prim, cons, tiph, dphi)) return 2;
   if (dump(argv[3], s, cells, gm, ts)) return 2;
+  io_destroy(io);
   dgpu_destroy(gctx);
   dgpu_sim_destroy(gs);
   free(prim);

@@ -156,10 +156,56 @@ def read_faces(path: str) -> Faces:
     return Faces(nri, L, R, *arrs)
 
 
+def read_ckpt(path: str) -> dict:
+    """A checkpoint buffer dump (ref_driver.c, dump_ckpt): t, gravmass [2][4]
+    and data [nrows][ncols] as io_setbuf fills them."""
+    with open(path, "rb") as f:
+        b = f.read()
+    assert b[:8] == b"DCKPT1\0\0", path
+    nrows, ncols = np.frombuffer(b, "<i4", 2, 8)
+    t = float(np.frombuffer(b, "<f8", 1, 16)[0])
+    gm = np.frombuffer(b, "<f8", 8, 24).reshape(2, 4).copy()
+    data = np.frombuffer(b, "<f8", int(nrows) * int(ncols), 88).reshape(int(nrows), int(ncols)).copy()
+    return {"t": t, "gravmass": gm, "data": data}
+
+
+def write_ckpt(path: str, ck: dict) -> None:
+    """The inverse of read_ckpt (the driver's --restart input)."""
+    data = np.ascontiguousarray(ck["data"], "<f8")
+    with open(path, "wb") as f:
+        f.write(b"DCKPT1\0\0")
+        f.write(np.array(data.shape, "<i4").tobytes())
+        f.write(np.array([ck["t"]], "<f8").tobytes())
+        f.write(np.ascontiguousarray(ck["gravmass"], "<f8").tobytes())
+        f.write(data.tobytes())
+
+
+def checkpoint(parfile: str, nsteps: int, *, load: State | None = None, restart: dict | None = None) -> dict:
+    """Reference build: run `nsteps` RK2 steps and return the checkpoint
+    buffer that io_setbuf fills (src/IO/io_buffer.c:26-58)."""
+    exe = _exe("ref")
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "ck.bin")
+        cmd = [exe, "checkpoint", parfile, str(nsteps), out]
+        if load is not None:
+            lp = os.path.join(td, "in.bin")
+            write_state(lp, load)
+            cmd += ["--load", lp]
+        if restart is not None:
+            rp = os.path.join(td, "restart.bin")
+            write_ckpt(rp, restart)
+            cmd += ["--restart", rp]
+        subprocess.run(cmd, check=True, stderr=subprocess.PIPE)
+        return read_ckpt(out)
+
+
 def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = None,
-        faces: bool = False, dtlog: bool = False, workdir: str | None = None, zfaces: bool = False):
+        faces: bool = False, dtlog: bool = False, workdir: str | None = None, zfaces: bool = False,
+        restart: dict | None = None):
     """Run `nsteps` RK2 steps; returns (final State, Faces|None, dt log array|None).
-    zfaces (reference build, 3-D disks): the Faces are the z faces."""
+    zfaces (reference build, 3-D disks): the Faces are the z faces.  restart
+    (reference build): a checkpoint (t, gravmass, data) to start from instead
+    of the initial data, through the reference's restart branch."""
     exe = _exe(impl)
     if not os.path.exists(exe):
         raise FileNotFoundError(f"oracle binary missing: {exe} (run oracle.build())")
@@ -170,6 +216,10 @@ def run(parfile: str, nsteps: int, *, impl: str = "ref", load: State | None = No
             lp = os.path.join(td, "in.bin")
             write_state(lp, load)
             cmd += ["--load", lp]
+        if restart is not None:
+            rp = os.path.join(td, "restart.bin")
+            write_ckpt(rp, restart)
+            cmd += ["--restart", rp]
         fp = os.path.join(td, "faces.bin")
         if faces:
             cmd += ["--zfaces" if zfaces else "--faces", fp]

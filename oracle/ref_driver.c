@@ -35,6 +35,18 @@
  *       the working directory.  Dump: "DDIAG1\0\0", int32 nr neq, double t,
  *       VectorDiag[nr][17], ScalarDiag[16], EquatDiag[neq][18].
  *
+ *   disco_ref checkpoint <par> <nsteps> <out.bin> [--load in.bin] [--restart ck.bin]
+ *       runs nsteps steps and dumps the reference's checkpoint buffer
+ *       (io_allocbuf + io_setbuf, src/IO/io_buffer.c:10-58): "DCKPT1\0\0",
+ *       int32 nrows ncols, double t, GravMassBuffer[2][4], buffer[nrows][ncols].
+ *
+ *   --restart ck.bin (run and checkpoint modes) replaces the initial data by
+ *       the restart branch of src/main.c:95-102, with io_hdf5_in replaced by
+ *       reading a buffer file in the checkpoint dump format above: T, the
+ *       GravMass buffer and the cell buffer, then io_readbuf.  gravMass_create
+ *       mallocs the GravMasses, so Mdot and Macc, which the checkpoint does
+ *       not hold, would be whatever malloc returned; they are zeroed first.
+ *
  *   disco_ref stage <par> <phase> <out.bin> [--load in.bin]
  *       runs the prologue of timestep_rk2 and then the body of
  *       timestep_substep (src/TimeStep/timestep_routines.c:16-113), calling
@@ -59,6 +71,7 @@
 #define TIMESTEP_PRIVATE_DEFS
 #define PLANET_PRIVATE_DEFS
 #define DIAGNOSTICS_PRIVATE_DEFS
+#define IO_PRIVATE_DEFS
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -67,6 +80,7 @@
 #include "Headers/Diagnostics.h"
 #include "Headers/Face.h"
 #include "Headers/GravMass.h"
+#include "Headers/IO.h"
 #include "Headers/MPIsetup.h"
 #include "Headers/Riemann.h"
 #include "Headers/Sim.h"
@@ -300,8 +314,61 @@ static void objectives(struct Sim *s, struct Cell ***cells, struct GravMass *gm,
   *mdot = M;
 }
 
+/* the checkpoint buffer of io_setbuf, dumped */
+static void dump_ckpt(const char *path, struct Sim *s, struct Cell ***cells, struct GravMass *gm,
+                      struct TimeStep *ts) {
+  struct IO *io = io_create(s);
+  int nrows = sim_Ncells(s), ncols = sim_NUM_Q(s) + 3;
+  FILE *f;
+  io_allocbuf(io, s);
+  io_setbuf(io, cells, s, gm);
+  f = fopen(path, "wb");
+  if (!f) {
+    fprintf(stderr, "cannot open %s\n", path);
+    exit(2);
+  }
+  wr(f, "DCKPT1\0", 1, 8);
+  wr(f, &nrows, sizeof(int), 1);
+  wr(f, &ncols, sizeof(int), 1);
+  wr(f, &ts->t, sizeof(double), 1);
+  wr(f, io->GravMassBuffer, sizeof(double), 8);
+  wr(f, io->buffer[0], sizeof(double), (size_t)nrows * (size_t)ncols);
+  fclose(f);
+  io_deallocbuf(io);
+  io_destroy(io);
+}
+
+/* the restart branch of main.c:95-102 with io_hdf5_in replaced by a read of
+ * the dump format of dump_ckpt */
+static void restart_from(const char *path, struct Sim *s, struct Cell ***cells, struct GravMass *gm,
+                         struct TimeStep *ts) {
+  struct IO *io = io_create(s);
+  int nrows, ncols;
+  char magic[8];
+  double t;
+  FILE *f = fopen(path, "rb");
+  if (!f || fread(magic, 1, 8, f) != 8 || memcmp(magic, "DCKPT1\0", 8) || fread(&nrows, sizeof(int), 1, f) != 1 ||
+      fread(&ncols, sizeof(int), 1, f) != 1 || nrows != sim_Ncells(s) || ncols != sim_NUM_Q(s) + 3) {
+    fprintf(stderr, "bad checkpoint buffer %s\n", path);
+    exit(2);
+  }
+  io_allocbuf(io, s);
+  if (fread(&t, sizeof(double), 1, f) != 1 || fread(io->GravMassBuffer, sizeof(double), 8, f) != 8 ||
+      fread(io->buffer[0], sizeof(double), (size_t)nrows * (size_t)ncols, f) != (size_t)nrows * (size_t)ncols) {
+    fprintf(stderr, "short checkpoint buffer %s\n", path);
+    exit(2);
+  }
+  fclose(f);
+  timestep_set_t(ts, t);
+  memset(gm, 0, sizeof(struct GravMass) * (size_t)sim_NumGravMass(s));
+  io_readbuf(io, cells, s, gm);
+  io_deallocbuf(io);
+  io_destroy(io);
+}
+
 int main(int argc, char **argv) {
-  const char *mode, *par, *out, *load = NULL, *faces = NULL, *zfaces = NULL, *dtlog = NULL, *dtfile = NULL;
+  const char *mode, *par, *out, *load = NULL, *faces = NULL, *zfaces = NULL, *dtlog = NULL, *dtfile = NULL,
+             *restart = NULL;
   int nsteps, a, step, warmup = 0;
   char parbuf[1024];
   struct MPIsetup *mpi;
@@ -325,6 +392,7 @@ int main(int argc, char **argv) {
     else if (!strcmp(argv[a], "--dtlog") && a + 1 < argc) dtlog = argv[++a];
     else if (!strcmp(argv[a], "--warmup") && a + 1 < argc) warmup = atoi(argv[++a]);
     else if (!strcmp(argv[a], "--dtfile") && a + 1 < argc) dtfile = argv[++a];
+    else if (!strcmp(argv[a], "--restart") && a + 1 < argc) restart = argv[++a];
     else {
       fprintf(stderr, "unknown option %s\n", argv[a]);
       return 2;
@@ -359,8 +427,12 @@ int main(int argc, char **argv) {
   cell_syncproc_z(cells, s, mpi);
   ts = timestep_create(s);
   ts->dt = 0.0;
-  (*gravMass_init_ptr(s))(gm, s);
-  (*cell_init_ptr(s))(cells, s, gm, mpi);
+  if (restart) {
+    restart_from(restart, s, cells, gm, ts);
+  } else {
+    (*gravMass_init_ptr(s))(gm, s);
+    (*cell_init_ptr(s))(cells, s, gm, mpi);
+  }
   gravMass_clean_pi(gm, s);
   if (load) load_state(load, s, cells);
   cell_syncproc_r(cells, s, mpi);
@@ -382,6 +454,9 @@ int main(int argc, char **argv) {
     fprintf(stderr, "steps_wall_s %.9f\n", (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec));
     if (flog) fclose(flog);
     dump_state(out, s, cells, gm, ts, 0);
+  } else if (!strcmp(mode, "checkpoint")) {
+    for (step = 0; step < nsteps; ++step) timestep_rk2(ts, s, cells, gm, mpi);
+    dump_ckpt(out, s, cells, gm, ts);
   } else if (!strcmp(mode, "objective")) {
     FILE *fo = fopen(out, "w"), *fd = dtfile ? fopen(dtfile, "r") : NULL;
     if (!fo || (dtfile && !fd)) {

@@ -6,6 +6,7 @@ from them by oracle/Makefile):
     python tests/golden/make_golden.py               # <case>.npz
     python tests/golden/make_golden.py --substep2    # <case>_sub2.npz
     python tests/golden/make_golden.py --three-d     # the 3-D cases' <case>.npz
+    python tests/golden/make_golden.py --checkpoint  # ckpt_<case>.npz
 
 Every fixture is the reference's own output (timestep_rk2 / face_create /
 the substep phases of timestep_substep) on a small disk, stored as a
@@ -205,6 +206,38 @@ def three_d(names: list[str]) -> None:
             print(name, st0.N, "cells", os.path.getsize(path), "bytes")
 
 
+CKPT_CASES = ("gresho16", "kepler24", "cbd32", "torus3d16")
+
+
+def checkpoint(names: list[str]) -> None:
+    """Writes ckpt_<name>.npz: the reference's checkpoint buffer (io_setbuf)
+    of the initial state (ck0_) and after 5 RK2 steps (ck5_), the state
+    after the reference's restart set-up from the 5-step buffer (rs_), and
+    after 5 more steps from there (rs5_)."""
+    if not oracle.have_ref():
+        oracle.build(ref=True, port=False)
+    cases = {**CASES, **CASES3D}
+    with tempfile.TemporaryDirectory() as td:
+        for name in CKPT_CASES:
+            if names and name not in names:
+                continue
+            p = cases[name]
+            par = configs.write_parfile(p, os.path.join(td, name + ".par"))
+            data = {"parfile": np.array(configs.parfile_text(p))}
+            for n in (0, 5):
+                ck = oracle.checkpoint(par, n)
+                data[f"ck{n}_t"] = np.float64(ck["t"])
+                data[f"ck{n}_gm"] = ck["gravmass"]
+                data[f"ck{n}_data"] = ck["data"]
+            ck5 = oracle.checkpoint(par, 5)
+            for n in (0, 5):
+                st = oracle.run(par, n, restart=ck5)[0]
+                data.update(_state_dict(st, "rs_" if n == 0 else f"rs{n}_"))
+            path = os.path.join(HERE, f"ckpt_{name}.npz")
+            np.savez_compressed(path, **data)
+            print(name, os.path.getsize(path), "bytes")
+
+
 def main(names: list[str]) -> None:
     """Writes the fixtures of the named cases (all cases when none is named);
     each case draws its face layouts from its own seeded generator."""
@@ -246,5 +279,7 @@ if __name__ == "__main__":
         substep2(sys.argv[2:])
     elif sys.argv[1:2] == ["--three-d"]:
         three_d(sys.argv[2:])
+    elif sys.argv[1:2] == ["--checkpoint"]:
+        checkpoint(sys.argv[2:])
     else:
         main(sys.argv[1:])
