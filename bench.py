@@ -340,7 +340,7 @@ def run_adjoint(args):
     """Cost of the gradient against the forward it differentiates: the
     circumbinary disk at 192 annuli, 500 RK2 steps, both objectives averaged
     over steps 251-500; forward = dgpu_objective (graph-replayed steps plus the
-    objective after each step), plain = the same number of dgpu_step_rk2
+    objective after each step of its window), plain = the same number of dgpu_step_rk2
     steps with no objective, adjoint = dgpu_adjoint (forward sweep with a
     checkpoint every 25 steps, then each segment replayed and reversed),
     tangent = dgpu_tangent along q.  Wall time of the synchronous calls."""

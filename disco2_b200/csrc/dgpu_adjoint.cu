@@ -237,10 +237,11 @@ __device__ __forceinline__ void snap_copy_dev(const DevPtrs &d, double *sb, Inst
 __global__ void __launch_bounds__(BLK) k_snap_ptr(DevPtrs d, double *sb, InstState *si, int save) {
   snap_copy_dev(d, sb, si, save);
 }
-// the store of slot *idx + off of a table of stores
+// the store of slot *idx + off of a table of stores (slot 0 below 0: the
+// reverse sweep's look-ahead rebuild past a segment's first step)
 __global__ void __launch_bounds__(BLK) k_snap_tab(DevPtrs d, double *const *bufs, InstState *const *ists,
                                                   const int *idx, int off, int save) {
-  const int k = *idx + off;
+  const int k = max(*idx + off, 0);
   snap_copy_dev(d, bufs[k], ists[k], save);
 }
 

@@ -19,7 +19,9 @@
  * The adjoint stores the state every ckpt_every steps, and replays each
  * segment forward before running it backwards: per step it keeps the state
  * before each substep, rebuilds that substep's intermediates with the
- * forward kernels and runs the substep's adjoint kernels.
+ * forward kernels and runs the substep's adjoint kernels.  The rebuild of a
+ * step's intermediates runs one reverse step ahead, on its own stream and
+ * buffer sets, beside the adjoint kernels of the step after it.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -37,10 +39,13 @@ typedef struct {
   InstState *ist;
 } Snap;
 
-/* step graphs: logged forward step, the same with a frozen dt, tangent step,
+/* step graphs: logged forward step, the same without the objective (steps
+ * before the objective window), the same with a frozen dt, tangent step,
  * segment replay step into stored-state set 0 / 1 (shadow buffers, second
- * stream), reverse step from set 0 / 1 */
-enum { G_OBJ, G_OBJ_DT, G_TAN, G_SEG0, G_SEG1, G_REV0, G_REV1, G_N };
+ * stream), reverse step from set s with intermediates in buffer parity p
+ * (G_REV + 2 s + p), the rebuild of a segment's first reverse step
+ * (G_PRIME + 2 s + p) */
+enum { G_OBJ, G_STEP, G_OBJ_DT, G_TAN, G_SEG0, G_SEG1, G_REV, G_PRIME = G_REV + 4, G_N = G_PRIME + 4 };
 
 struct dgpu_diff {
   /* tangent */
@@ -68,10 +73,11 @@ struct dgpu_diff {
   void *sh_mem;
   cudaStream_t s2;
   cudaEvent_t e_rep, e_rev;
-  /* a second copy for the reverse step: substep 1's intermediates are rebuilt
-   * there (stream s3) while substep 2 is reversed on the context's buffers */
-  DevPtrs pp;
-  void *pp_mem;
+  /* the reverse step's buffers: rb[p] holds substep 2's intermediates and
+   * rb[2 + p] substep 1's, for the reverse steps of parity p; the other
+   * parity's are rebuilt (stream s3) while these are reversed */
+  DevPtrs rb[4];
+  void *rb_mem[4];
   cudaStream_t s3;
   cudaEvent_t e_fork, e_join;
   /* step graphs (G_*), valid for tab_K */
@@ -115,7 +121,7 @@ void dctx_diff_free(struct dgpu_ctx *c) {
   if (D->s2) cudaStreamDestroy(D->s2);
   if (D->e_rep) cudaEventDestroy(D->e_rep);
   if (D->e_rev) cudaEventDestroy(D->e_rev);
-  cudaFree(D->pp_mem);
+  for (k = 0; k < 4; ++k) cudaFree(D->rb_mem[k]);
   if (D->s3) cudaStreamDestroy(D->s3);
   if (D->e_fork) cudaEventDestroy(D->e_fork);
   if (D->e_join) cudaEventDestroy(D->e_join);
@@ -365,7 +371,10 @@ static int alloc_shadow(struct dgpu_ctx *c, DevPtrs *h, void **mem) {
 
 static int ensure_shadow(struct dgpu_ctx *c, struct dgpu_diff *D) {
   if (D->sh_mem) return DGPU_OK;
-  if (alloc_shadow(c, &D->sh, &D->sh_mem) || alloc_shadow(c, &D->pp, &D->pp_mem)) return DGPU_ERR_CUDA;
+  int k;
+  if (alloc_shadow(c, &D->sh, &D->sh_mem)) return DGPU_ERR_CUDA;
+  for (k = 0; k < 4; ++k)
+    if (alloc_shadow(c, &D->rb[k], &D->rb_mem[k])) return DGPU_ERR_CUDA;
   CK(cudaMalloc((void **)&D->d_idx2, sizeof(int)));
   CK(cudaStreamCreateWithFlags(&D->s2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&D->e_rep, cudaEventDisableTiming));
@@ -426,7 +435,8 @@ static int prep_substep(struct dgpu_ctx *c, DevPtrs *h, cudaStream_t s, int sub)
 static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
   struct dgpu_diff *Dd = D;
   const int nbK = D->tab_K;
-  const int set = (which == G_SEG1 || which == G_REV1) ? 1 : 0;
+  const int set = which == G_SEG1 ? 1 : which >= G_REV ? ((which - G_REV) / 2) & 1 : 0;
+  const int par = which >= G_REV ? (which - G_REV) & 1 : 0;
   double *const *tabS = (double *const *)D->tab_buf[set];
   InstState *const *istS = (InstState *const *)D->tab_ist[set];
   double *const *tabM = (double *const *)(D->tab_buf[set] + nbK + 1);
@@ -435,6 +445,9 @@ static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
     case G_OBJ: /* one step, its objective and dt into slot *idx, ++*idx */
       if (dctx_launch_step(c)) return -1;
       if (dgk_objective(&c->d, NULL, Dd->o_part, Dd->o_val, NULL, Dd->d_idx, c->stream)) return -1;
+      return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
+    case G_STEP: /* one step and its dt into slot *idx, ++*idx */
+      if (dctx_launch_step(c)) return -1;
       return dgk_step_end(&c->d, Dd->dtlog, Dd->d_idx, c->stream);
     case G_OBJ_DT: /* the same with dt = dtin[*idx] */
       if (dgk_cellprep(&c->d, NULL, 1, c->stream) || dgk_merge(&c->d, 1, c->stream) ||
@@ -459,25 +472,46 @@ static int record_graph(struct dgpu_ctx *c, struct dgpu_diff *D, int which) {
           shadow_substep(c, &Dd->sh, Dd->s2, 2, Dd->rec[set], Dd->d_idx2))
         return -1;
       return dgk_add_int(Dd->d_idx2, 1, Dd->s2);
-    case G_REV0:
-    case G_REV1: /* reverse step *idx of the segment (step n = *base + *idx):
-                    substep 1's intermediates are rebuilt on the second buffer
-                    set (stream s3) while substep 2 is reversed */
+    case G_REV:
+    case G_REV + 1:
+    case G_REV + 2:
+    case G_REV + 3: { /* reverse step *idx of the segment (step n = *base + *idx)
+                         on the intermediates of buffers rb[par], rb[2 + par],
+                         while step *idx - 1's are rebuilt in the other parity's
+                         (stream s3; at *idx = 0 the slot is clamped to 0 and the
+                         rebuild goes unused) */
+      DevPtrs *b2 = &Dd->rb[par], *b1 = &Dd->rb[2 + par], *n2 = &Dd->rb[1 - par], *n1 = &Dd->rb[3 - par];
       if (dgk_adj_objective(&c->d, &Dd->J, tabS, istS, Dd->d_idx, 1, Dd->wts, Dd->d_base, c->stream)) return -1;
       if (cudaEventRecord(Dd->e_fork, c->stream) != cudaSuccess ||
           cudaStreamWaitEvent(Dd->s3, Dd->e_fork, 0) != cudaSuccess)
         return -1;
-      if (dgk_snap_tab(&Dd->pp, tabS, istS, Dd->d_idx, 0, 0, Dd->s3) || prep_substep(c, &Dd->pp, Dd->s3, 1)) return -1;
-      if (dgk_snap_tab(&c->d, tabM, istM, Dd->d_idx, 0, 0, c->stream) ||
-          dctx_substep(c, NULL, 2, DCTX_ADJPREP, NULL, NULL) ||
-          dgk_adj_substep(&c->d, &Dd->J, 2, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
+      if (dgk_snap_tab(n2, tabM, istM, Dd->d_idx, -1, 0, Dd->s3) || prep_substep(c, n2, Dd->s3, 2) ||
+          dgk_snap_tab(n1, tabS, istS, Dd->d_idx, -1, 0, Dd->s3) || prep_substep(c, n1, Dd->s3, 1))
+        return -1;
+      if (dgk_adj_substep(b2, &Dd->J, 2, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]) ||
+          dgk_adj_substep(b1, &Dd->J, 1, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
         return -1;
       if (cudaEventRecord(Dd->e_join, Dd->s3) != cudaSuccess ||
           cudaStreamWaitEvent(c->stream, Dd->e_join, 0) != cudaSuccess)
         return -1;
-      if (dgk_adj_substep(&Dd->pp, &Dd->J, 1, Dd->rec[set], Dd->d_idx, c->stream, c->side, c->fork[0], c->fork[1]))
-        return -1;
       return dgk_add_int(Dd->d_idx, -1, c->stream);
+    }
+    case G_PRIME:
+    case G_PRIME + 1:
+    case G_PRIME + 2:
+    case G_PRIME + 3: { /* the intermediates of reverse step *idx in rb[par], rb[2 + par] */
+      const int pr = (which - G_PRIME) & 1;
+      const int st = ((which - G_PRIME) / 2) & 1;
+      double *const *tS = (double *const *)D->tab_buf[st];
+      InstState *const *iS = (InstState *const *)D->tab_ist[st];
+      double *const *tM = (double *const *)(D->tab_buf[st] + nbK + 1);
+      InstState *const *iM = (InstState *const *)(D->tab_ist[st] + nbK + 1);
+      if (dgk_snap_tab(&Dd->rb[pr], tM, iM, Dd->d_idx, 0, 0, c->stream) || prep_substep(c, &Dd->rb[pr], c->stream, 2) ||
+          dgk_snap_tab(&Dd->rb[2 + pr], tS, iS, Dd->d_idx, 0, 0, c->stream) ||
+          prep_substep(c, &Dd->rb[2 + pr], c->stream, 1))
+        return -1;
+      return DGPU_OK;
+    }
   }
   return -1;
 }
@@ -553,7 +587,7 @@ int dgpu_objective(dgpu_ctx *c, int nsteps, int window_start, const double *dt_i
   if (dt_in) CK(cudaMemcpyAsync(D->dtin, dt_in, sizeof(double) * (size_t)nsteps, cudaMemcpyHostToDevice, c->stream));
   CKK(dgk_set_int(D->d_idx, 0, c->stream));
   for (n = 0; n < nsteps; ++n)
-    if ((rc = launch_graph(c, D, dt_in ? G_OBJ_DT : G_OBJ))) return rc;
+    if ((rc = launch_graph(c, D, dt_in ? G_OBJ_DT : n >= window_start ? G_OBJ : G_STEP))) return rc;
   if ((rc = dgpu_synchronize(c))) return rc;
   if (dt_out) CK(cudaMemcpy(dt_out, D->dtlog, sizeof(double) * (size_t)nsteps, cudaMemcpyDeviceToHost));
   return window_mean(c, D, nsteps, window_start, D->o_val, J, NULL);
@@ -621,7 +655,8 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
   CKK(dgk_set_int(D->d_idx, 0, c->stream));
   for (n = 0; n < nsteps; ++n) {
     if (n % K == 0) CKK(dgk_snap(&c->d, ck[n / K].buf, ck[n / K].ist, 1, c->stream));
-    if ((rc = launch_graph(c, D, G_OBJ))) return rc;
+    /* the objective only inside its window */
+    if ((rc = launch_graph(c, D, n >= window_start ? G_OBJ : G_STEP))) return rc;
   }
   CKK(dgk_snap(&c->d, fin->buf, fin->ist, 1, c->stream));
   if ((rc = dgpu_synchronize(c))) return rc;
@@ -670,8 +705,9 @@ int dgpu_adjoint(dgpu_ctx *c, int nsteps, int window_start, int ckpt_every, cons
       CK(cudaStreamWaitEvent(c->stream, D->e_rep, 0));
       CKK(dgk_set_int(D->d_idx, n1 - n0 - 1, c->stream));
       CKK(dgk_set_int(D->d_base, n0, c->stream));
+      if ((rc = launch_graph(c, D, G_PRIME + 2 * set + ((n1 - 1 - n0) & 1)))) return rc;
       for (n = n1 - 1; n >= n0; --n)
-        if ((rc = launch_graph(c, D, set ? G_REV1 : G_REV0))) return rc;
+        if ((rc = launch_graph(c, D, G_REV + 2 * set + ((n - n0) & 1)))) return rc;
       CK(cudaEventRecord(D->e_rev, c->stream));
     }
     if (seg - 1 >= 0) CK(cudaEventRecord(D->e_rep, D->s2));
