@@ -206,7 +206,7 @@ def three_d(names: list[str]) -> None:
             print(name, st0.N, "cells", os.path.getsize(path), "bytes")
 
 
-CKPT_CASES = ("gresho16", "kepler24", "cbd32", "torus3d16")
+CKPT_CASES = ("gresho16", "kepler24", "cbd32", "torus3d16", "vortex16dye")
 
 
 def checkpoint(names: list[str]) -> None:

@@ -29,7 +29,7 @@ except ImportError:
     pass
 
 needs_scipy_file = pytest.mark.skipif(SCIPY_H5 is None, reason="scipy's HDF5 test file is not installed")
-CASES = ("gresho16", "kepler24", "cbd32", "torus3d16")
+CASES = ("gresho16", "kepler24", "cbd32", "torus3d16", "vortex16dye")
 
 
 def ckpt(name):
