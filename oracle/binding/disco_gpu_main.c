@@ -13,10 +13,14 @@
  * into the reference's own structures, which are dumped in the oracle
  * driver's state format.
  *
- *   disco_gpu_main <par> <nsteps> <out.bin> [--fused]
+ *   disco_gpu_main <par> <nsteps> <out.bin> [--fused] [--lazy]
  *
- * --fused steps with the fused substep (k_prep + k_sweep) instead of the
- * eight kernels.
+ * The loop is the reference's own (src/main.c:124-141) with timestep_rk2
+ * replaced by timestep_rk2_gpu (timestep_gpu.c: the same signature, the
+ * state kept on the GPU), for at most nsteps steps.  --fused steps with the
+ * fused substep (k_prep + k_sweep) instead of the eight kernels; --lazy
+ * leaves the state on the GPU between steps and brings it back only for the
+ * checkpoints and the final dump.
  *
  * Checkpoints follow the reference too: with Restart 1 the state comes from
  * input.h5 (main.c:95-102), and after a step that passes the next checkpoint
@@ -46,6 +50,7 @@
 #include "cell_pack.h"
 #include "disco_gpu.h"
 #include "ref_newic.h"
+#include "timestep_gpu.h"
 
 int readvar(char *filename, char *varname, int vartype, void *ptr);
 
@@ -97,47 +102,28 @@ static int dump(const char *path, struct Sim *s, struct Cell ***cells, struct Gr
   return 0;
 }
 
-/* download the GPU state into the reference's cells and GravMasses */
-static int download(dgpu_ctx *gctx, struct Sim *s, struct Cell ***cells, struct GravMass *gm, double *prim,
-                    double *cons, double *tiph, double *dphi) {
-  double g6[12];
-  int p;
-  if (dgpu_get_state(gctx, 0, prim, cons, tiph, dphi) != DGPU_OK || dgpu_get_gravmass(gctx, 0, g6) != DGPU_OK)
-    return die("state download", dgpu_last_error(gctx));
-  cell_unpack(cells, s, prim, cons, tiph, dphi);
-  for (p = 0; p < 2; ++p) {
-    gm[p].r = g6[6 * p + 0];
-    gm[p].phi = g6[6 * p + 1];
-    gm[p].M = g6[6 * p + 2];
-    gm[p].omega = g6[6 * p + 3];
-    gm[p].Mdot = g6[6 * p + 4];
-    gm[p].Macc = g6[6 * p + 5];
-  }
-  return 0;
-}
-
 int main(int argc, char **argv) {
   char parbuf[1024];
-  int nsteps, step, p, fused = 0, N, NQ;
-  double g6[12], t, dt;
-  double *prim, *cons, *tiph, *dphi;
+  int nsteps, step = 0, a, fused = 0, lazy = 0;
   struct MPIsetup *mpi;
   struct Sim *s;
   struct GravMass *gm;
   struct Cell ***cells;
   struct TimeStep *ts;
   struct IO *io;
-  dgpu_sim *gs = NULL;
-  dgpu_ctx *gctx = NULL;
   if (argc < 4) {
-    fprintf(stderr, "usage: disco_gpu_main <parfile> <nsteps> <out.bin> [--fused]\n");
+    fprintf(stderr, "usage: disco_gpu_main <parfile> <nsteps> <out.bin> [--fused] [--lazy]\n");
     return 2;
   }
   strncpy(parbuf, argv[1], sizeof(parbuf) - 1);
   parbuf[sizeof(parbuf) - 1] = 0;
   nsteps = atoi(argv[2]);
-  if (argc > 4 && !strcmp(argv[4], "--fused")) fused = 1;
-  /* the reference prints read notices on stdout */
+  for (a = 4; a < argc; ++a) {
+    if (!strcmp(argv[a], "--fused")) fused = 1;
+    else if (!strcmp(argv[a], "--lazy")) lazy = 1;
+    else return die("unknown option", argv[a]);
+  }
+  /* the reference prints read notices and its per-step line on stdout */
   if (!freopen("/dev/null", "w", stdout)) return 2;
 
   /* src/main.c:56-119 */
@@ -183,64 +169,32 @@ int main(int argc, char **argv) {
   cell_syncproc_z(cells, s, mpi);
   cell_calc_cons(cells, s);
 
-  /* the state crosses to the GPU once */
-  N = cell_pack_count(s);
-  NQ = sim_NUM_Q(s);
-  prim = (double *)malloc(sizeof(double) * (size_t)N * (size_t)NQ);
-  cons = (double *)malloc(sizeof(double) * (size_t)N * (size_t)NQ);
-  tiph = (double *)malloc(sizeof(double) * (size_t)N);
-  dphi = (double *)malloc(sizeof(double) * (size_t)N);
-  if (!prim || !cons || !tiph || !dphi) return die("out of memory", NULL);
-  if (dgpu_sim_from_parfile(parbuf, &gs) != DGPU_OK) return die("dgpu_sim_from_parfile", dgpu_last_error(NULL));
-  if (dgpu_sim_num_cells(gs) != N) return die("grid", "the library's grid differs from the reference's");
-  if (dgpu_create((const dgpu_sim *const *)&gs, 1, 0, NULL, &gctx) != DGPU_OK)
-    return die("dgpu_create", dgpu_last_error(NULL));
-  if (fused && dgpu_set_fused(gctx, 1) != DGPU_OK) return die("dgpu_set_fused", dgpu_last_error(gctx));
-  cell_pack(cells, s, prim, tiph, dphi);
-  for (p = 0; p < 2; ++p) {
-    g6[6 * p + 0] = gm[p].r;
-    g6[6 * p + 1] = gm[p].phi;
-    g6[6 * p + 2] = gm[p].M;
-    g6[6 * p + 3] = gm[p].omega;
-    g6[6 * p + 4] = gm[p].Mdot;
-    g6[6 * p + 5] = gm[p].Macc;
-  }
-  if (dgpu_set_state(gctx, 0, prim, tiph, dphi) != DGPU_OK || dgpu_set_gravmass(gctx, 0, g6) != DGPU_OK ||
-      dgpu_set_time(gctx, 0, timestep_get_t(ts)) != DGPU_OK)
-    return die("state upload", dgpu_last_error(gctx));
+  if (timestep_gpu_open(parbuf, 0, fused) != DGPU_OK) return 1;
+  timestep_gpu_lazy(lazy);
 
-  /* src/main.c:124-141: timestep_rk2 becomes dgpu_step_rk2 */
-  for (step = 0; step < nsteps && timestep_get_t(ts) < sim_get_T_MAX(s); ++step) {
-    if (dgpu_step_rk2(gctx, 1) != DGPU_OK || dgpu_get_time(gctx, 0, &t, &dt) != DGPU_OK)
-      return die("dgpu_step_rk2", dgpu_last_error(gctx));
-    ts->t = t;
-    ts->dt = dt;
+  /* src/main.c:124-141 */
+  while (timestep_get_t(ts) < sim_get_T_MAX(s) && step < nsteps) {
+    timestep_rk2_gpu(ts, s, cells, gm, mpi);
+    ++step;
     if (timestep_get_t(ts) > io_tcheck(io)) {
       /* main.c:132-139 with io_hdf5_out -> dgpu_hdf5_out, and the bookkeeping
        * of io_hdf5.c:152-155 */
-      if (download(gctx, s, cells, gm, prim, cons, tiph, dphi)) return 2;
+      if (lazy) timestep_gpu_sync(s, cells, gm);
       io_allocbuf(io, s);
       io_setbuf(io, cells, s, gm);
       if (dgpu_hdf5_out(io->filename, timestep_get_t(ts), &io->GravMassBuffer[0][0], io->buffer[0], sim_Ncells(s),
                         sim_NUM_Q(s) + 3) != DGPU_OK)
         return die("dgpu_hdf5_out", dgpu_last_error(NULL));
       io_deallocbuf(io);
-      fprintf(stderr, "checkpoint %s step %d\n", io->filename, step + 1);
+      fprintf(stderr, "checkpoint %s step %d\n", io->filename, step);
       io->tcheck += io->dtcheck;
       ++io->nfile;
       sprintf(io->filename, "checkpoint_%04d.h5", io_nfile(io));
     }
   }
-
-  /* and back into the reference's structures */
-  if (download(gctx, s, cells, gm, prim, cons, tiph, dphi)) return 2;
+  if (lazy) timestep_gpu_sync(s, cells, gm);
   if (dump(argv[3], s, cells, gm, ts)) return 2;
+  timestep_gpu_close();
   io_destroy(io);
-  dgpu_destroy(gctx);
-  dgpu_sim_destroy(gs);
-  free(prim);
-  free(cons);
-  free(tiph);
-  free(dphi);
   return 0;
 }
