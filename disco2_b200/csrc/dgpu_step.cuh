@@ -140,20 +140,7 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
           }
         }
       };
-      int n = s;
-      for (; n + 1 < e; n += 2) {
-        T u[8], v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          if (q < 5 || visc) {
-            u[q] = ldinc<T, NC>(d.frf, tp.frf, q, NS, n);
-            v[q] = ldinc<T, NC>(d.frf, tp.frf, q, NS, n + 1);
-          }
-        }
-        apply(u);
-        apply(v);
-      }
-      if (n < e) {
+      for (int n = s; n < e; ++n) {
         T u[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q)
