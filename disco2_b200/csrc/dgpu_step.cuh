@@ -113,7 +113,8 @@ __device__ __forceinline__ bool update_sum(const DevPtrs &d, const TanPtrs &tp, 
     }
   }
   if (stop == 2) return false;
-  // r faces in face-list order, two faces' increments loaded at a time
+  // r faces in face-list order, one face's increments at a time (two at a time
+  // spill more at the kernel's 64-register budget)
   {
     const int NS = d.n_slots;
     const bool visc = P.has_visc;
