@@ -169,3 +169,34 @@ def test_binding_checkpoints_and_restart(tmp_path):
     for k in ("prim", "tiph", "dphi"):
         assert np.array_equal(getattr(got, k), st[k]), k
     assert got.t == ctx.time(0)[0]
+
+
+def test_checkpoints_of_one_disk_in_a_batch(tmp_path):
+    """In a context of several disks, checkpoint_out / checkpoint_in act on the
+    named disk alone: its file equals that of a context holding it alone, and
+    a restart of disk 1 leaves disk 0 as it was."""
+    ga, gb = ckpt("kepler24"), ckpt("cbd32")
+    sa, sb = lib.Sim(str(ga["parfile"])), lib.Sim(str(gb["parfile"]))
+    both = lib.Context([sa, sb])
+    both.init_state(0)
+    both.init_state(1)
+    both.step(3)
+    alone = lib.Context(sb)
+    alone.init_state(0)
+    alone.step(3)
+    p1, p2 = str(tmp_path / "b1.h5"), str(tmp_path / "alone.h5")
+    both.checkpoint_out(p1, inst=1)
+    alone.checkpoint_out(p2)
+    a, b = lib.hdf5_in(p1), lib.hdf5_in(p2)
+    assert np.array_equal(a["data"], b["data"]) and a["t"] == b["t"]
+    assert np.array_equal(a["gravmass"], b["gravmass"])
+    before = both.get_state(0)
+    path = str(tmp_path / "input.h5")
+    lib.hdf5_out(path, float(gb["ck5_t"]), gb["ck5_gm"], gb["ck5_data"])
+    both.checkpoint_in(path, inst=1)
+    after = both.get_state(0)
+    for k in ("prim", "cons", "tiph", "dphi"):
+        assert np.array_equal(before[k], after[k]), k
+    st = both.get_state(1)
+    for k in ("prim", "tiph", "dphi"):
+        assert np.array_equal(st[k], gb["rs_" + k]), k
