@@ -750,21 +750,37 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double
   return DGPU_OK;
 }
 
-/* One substep of a context holding a 3-D disk, on the context's stream: the
- * z faces join after the r fluxes (timestep_routines.c:63-71), the viscous
- * source reads the z slopes, and the periodic z copy closes the substep. */
+/* One substep of a context holding a 3-D disk: the z faces' increments are
+ * added after the r faces' in the update (timestep_routines.c:63-71), the
+ * viscous source reads the z slopes, and the periodic z copy closes the
+ * substep.  Three branches on the second stream: the r- and z-face lists
+ * beside cellprep, the z slopes beside the r slopes, and the sources, phi and
+ * z faces beside the r faces; each branch reads only what was written before
+ * its fork. */
 static int launch_substep_3d(struct dgpu_ctx *c, int sub) {
+  CK(cudaEventRecord(c->fork[0], c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
+  CKK(dgk_merge(&c->d, sub, c->side));
+  CKK(dgk_zmerge(&c->d, sub, c->side));
   CKK(dgk_cellprep(&c->d, NULL, sub, c->stream));
-  CKK(dgk_merge(&c->d, sub, c->stream));
-  CKK(dgk_zmerge(&c->d, sub, c->stream));
+  CK(cudaEventRecord(c->fork[1], c->side));
+  CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
+  CK(cudaEventRecord(c->fork[2], c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->fork[2], 0));
+  CKK(dgk_zslope(&c->d, c->side));
+  CKK(dgk_plm_z(&c->d, c->side));
   CKK(dgk_rslope(&c->d, NULL, c->stream));
   CKK(dgk_plm_r(&c->d, NULL, sub, c->stream));
-  CKK(dgk_flux_phi(&c->d, NULL, sub, c->stream));
+  CK(cudaEventRecord(c->fork[3], c->side));
+  CK(cudaStreamWaitEvent(c->stream, c->fork[3], 0));
+  CK(cudaEventRecord(c->fork[0], c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
+  CKK(dgk_source(&c->d, NULL, sub, c->side));
+  CKK(dgk_flux_phi(&c->d, NULL, sub, c->side));
+  CKK(dgk_flux_z(&c->d, sub, c->side));
   CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
-  CKK(dgk_zslope(&c->d, c->stream));
-  CKK(dgk_plm_z(&c->d, c->stream));
-  CKK(dgk_flux_z(&c->d, sub, c->stream));
-  CKK(dgk_source(&c->d, NULL, sub, c->stream));
+  CK(cudaEventRecord(c->fork[1], c->side));
+  CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
   CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
   if (c->n_ob > 0) CKK(dgk_outflow(&c->d, 7, c->stream));
   CKK(dgk_zsync(&c->d, sub, c->stream));
