@@ -393,6 +393,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-alt", action="store_true", help="skip timing the other substep form")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--batch-cpu-steps", type=int, default=1,
                     help="RK2 steps per disk of the sweep's host baseline (0: skip it)")
@@ -533,6 +534,36 @@ def main():
     e2e = nin * ke * world / e2e_s
 
     ctx.close()
+
+    # the other substep form on the same disk (informational): the fused
+    # k_prep + k_sweep when the line is the eight-kernel graph, and back
+    alt = None
+    if world == 1 and not args.no_alt:
+        actx = lib.Context(sim, device=local, stream=stream.cuda_stream)
+        actx.set_fused(not fused)
+        actx.init_state(0)
+        if args.tune_steps > 0:
+            actx.autotune(args.tune_steps)
+        with torch.cuda.stream(stream):
+            actx.step(args.warmup, sync=False)
+        actx.synchronize()
+        ka = max(3, min(args.steps, 100))
+        a_s = [torch.cuda.Event(enable_timing=True) for _ in range(ka)]
+        a_e = [torch.cuda.Event(enable_timing=True) for _ in range(ka)]
+        for k in range(ka):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a_s[k].record(stream)
+                L.dgpu_step_rk2(actx.handle, 1)
+                a_e[k].record(stream)
+        actx.synchronize()
+        torch.cuda.synchronize()
+        a_ms = sum(x.elapsed_time(y) for x, y in zip(a_s, a_e))
+        alt = {"substep": "eight kernels" if fused else "fused (k_prep + k_sweep)", "steps": ka,
+               "ms_per_step": a_ms / ka, "value": nin * ka / (a_ms / 1e3), "unit": UNIT,
+               "how": "same disk and timing as the line (autotuned, L2 flushed before each step)"}
+        actx.close()
+
     batched = None
     if not args.no_batched:
         batched = run_batched(args, rank, world, flush, barrier, max_over_ranks)
@@ -582,6 +613,7 @@ def main():
                                         "dgpu_step_rk2(1), dgpu_get_state to pinned host, per step"},
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "alt_substep": alt,
             "batched": batched,
             "adjoint": adjoint,
         }
