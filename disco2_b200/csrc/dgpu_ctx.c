@@ -458,6 +458,17 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
     }
     c->d.smem_face = mx <= 48 * 1024 ? mx : 0;
   }
+  {
+    /* threads per merge block: 256, or fewer when every annulus is small, so
+     * that more pairs are resident per SM (a torus ring of 20 cells leaves
+     * most of 256 threads idle); at least a warp, and about two inner cells
+     * per thread at most */
+    int a, mnp = 0, nt = 32;
+    for (a = 0; a < c->n_ann; ++a)
+      if (c->h_ann[a].np > mnp) mnp = c->h_ann[a].np;
+    while (nt < 256 && 2 * nt < mnp) nt *= 2;
+    c->d.merge_nt = nt;
+  }
   /* the fused substep covers the forward step of disks without passive
    * scalars, outflow radial boundary or sink; it is opt-in (dgpu_set_fused):
    * on B200 the eight-kernel graph is faster (0.375 against 0.55 ms per step

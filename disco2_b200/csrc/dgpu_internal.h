@@ -157,6 +157,7 @@ typedef struct {
   double *fdp;            /* [2][n_slots] r-face offsets dpL, dpR (wrapped to [-pi, pi]) */
   double *ann_c;          /* [4][n_ann] per substep: kappa, cos(kappa dt), sin(kappa dt), 1-exp(-rate dt) */
   int smem_face;          /* dynamic shared bytes of k_merge (0: merge reads global memory) */
+  int merge_nt;           /* threads per k_merge / k_zmerge block (32..256) */
   int *fstart;            /* first r-face (within the pair slab) of each inner cell */
   int *rr;                /* [n_cells][4] r-face ranges (within the slab of pair i-1) of each outer cell:
                              [x, y) and [z, w) for its two runs; z = INT_MIN: more runs */

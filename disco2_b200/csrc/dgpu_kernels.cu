@@ -1805,7 +1805,7 @@ int dgk_cellprep(const DevPtrs *d, const TanPtrs *t, int substep, void *stream) 
   return (int)cudaGetLastError();
 }
 int dgk_merge(const DevPtrs *d, int substep, void *stream) {
-  k_merge<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
+  k_merge<<<d->n_ann, d->merge_nt > 0 ? d->merge_nt : BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_rslope(const DevPtrs *d, const TanPtrs *t, void *stream) {
@@ -1865,7 +1865,7 @@ int dgk_update_stage(const DevPtrs *d, int substep, int stop, void *stream) {
 }
 int dgk_zmerge(const DevPtrs *d, int substep, void *stream) {
   if (!d->has_z) return 0;
-  k_zmerge<<<d->n_ann, BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
+  k_zmerge<<<d->n_ann, d->merge_nt > 0 ? d->merge_nt : BLK, d->smem_face, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_zslope(const DevPtrs *d, void *stream) {
