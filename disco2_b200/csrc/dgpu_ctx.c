@@ -338,6 +338,11 @@ int dgpu_create(const dgpu_sim *const *sims, int n, int device, void *stream, dg
   c->d.max_nz = 1;
   for (k = 0; k < n; ++k)
     if (c->sims[k]->NZ > c->d.max_nz) c->d.max_nz = c->sims[k]->NZ;
+  /* one 3-D disk: its ghost layers are the first and last cells, and the
+   * periodic z copy launches over those alone */
+  c->d.zghost = 0;
+  if (n == 1 && has_z && c->sims[0]->NZ >= 2 * c->sims[0]->ng_min[1])
+    c->d.zghost = c->sims[0]->ng_min[1] * (c->sims[0]->Ncells / c->sims[0]->NZ);
   c->n_upd_blocks = dgk_update_blocks(c->n_cells);
 
   if (cudaSetDevice(device) != cudaSuccess) {

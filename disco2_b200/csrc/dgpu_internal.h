@@ -158,6 +158,8 @@ typedef struct {
   double *ann_c;          /* [4][n_ann] per substep: kappa, cos(kappa dt), sin(kappa dt), 1-exp(-rate dt) */
   int smem_face;          /* dynamic shared bytes of k_merge (0: merge reads global memory) */
   int merge_nt;           /* threads per k_merge / k_zmerge block (32..256) */
+  int zghost;             /* cells of the ng lowest layers of the context's one 3-D disk, which
+                             with the ng highest are the first and last cells (0: several disks) */
   int *fstart;            /* first r-face (within the pair slab) of each inner cell */
   int *rr;                /* [n_cells][4] r-face ranges (within the slab of pair i-1) of each outer cell:
                              [x, y) and [z, w) for its two runs; z = INT_MIN: more runs */

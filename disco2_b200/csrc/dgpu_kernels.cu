@@ -965,9 +965,11 @@ __global__ void __launch_bounds__(BLK) k_flux_z(DevPtrs d, int substep) {
 // ng highest those of layers ng .. 2ng-1 (dphi stays the cell's own).  Runs
 // after k_update and the radial boundary, which have finished every layer.
 __global__ void __launch_bounds__(BLK) k_zsync(DevPtrs d, int substep) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int N = d.n_cells;
-  if (g >= N) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = d.n_cells, zg = d.zghost;
+  // zghost > 0: threads cover the ng lowest layers' cells, then the ng highest
+  const int g = zg > 0 ? (t < zg ? t : N - 2 * zg + t) : t;
+  if (zg > 0 ? t >= 2 * zg : g >= N) return;
   const int a = d.cell_ann[g];
   const Annulus &A = d.ann[a];
   const DiskParams &P = d.par[A.inst];
@@ -1617,28 +1619,35 @@ __global__ void __launch_bounds__(BLK) k_calc_cons(DevPtrs d, TanPtrs tp) {
 // (prim - 0 * grad * (...) / 2.) * dA is prim * dA for a finite slope.  A cell
 // with no face keeps its own value, divided (the reference zeroes only the
 // cells its face loop visits).
-__device__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int base, int i, int outer) {
+__device__ __forceinline__ void outflow_pass(const DevPtrs &d, const DiskParams &P, int base, int i, int outer) {
   const int a = base + i + outer;
   const Annulus &A = d.ann[a];
   const Annulus &S = d.ann[base + i + 1 - outer];  // the annulus read
   const double rf = d.ann[base + i].f_r;           // FacePos(i)
   const size_t NB = d.n_ob;
   const int nq = 5 + P.num_n;
+  const int np = nq - 5;
   for (int j = threadIdx.x; j < A.np; j += blockDim.x) {
     const int g = A.cell_off + j;
-    double s[5 + DGPU_MAX_PASSIVE];
-    for (int q = 0; q < nq; ++q) s[q] = 0.0;
+    // the five hydro sums in registers, the passive scalars' apart
+    double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, sp[DGPU_MAX_PASSIVE];
+    for (int k = 0; k < np; ++k) sp[k] = 0.0;
     int nface = 0;
     for_cell_rfaces(d, A, a, g, P.NR, [&](const RFace &F, int, int side) {
       if (side != outer) return;
       const int o = S.ob_off + ((outer ? F.cL : F.cR) - S.cell_off);
       const double dA = F.r * F.dphi * F.dperp;
-      for (int q = 0; q < nq; ++q) s[q] += d.obuf[q * NB + o] * dA;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) s[q] += d.obuf[q * NB + o] * dA;
+      for (int k = 0; k < np; ++k) sp[k] += d.obuf[(5 + k) * NB + o] * dA;
       ++nface;
     });
     const double dA = A.dz * rf * d.dphi[g];
     const size_t self = (size_t)A.ob_off + j;
-    for (int q = 0; q < nq; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) d.obuf[q * NB + self] = (nface ? s[q] : d.obuf[q * NB + self]) / dA;
+    for (int k = 0; k < np; ++k)
+      d.obuf[(5 + k) * NB + self] = (nface ? sp[k] : d.obuf[(5 + k) * NB + self]) / dA;
   }
 }
 
@@ -1885,7 +1894,8 @@ int dgk_flux_z(const DevPtrs *d, int substep, void *stream) {
 }
 int dgk_zsync(const DevPtrs *d, int substep, void *stream) {
   if (!d->has_z) return 0;
-  k_zsync<<<(d->n_cells + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
+  const int n = d->zghost > 0 ? 2 * d->zghost : d->n_cells;
+  k_zsync<<<(n + BLK - 1) / BLK, BLK, 0, (cudaStream_t)stream>>>(*d, substep);
   return (int)cudaGetLastError();
 }
 int dgk_prep(const DevPtrs *d, int substep, void *stream) {
