@@ -770,9 +770,9 @@ int dctx_substep(struct dgpu_ctx *c, const TanPtrs *t, int sub, int mode, double
  * added after the r faces' in the update (timestep_routines.c:63-71), the
  * viscous source reads the z slopes, and the periodic z copy closes the
  * substep.  Three branches on the second stream: the r- and z-face lists
- * beside cellprep, the z slopes beside the r slopes, and the sources, phi and
- * z faces beside the r faces; each branch reads only what was written before
- * its fork. */
+ * beside cellprep, the z slopes beside the r slopes, and the sources and phi
+ * faces beside the r and z faces; each branch reads only what was written
+ * before its fork. */
 static int launch_substep_3d(struct dgpu_ctx *c, int sub) {
   CK(cudaEventRecord(c->fork[0], c->stream));
   CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
@@ -793,8 +793,8 @@ static int launch_substep_3d(struct dgpu_ctx *c, int sub) {
   CK(cudaStreamWaitEvent(c->side, c->fork[0], 0));
   CKK(dgk_source(&c->d, NULL, sub, c->side));
   CKK(dgk_flux_phi(&c->d, NULL, sub, c->side));
-  CKK(dgk_flux_z(&c->d, sub, c->side));
   CKK(dgk_flux_r(&c->d, NULL, sub, c->stream));
+  CKK(dgk_flux_z(&c->d, sub, c->stream));
   CK(cudaEventRecord(c->fork[1], c->side));
   CK(cudaStreamWaitEvent(c->stream, c->fork[1], 0));
   CKK(dgk_update(&c->d, NULL, sub, 7, c->stream));
