@@ -394,6 +394,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-alt", action="store_true", help="skip timing the other substep form")
+    ap.add_argument("--no-3d", action="store_true", help="skip timing the 3-D torus")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--batch-cpu-steps", type=int, default=1,
                     help="RK2 steps per disk of the sweep's host baseline (0: skip it)")
@@ -564,6 +565,37 @@ def main():
                "how": "same disk and timing as the line (autotuned, L2 flushed before each step)"}
         actx.close()
 
+    # the reference's torus.par (3-D, 80 x 80 annuli and layers), informational
+    three_d = None
+    if world == 1 and not args.no_3d:
+        from disco2_b200 import configs as _cf
+        tsim = lib.Sim(_cf.torus_3d())
+        tctx = lib.Context(tsim, device=local, stream=stream.cuda_stream)
+        tctx.init_state(0)
+        if args.tune_steps > 0:
+            tctx.autotune(args.tune_steps)
+        with torch.cuda.stream(stream):
+            tctx.step(args.warmup, sync=False)
+        tctx.synchronize()
+        kt = max(3, min(args.steps, 100))
+        t_s = [torch.cuda.Event(enable_timing=True) for _ in range(kt)]
+        t_e = [torch.cuda.Event(enable_timing=True) for _ in range(kt)]
+        for k in range(kt):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                t_s[k].record(stream)
+                L.dgpu_step_rk2(tctx.handle, 1)
+                t_e[k].record(stream)
+        tctx.synchronize()
+        torch.cuda.synchronize()
+        t_ms = sum(x.elapsed_time(y) for x, y in zip(t_s, t_e))
+        tin = interior_cells(tsim) * int(tsim.param("NumZ"))  # non-ghost annuli of the non-ghost layers
+        three_d = {"workload": f"torus.par: 3-D torus, 80 annuli x 80 layers, periodic z ({tsim.num_cells} cells, "
+                               f"{tin} interior)", "steps": kt, "ms_per_step": t_ms / kt,
+                   "value": tin * kt / (t_ms / 1e3), "unit": UNIT,
+                   "how": "autotuned, L2 flushed before each step, CUDA events on the library's stream"}
+        tctx.close()
+
     batched = None
     if not args.no_batched:
         batched = run_batched(args, rank, world, flush, barrier, max_over_ranks)
@@ -614,6 +646,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clocks,
             "alt_substep": alt,
+            "three_d": three_d,
             "batched": batched,
             "adjoint": adjoint,
         }
