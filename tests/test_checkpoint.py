@@ -163,3 +163,102 @@ def test_restart_state_refuses_another_grid(tmp_path):
     lib.hdf5_out(path, 0.0, g["ck5_gm"], g["ck5_data"][:-1])
     with pytest.raises(lib.DiscoError, match="IO"):
         lib.Sim(str(g["parfile"])).restart_state(path)
+
+
+# ---------------------------------------------------------------------------
+# The reader's wider formats, on a file laid out here by hand from the format
+# specification: a 512-byte user block, superblock version 1, a root group
+# whose B-tree has an internal node over two leaves (two symbol-table nodes),
+# a NIL message in the root header, a dataset header split by a continuation
+# message, layout versions 1 (contiguous) and 3 (compact), dataspace
+# version 2.
+# ---------------------------------------------------------------------------
+def _crafted(path):
+    import struct
+
+    UB, UND = 512, 0xFFFFFFFFFFFFFFFF
+    buf = bytearray(8192)
+
+    def put(at, fmt, *v):
+        struct.pack_into("<" + fmt, buf, UB + at, *v)
+
+    def msg(at, typ, body, flags=0):
+        body = body + b"\0" * (-len(body) % 8)
+        put(at, "HHB3x", typ, len(body), flags)
+        buf[UB + at + 8:UB + at + 8 + len(body)] = body
+        return at + 8 + len(body)
+
+    def header(at, msgs, size):
+        put(at, "BxHII4x", 1, len(msgs), 1, size)
+        m = at + 16
+        for typ, body in msgs:
+            m = msg(m, typ, body)
+        assert m - at - 16 <= size
+
+    f64 = bytes([0x11, 0x20, 63, 0]) + struct.pack("<IHHBBBBI", 8, 0, 64, 52, 11, 0, 52, 1023)
+    a_vals = np.arange(6.0).reshape(3, 2) + 0.5
+    b_vals = np.array([2.0, -3.0, 4.25])
+    c_vals = np.array([[7.0, 8.0]])
+    # names in the local heap
+    names = {"": 0, "A": 8, "B": 16, "C": 24}
+    heap, heap_data = 200, 240
+    put(heap, "4sB3xQQQ", b"HEAP", 0, 32, 1, heap_data)
+    for nm, off in names.items():
+        raw = nm.encode() + b"\0"
+        buf[UB + heap_data + off:UB + heap_data + off + len(raw)] = raw
+    # B-tree: an internal node (level 1) over two leaves, each with one SNOD
+    root_bt, leaf1, leaf2, snod1, snod2 = 300, 900, 1500, 2100, 2500
+    put(root_bt, "4sBBHQQ", b"TREE", 0, 1, 2, UND, UND)
+    put(root_bt + 24, "QQQQQ", 0, leaf1, names["B"], leaf2, names["C"])
+    put(leaf1, "4sBBHQQ", b"TREE", 0, 0, 1, UND, leaf2)
+    put(leaf1 + 24, "QQQ", 0, snod1, names["B"])
+    put(leaf2, "4sBBHQQ", b"TREE", 0, 0, 1, leaf1, UND)
+    put(leaf2 + 24, "QQQ", names["B"], snod2, names["C"])
+    oh_a, oh_b, oh_b2, oh_c = 3000, 3300, 3600, 3900
+    put(snod1, "4sBxH", b"SNOD", 1, 2)
+    put(snod1 + 8, "QQI4x16x", names["A"], oh_a, 0)
+    put(snod1 + 48, "QQI4x16x", names["B"], oh_b, 0)
+    put(snod2, "4sBxH", b"SNOD", 1, 1)
+    put(snod2 + 8, "QQI4x16x", names["C"], oh_c, 0)
+    # root group header: a NIL message, then the symbol table message
+    root = 100
+    header(root, [(0x0000, b"\0" * 8), (0x0011, struct.pack("<QQ", root_bt, heap))], 48)
+    # A: dataspace v1 (3 x 2), datatype, layout v1 contiguous
+    a_data = 4200
+    header(oh_a, [(0x0001, struct.pack("<BBBx4xQQ", 1, 2, 0, 3, 2)), (0x0003, f64),
+                  (0x0008, struct.pack("<BBB5xQIII", 1, 3, 1, a_data, 3, 2, 8))], 120)
+    buf[UB + a_data:UB + a_data + 48] = a_vals.astype("<f8").tobytes()
+    # B: dataspace in the first block, then a continuation to a second block
+    # holding the datatype and a layout v3 contiguous
+    b_data = 4300
+    header(oh_b, [(0x0001, struct.pack("<BBBx4xQ", 1, 1, 0, 3)), (0x0010, struct.pack("<QQ", oh_b2, 64))], 48)
+    m = msg(oh_b2, 0x0003, f64)
+    msg(m, 0x0008, struct.pack("<BBQQ", 3, 1, b_data, 24))
+    put(oh_b, "BxHII4x", 1, 4, 1, 48)  # four messages over both blocks
+    buf[UB + b_data:UB + b_data + 24] = b_vals.astype("<f8").tobytes()
+    # C: dataspace v2, compact layout v3 holding the values
+    header(oh_c, [(0x0001, struct.pack("<BBBBQQ", 2, 2, 0, 1, 1, 2)), (0x0003, f64),
+                  (0x0008, struct.pack("<BBH", 3, 0, 16) + c_vals.astype("<f8").tobytes())], 96)
+    eof = 4400
+    # superblock version 1 at the end of the user block, base address 512
+    sb = b"\x89HDF\r\n\x1a\n" + struct.pack("<BBBBBBBBHHIHH", 1, 0, 0, 0, 0, 8, 8, 0, 4, 16, 0, 32, 0)
+    sb += struct.pack("<QQQQ", UB, UND, eof, UND)
+    sb += struct.pack("<QQI4x16x", 0, root, 0)
+    buf[UB:UB + len(sb)] = sb
+    buf[:16] = b"user block here\0"
+    with open(path, "wb") as f:
+        f.write(bytes(buf[:UB + eof]))
+    return {"A": a_vals, "B": b_vals, "C": c_vals}
+
+
+def test_reader_formats_beyond_the_writer(tmp_path):
+    path = str(tmp_path / "crafted.h5")
+    want = _crafted(path)
+    for name, w in want.items():
+        got = lib.hdf5_dataset(path, name)
+        assert np.array_equal(got.reshape(w.shape), w), name
+    # the independent walk reads the contiguous ones the same way
+    f = H5(path)
+    assert f.sb_version == 1 and f.base == 512 and len(f.snods) == 2
+    assert np.array_equal(f.dataset("A")[0], want["A"])
+    assert np.array_equal(f.dataset("B")[0], want["B"])
