@@ -262,3 +262,32 @@ def test_reader_formats_beyond_the_writer(tmp_path):
     assert f.sb_version == 1 and f.base == 512 and len(f.snods) == 2
     assert np.array_equal(f.dataset("A")[0], want["A"])
     assert np.array_equal(f.dataset("B")[0], want["B"])
+
+
+def test_corrupted_files_are_errors_not_crashes(tmp_path):
+    """Seeded byte corruptions and truncations of a checkpoint: each read
+    either succeeds or raises DiscoError; the reading process never crashes
+    (run in a child process, so a fault would show as its exit status)."""
+    import random
+    import subprocess
+    import sys
+
+    good = str(tmp_path / "ck.h5")
+    lib.hdf5_out(good, 1.0, np.zeros((2, 4)), np.arange(80.0).reshape(10, 8))
+    raw = open(good, "rb").read()
+    rng = random.Random(20251204)
+    files = []
+    for k in range(200):
+        b = bytearray(raw)
+        for _ in range(rng.randint(1, 8)):
+            b[rng.randrange(len(b))] = rng.randrange(256)
+        if rng.random() < 0.2:
+            b = b[:rng.randrange(len(b))]
+        q = tmp_path / f"c{k}.h5"
+        q.write_bytes(bytes(b))
+        files.append(str(q))
+    code = ("import sys\nsys.path.insert(0, sys.argv[1])\nfrom disco2_b200 import lib\n"
+            "for f in sys.argv[2:]:\n    try:\n        lib.hdf5_in(f)\n    except lib.DiscoError:\n        pass\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code, root] + files, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
