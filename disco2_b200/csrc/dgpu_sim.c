@@ -143,6 +143,12 @@ int dsim_build_grid(struct dgpu_sim *s, char *err, int errlen) {
     snprintf(err, (size_t)errlen, "grid: NumR, NumZ and ng must be positive");
     return DGPU_ERR_PARFILE;
   }
+  /* every annulus holds at least one cell, so NumR x NumZ bounds the cell
+   * count from below: refuse what cannot fit before laying out the grid */
+  if ((long)s->NumR * (long)s->NumZ > 0x7fffffffL / 16 || s->ng > 1024) {
+    snprintf(err, (size_t)errlen, "grid: NumR %d x NumZ %d (ng %d) is too large", s->NumR, s->NumZ, s->ng);
+    return DGPU_ERR_ARG;
+  }
   /* sim_alloc_arr (src/Sim/sim_alloc_arr.c:9-46) for the only rank */
   s->ng_min[0] = 1;
   s->ng_max[0] = s->ng;

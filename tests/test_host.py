@@ -132,3 +132,25 @@ def test_three_d_initial_state_matches_the_reference():
     h = sim.initial_state()
     for k in ("prim", "tiph", "dphi"):
         assert np.array_equal(h[k], g["init_" + k]), k
+
+
+@pytest.mark.parametrize("over,code", [
+    ({"NumR": 0}, "PARFILE"),
+    ({"NumR": -5}, "PARFILE"),
+    ({"NumR": 2147483647}, "ARG"),
+    ({"NumZ": 2147483647}, "ARG"),
+    ({"NumR": 400000, "NumZ": 400000}, "ARG"),
+    ({"ng": 100000}, "ARG"),
+])
+def test_impossible_grids_are_refused_quickly(over, code):
+    """Grids the int cell numbering cannot hold (or nonsense sizes) are
+    refused before the grid is laid out, not by an allocation failure or an
+    overflow."""
+    import time
+
+    p = configs.kepler_ring(num_r=24)
+    p.update(over)
+    t0 = time.perf_counter()
+    with pytest.raises(lib.DiscoError, match=code):
+        lib.Sim(configs.parfile_text(p))
+    assert time.perf_counter() - t0 < 5.0
